@@ -1,0 +1,223 @@
+/*
+ * rtm.h - C ABI of librtm.so, the B200 (sm_100a) solve path of rooftop-mom.
+ *
+ * A thin MEX gateway binds these entry points under the unchanged MATLAB
+ * +rooftopMoM call signatures; the tests bind them through Python ctypes.
+ *
+ * Conventions
+ *   - Complex arrays are interleaved (re, im) doubles (MATLAB R2018a+ interleaved complex, the same
+ *     layout as cuDoubleComplex). FP32 device vectors are interleaved floats.
+ *   - Grids are column-major with the x index fastest, exactly as the MATLAB arrays: generator
+ *     magneticXX is (countX-1) x countY, magneticYY countX x (countY-1), electric countX x countY.
+ *   - Rooftop vectors hold the x-directed rooftops first, then the y-directed ones, each grid
+ *     column-major (src/+rooftopMoM/+basisFunctions/UniformRooftops.m:1-8).
+ *   - `where` says whether a pointer is host (RTM_HOST) or device (RTM_DEVICE) memory. Host
+ *     arguments are copied in and out inside the call.
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the library's own stream of the handle.
+ *   - Every call returns an rtm_status; rtm_last_error() gives the message of the last failure on
+ *     the calling thread. Nothing here aborts the process or falls back to the CPU.
+ */
+#ifndef RTM_H
+#define RTM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RTM_API __attribute__((visibility("default")))
+#else
+#define RTM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTM_VERSION_MAJOR 3
+#define RTM_VERSION_MINOR 5
+#define RTM_VERSION_PATCH 0
+
+typedef enum rtm_status {
+    RTM_OK = 0,
+    RTM_ERR_ARG = 1,        /* invalid argument (null pointer, bad enum, non-finite) */
+    RTM_ERR_SIZE = 2,       /* vector length does not match the operator */
+    RTM_ERR_OOM_BUDGET = 3, /* the HBM budget (rtm_budget_configure) or the device refuses the bytes */
+    RTM_ERR_CUDA = 4,       /* a CUDA call failed */
+    RTM_ERR_TIMEOUT = 5,    /* a bounded wait ran out */
+    RTM_ERR_SINGULAR = 6,   /* the circulant approximation is singular at some frequency */
+    RTM_ERR_UNSUPPORTED = 7 /* size or option outside what this build supports */
+} rtm_status;
+
+typedef enum rtm_content { RTM_NONE = 0, RTM_XONLY = 1, RTM_YONLY = 2, RTM_BOTH = 3 } rtm_content;
+typedef enum rtm_product { RTM_PRODUCT_FFT = 0, RTM_PRODUCT_SPLIT = 1, RTM_PRODUCT_LEAN = 2 } rtm_product;
+typedef enum rtm_precision { RTM_FP64 = 0, RTM_FP32 = 1 } rtm_precision;
+typedef enum rtm_where { RTM_HOST = 0, RTM_DEVICE = 1 } rtm_where;
+typedef enum rtm_modifier { RTM_MODIFY_NONE = 0, RTM_MODIFY_REAL = 1, RTM_MODIFY_IMAG = 2 } rtm_modifier;
+typedef enum rtm_kernel {
+    RTM_KERNEL_STRANG = 0, RTM_KERNEL_TCHAN = 1, RTM_KERNEL_RCHAN = 2, RTM_KERNEL_HUCKLE = 3,
+    RTM_KERNEL_SUPEROPTIMAL = 4
+} rtm_kernel;
+typedef enum rtm_builder { RTM_BUILDER_PARTWISE = 0, RTM_BUILDER_BLOCKWISE = 1, RTM_BUILDER_HYBRID = 2 } rtm_builder;
+typedef enum rtm_method { RTM_METHOD_CG = 0, RTM_METHOD_GMRES = 1, RTM_METHOD_FGMRES_IR = 2 } rtm_method;
+
+typedef struct rtm_generators rtm_generators;
+typedef struct rtm_operator rtm_operator;
+typedef struct rtm_preconditioner rtm_preconditioner;
+
+/* Library ------------------------------------------------------------------------------------ */
+
+/* Package version of the reference this build follows (src/+rooftopMoM/version.m:7, '3.5.0'). */
+RTM_API int rtm_version(int* major, int* minor, int* patch);
+
+/* Copies the message of the last failed call of this thread into buf (always NUL-terminated). */
+RTM_API int rtm_last_error(char* buf, size_t len);
+
+/* Selects the CUDA device of the calling thread for the handles it creates next. */
+RTM_API int rtm_set_device(int device);
+
+/* Number of launches of this library's own kernels since load (a counter for benchmarks). */
+RTM_API int rtm_launch_count(int64_t* count);
+
+/* Budget ------------------------------------------------------------------------------------- */
+/* The HBM admission ledger; replaces src/+rooftopMoM/+resources/Budget.m:43-106 for device memory.
+ * ceiling_bytes <= 0 means no ceiling (device free memory still applies). */
+RTM_API int rtm_budget_configure(double ceiling_bytes);
+RTM_API int rtm_budget_query(double* ceiling_bytes, double* held_bytes);
+/* Fails with RTM_ERR_OOM_BUDGET if bytes do not fit below the ceiling and the device's free memory
+ * (Budget.require, Budget.m:82-106). */
+RTM_API int rtm_budget_require(double bytes);
+
+/* Byte models of every stage before it is built (src/+rooftopMoM/+resources/estimate*.m).
+ * out[0] generators, out[1] product spectra, out[2] product working, out[3] preconditioner
+ * spectra, out[4] preconditioner working, out[5] solver vectors. */
+RTM_API int rtm_estimate_bytes(int count_x, int count_y, int product, int method, int preconditioned, int restart,
+                       int max_iterations, double out[6]);
+
+/* Generators (Problem.generators / MomentAssembler.generate) ---------------------------------- */
+
+/* Assembles the generators on the device (replaces
+ * src/+rooftopMoM/+assembler/+greensMatrix/@MomentAssembler/generate.m:10-59): near pairs with the
+ * order near_order, far pairs on the shared lattice with far_order, touching pairs by singularity
+ * extraction with closed-form moments in FP64. */
+RTM_API int rtm_generators_assemble(int count_x, int count_y, double size_x, double size_y, double wavenumber,
+                            int near_order, int far_order, void* stream, rtm_generators** out);
+
+/* Wraps given generators (e.g. the reference's stored ones; Generators.m:16-21). Pointers may be
+ * NULL for a missing direction. */
+RTM_API int rtm_generators_create(int count_x, int count_y, const double* magnetic_xx, const double* magnetic_yy,
+                          const double* electric, int where, rtm_generators** out);
+
+/* Applies @real / @imag to every generator into a new handle (Generators.modify, Generators.m:25-37). */
+RTM_API int rtm_generators_modify(const rtm_generators* g, int modifier, rtm_generators** out);
+
+/* Copies the generators out; any pointer may be NULL. */
+RTM_API int rtm_generators_read(const rtm_generators* g, double* magnetic_xx, double* magnetic_yy, double* electric,
+                        int where);
+RTM_API int rtm_generators_info(const rtm_generators* g, int* count_x, int* count_y, int* content);
+RTM_API int rtm_generators_destroy(rtm_generators* g);
+
+/* Operator (Operator.m:7-54, Applicator.apply) ----------------------------------------------- */
+
+/* Builds the spectra on the device and the product of the kind 'fft' (circulant embedding,
+ * generateEmbeddingSpectra.m), 'splitFFT' (subbands, generateSubbandSpectra.m) or 'leanSplitFFT'
+ * (same spectra, half the working grid). max_rhs bounds the number of right-hand sides of one
+ * rtm_operator_apply. */
+RTM_API int rtm_operator_create(const rtm_generators* g, double size_x, double size_y, int product, int precision,
+                        int max_rhs, rtm_operator** out);
+
+/* y = A x for nrhs vectors of length n, stored one after another (replaces Applicator.apply,
+ * src/+rooftopMoM/+assembler/+greensMatrix/@SplitFFTApplicator/apply.m:10-20 and
+ * FFTApplicator.m:14-32). For an FP64 operator x, y are complex doubles; for an FP32 operator they
+ * are complex floats when where == RTM_DEVICE and complex doubles (converted) when RTM_HOST. */
+RTM_API int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int nrhs, int where, void* stream);
+
+/* A dense n x n complex operator (column-major), for solving any small system with the same solvers
+ * (the matrix operator of IterativeMethod.solve, convertToHandle.m:10-16). */
+RTM_API int rtm_operator_create_dense(const double* matrix, int64_t n, int where, rtm_operator** out);
+
+/* Spectra bytes held and the grid of the transforms. */
+RTM_API int rtm_operator_info(const rtm_operator* op, int64_t* n, int* fft_x, int* fft_y, double* spectra_bytes,
+                      double* working_bytes);
+/* Copies the stored spectra out (complex doubles): count blocks of fft_x*fft_y each, in the order
+ * subband-major, then E, MXX, MYY (split / fft products). Returns the block count in *count. */
+RTM_API int rtm_operator_read_spectra(const rtm_operator* op, double* out, int* count);
+RTM_API int rtm_operator_destroy(rtm_operator* op);
+
+/* Preconditioner (Preconditioner.m:7-70) ------------------------------------------------------ */
+
+/* Circulant preconditioner on the face grid: kernel (strang, tChan, rChan, huckle, superoptimal) x
+ * builder (partwise, blockwise, hybrid) (generateCirculant.m:16-25). bandwidth may be NULL (whole
+ * grid). Fails with RTM_ERR_SINGULAR when the approximation is singular (Preconditioner.m:60-67). */
+RTM_API int rtm_preconditioner_create(const rtm_generators* g, double size_x, double size_y, int kernel, int builder,
+                              const int* bandwidth, int precision, rtm_preconditioner** out);
+
+/* Block-Jacobi preconditioner with blocks of block_x x block_y faces (the rooftops whose first face
+ * lies in a block). Each block of the Green's matrix is formed from the generators and inverted on
+ * the device. Not in the reference. */
+RTM_API int rtm_preconditioner_create_block_jacobi(const rtm_generators* g, double size_x, double size_y, int block_x,
+                                           int block_y, int precision, rtm_preconditioner** out);
+
+RTM_API int rtm_preconditioner_apply(rtm_preconditioner* pc, const void* x, void* y, int64_t n, int nrhs, int where,
+                             void* stream);
+RTM_API int rtm_preconditioner_destroy(rtm_preconditioner* pc);
+
+/* Solve (Solver.solve / IterativeMethod.solve) ------------------------------------------------ */
+
+typedef struct rtm_solve_config {
+    int method;            /* RTM_METHOD_CG (COCG), RTM_METHOD_GMRES, RTM_METHOD_FGMRES_IR */
+    double tolerance;      /* relative residual to stop at (Solver.m:29, default 1e-6) */
+    int max_iterations;    /* Solver.m:30, default 1000 */
+    int restart;           /* GMRES cycle length (Solver.m:31, default 50); FGMRES inner cycle */
+    double inner_tolerance;/* FGMRES_IR: relative residual of one FP32 inner solve */
+    int max_refinements;   /* FGMRES_IR: bound on the FP64 outer refinement steps */
+    int check_every;       /* iterations between host convergence checks (0: library default) */
+} rtm_solve_config;
+
+typedef struct rtm_solve_stats {
+    int converged;         /* Output.converged */
+    int iteration_count;   /* Output.iterationCount (inner iterations for FGMRES_IR) */
+    double residual_norm;  /* Output.residualNorm, the true relative residual in FP64 */
+    double time_s;         /* Output.time, device time of the whole solve */
+    int refinements;       /* FGMRES_IR outer steps */
+    int matvecs;           /* products applied */
+} rtm_solve_stats;
+
+/* Solves op * x = b for nrhs right-hand sides of length n (replaces IterativeMethod.solve,
+ * src/+rooftopMoM/+solver/IterativeMethod.m:27-70, with ConjugateGradient.iterate_,
+ * PreconditionedConjugateGradient.precondition_ and GeneralizedMinimumResidual.iterate_).
+ * pc may be NULL; x0 may be NULL (zeros). history may be NULL, otherwise it receives
+ * nrhs x (max_iterations+1) relative residuals (NaN after the last iteration). stats has nrhs
+ * entries. The FP64 operator gives the true residual; FGMRES_IR needs op FP64 and uses inner_op
+ * (FP32) and inner_pc for the inner solves. */
+RTM_API int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_config* config, const void* b,
+              const void* x0, void* x, int64_t n, int nrhs, int where, double* history, rtm_solve_stats* stats,
+              void* stream);
+RTM_API int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner* inner_pc,
+                    const rtm_solve_config* config, const void* b, const void* x0, void* x, int64_t n, int nrhs,
+                    int where, double* history, rtm_solve_stats* stats, void* stream);
+
+/* Excitation and results (src/+rooftopMoM/+operator) ------------------------------------------ */
+
+/* generatePlaneWave.m:18-42 on the device, for nrhs waves: direction and polarization are 3*nrhs
+ * unit vectors, intensity nrhs values. order is the far quadrature order of the rooftops. */
+RTM_API int rtm_plane_wave(int count_x, int count_y, double size_x, double size_y, int order, double wavenumber,
+                   const double* directions, const double* polarizations, const double* intensities, int nrhs,
+                   void* out, int where, void* stream);
+
+/* generateDeltaGap.m:13-14 with generateMiddlePort.m:14-28 (port of the given direction, 'x' = 0 or
+ * 'y' = 1) or an explicit 0-based port. */
+RTM_API int rtm_delta_gap(int count_x, int count_y, double size_x, double size_y, const int64_t* port, int port_count,
+                  int direction, double voltage, void* out, int where);
+
+/* computeRadarCrossSection.m:18-19 and computeInputImpedance.m:17 (current on host or device). */
+RTM_API int rtm_radar_cross_section(double wavenumber, const void* excitation, const void* current, int64_t n,
+                            double intensity, int where, double* out);
+RTM_API int rtm_input_impedance(int count_x, int count_y, double size_x, double size_y, const void* current,
+                        const int64_t* port, int port_count, double voltage, int where, double* out);
+/* (out of rtm_input_impedance: out[0] + i out[1], the complex input impedance in ohms) */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTM_H */

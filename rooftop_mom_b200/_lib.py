@@ -1,0 +1,140 @@
+"""ctypes binding of librtm.so (the C ABI declared in include/rtm.h).
+
+Loading needs no GPU; every compute call does. There is no CPU fallback: if the library is missing
+or a call fails, an RtmError is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("RTM_LIBRARY", os.path.join(HERE, "librtm.so"))
+
+OK, ERR_ARG, ERR_SIZE, ERR_OOM_BUDGET, ERR_CUDA, ERR_TIMEOUT, ERR_SINGULAR, ERR_UNSUPPORTED = range(8)
+XONLY, YONLY, BOTH = 1, 2, 3
+PRODUCTS = {"fft": 0, "splitFFT": 1, "leanSplitFFT": 2}
+PRECISIONS = {"double": 0, "single": 1}
+HOST, DEVICE = 0, 1
+MODIFIERS = {None: 0, "real": 1, "imag": 2}
+KERNELS = {"strang": 0, "tChan": 1, "rChan": 2, "huckle": 3, "superoptimal": 4}
+BUILDERS = {"partwise": 0, "blockwise": 1, "hybrid": 2}
+METHODS = {"cg": 0, "gmres": 1, "fgmres": 2}
+
+# Error identifiers of the reference (src/+rooftopMoM/*.m) for the statuses that have one.
+_IDS = {
+    ERR_ARG: "rooftopMoM:gpu:invalidArgument",
+    ERR_SIZE: "rooftopMoM:product:sizeMismatch",
+    ERR_OOM_BUDGET: "rooftopMoM:resources:insufficientMemory",
+    ERR_CUDA: "rooftopMoM:gpu:cuda",
+    ERR_TIMEOUT: "rooftopMoM:gpu:timeout",
+    ERR_SINGULAR: "rooftopMoM:preconditioner:singular",
+    ERR_UNSUPPORTED: "rooftopMoM:gpu:unsupported",
+}
+
+
+class RtmError(RuntimeError):
+    """A failed librtm call; ``identifier`` follows the reference's error IDs."""
+
+    def __init__(self, status: int, message: str, identifier: str | None = None):
+        self.status = status
+        self.identifier = identifier or _IDS.get(status, "rooftopMoM:gpu:error")
+        super().__init__(f"{self.identifier}: {message}")
+
+
+class SolveConfig(C.Structure):
+    _fields_ = [("method", C.c_int), ("tolerance", C.c_double), ("max_iterations", C.c_int),
+                ("restart", C.c_int), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int),
+                ("check_every", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iteration_count", C.c_int), ("residual_norm", C.c_double),
+                ("time_s", C.c_double), ("refinements", C.c_int), ("matvecs", C.c_int)]
+
+
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+_SIGNATURES = {
+    "rtm_version": [C.POINTER(C.c_int)] * 3,
+    "rtm_last_error": [C.c_char_p, C.c_size_t],
+    "rtm_set_device": [C.c_int],
+    "rtm_launch_count": [C.POINTER(C.c_int64)],
+    "rtm_budget_configure": [C.c_double],
+    "rtm_budget_query": [C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    "rtm_budget_require": [C.c_double],
+    "rtm_estimate_bytes": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)],
+    "rtm_generators_assemble": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _P, _PP],
+    "rtm_generators_create": [C.c_int, C.c_int, _P, _P, _P, C.c_int, _PP],
+    "rtm_generators_modify": [_P, C.c_int, _PP],
+    "rtm_generators_read": [_P, _P, _P, _P, C.c_int],
+    "rtm_generators_info": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "rtm_generators_destroy": [_P],
+    "rtm_operator_create": [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _PP],
+    "rtm_operator_apply": [_P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
+    "rtm_operator_create_dense": [_P, C.c_int64, C.c_int, _PP],
+    "rtm_operator_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                          C.POINTER(C.c_double)],
+    "rtm_operator_read_spectra": [_P, _P, C.POINTER(C.c_int)],
+    "rtm_operator_destroy": [_P],
+    "rtm_preconditioner_create": [_P, C.c_double, C.c_double, C.c_int, C.c_int, _P, C.c_int, _PP],
+    "rtm_preconditioner_create_block_jacobi": [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _PP],
+    "rtm_preconditioner_apply": [_P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
+    "rtm_preconditioner_destroy": [_P],
+    "rtm_solve": [_P, _P, C.POINTER(SolveConfig), _P, _P, _P, C.c_int64, C.c_int, C.c_int, _P, C.POINTER(SolveStats),
+                  _P],
+    "rtm_solve_mixed": [_P, _P, _P, C.POINTER(SolveConfig), _P, _P, _P, C.c_int64, C.c_int, C.c_int, _P,
+                        C.POINTER(SolveStats), _P],
+    "rtm_plane_wave": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double, _P, _P, _P, C.c_int, _P,
+                       C.c_int, _P],
+    "rtm_delta_gap": [C.c_int, C.c_int, C.c_double, C.c_double, _P, C.c_int, C.c_int, C.c_double, _P, C.c_int],
+    "rtm_radar_cross_section": [C.c_double, _P, _P, C.c_int64, C.c_double, C.c_int, C.POINTER(C.c_double)],
+    "rtm_input_impedance": [C.c_int, C.c_int, C.c_double, C.c_double, _P, _P, C.c_int, C.c_double, C.c_int,
+                            C.POINTER(C.c_double)],
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Returns the loaded library; raises RtmError if librtm.so is absent."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RtmError(ERR_UNSUPPORTED, f"{LIB_PATH} is missing; build it with "
+                                                "`python -m rooftop_mom_b200.build` (no CPU fallback exists)")
+            lib = C.CDLL(LIB_PATH)
+            for name, args in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = args
+                fn.restype = C.c_int
+            _lib = lib
+        return _lib
+
+
+def exported_symbols():
+    return list(_SIGNATURES)
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    load().rtm_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, identifier: str | None = None):
+    if status != OK:
+        raise RtmError(status, last_error(), identifier)
+
+
+def call(name: str, *args, identifier: str | None = None):
+    check(getattr(load(), name)(*args), identifier)
+
+
+def launch_count() -> int:
+    v = C.c_int64()
+    call("rtm_launch_count", C.byref(v))
+    return v.value

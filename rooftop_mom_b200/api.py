@@ -1,0 +1,644 @@
+"""Host-side mirror of the reference's MATLAB API for the solve path, over the C ABI.
+
+The classes keep the names, arguments and error identifiers of src/+rooftopMoM/{Mesh,Problem,
+Operator,Preconditioner,Solver,Excitation,Result,Resources}.m; their bodies call librtm.so, which
+assembles, transforms and solves on the GPU. Vectors are numpy arrays (host) or CUDA torch tensors
+(device, complex128, or complex64 for single-precision products).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import RtmError
+
+Z0 = 376.730313668  # src/+rooftopMoM/+assembler/Constants.m:11
+SPEED_OF_LIGHT = 299792458.0  # Constants.m:8
+
+
+def _err(identifier: str, message: str):
+    return RtmError(L.ERR_ARG, message, identifier)
+
+
+def _is_device(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _vec_in(x, n: int, dtype=np.complex128):
+    """(pointer, where, keepalive) of a vector argument of n * nrhs complex entries."""
+    if _is_device(x):
+        if not x.is_contiguous():
+            x = x.contiguous()
+        return C.c_void_p(x.data_ptr()), L.DEVICE, x
+    a = np.ascontiguousarray(np.asarray(x, dtype=dtype))
+    return a.ctypes.data_as(C.c_void_p), L.HOST, a
+
+
+def fast_fft_size(count: int) -> int:
+    """generateFastFFTSize.m:11-15."""
+    n = int(count)
+    while True:
+        m = n
+        for p in (2, 3, 5, 7):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            return n
+        n += 1
+
+
+class Mesh:
+    """src/+rooftopMoM/Mesh.m: countX x countY faces of sizeX x sizeY in the plane z = 0."""
+
+    def __init__(self, countX: int, countY: int, sizeX: float, sizeY: float):
+        for v, name in ((countX, "countX"), (countY, "countY")):
+            if int(v) != v or v < 1:
+                raise _err("rooftopMoM:mesh:invalidCount", f"{name} must be a positive integer.")
+        for v in (sizeX, sizeY):
+            if not (math.isfinite(v) and v > 0):
+                raise _err("rooftopMoM:mesh:invalidSize", "The face sizes must be positive and finite.")
+        if countX == 1 and countY == 1:
+            raise _err("rooftopMoM:mesh:noRooftops",
+                       "A single face has no interior edge, so it carries no rooftop.")
+        self._c = (int(countX), int(countY))
+        self._s = (float(sizeX), float(sizeY))
+
+    def count(self):
+        return self._c
+
+    def faceSize(self):
+        return self._s
+
+    def radius(self) -> float:
+        return math.hypot(self._c[0] * self._s[0], self._c[1] * self._s[1]) / 2
+
+    # rooftop layout (UniformRooftops.m:31-55)
+    def gridSize(self, direction: str):
+        cx, cy = self._c
+        return (cx - 1, cy) if direction == "x" else (cx, cy - 1)
+
+    def rooftopCount(self) -> int:
+        (a, b), (c, d) = self.gridSize("x"), self.gridSize("y")
+        return a * b + c * d
+
+
+class Generators:
+    """Generators.m: the three Toeplitz generators, held on the device."""
+
+    def __init__(self, handle, mesh: Mesh):
+        self._h = handle
+        self._mesh = mesh
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            L.load().rtm_generators_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def modify(self, modifier):
+        """Generators.modify with 'real' / 'imag' (or np.real / np.imag)."""
+        key = {np.real: "real", np.imag: "imag"}.get(modifier, modifier)
+        if key not in L.MODIFIERS:
+            raise _err("rooftopMoM:operator:invalidModifier", "The modifier is 'real', 'imag' or None.")
+        out = C.c_void_p()
+        L.call("rtm_generators_modify", self._h, L.MODIFIERS[key], C.byref(out))
+        return Generators(out, self._mesh)
+
+    def arrays(self):
+        """(magneticXX, magneticYY, electric) as numpy arrays [x, y]; None for a missing direction."""
+        cx, cy = self._mesh.count()
+        xx = np.zeros((cx - 1) * cy, np.complex128)
+        yy = np.zeros(cx * (cy - 1), np.complex128)
+        e = np.zeros(cx * cy, np.complex128)
+        L.call("rtm_generators_read", self._h, xx.ctypes.data_as(C.c_void_p) if xx.size else None,
+               yy.ctypes.data_as(C.c_void_p) if yy.size else None, e.ctypes.data_as(C.c_void_p), L.HOST)
+        f = lambda v, r, c: v.reshape(r, c, order="F") if v.size else None
+        return f(xx, cx - 1, cy), f(yy, cx, cy - 1), e.reshape(cx, cy, order="F")
+
+    def magneticXX(self):
+        return self.arrays()[0]
+
+    def magneticYY(self):
+        return self.arrays()[1]
+
+    def electric(self):
+        return self.arrays()[2]
+
+    @staticmethod
+    def fromArrays(mesh: Mesh, magneticXX, magneticYY, electric):
+        """Wraps given generators (the reference's Generators constructor)."""
+        cx, cy = mesh.count()
+        ptr = lambda a: (np.ascontiguousarray(np.asarray(a, np.complex128).ravel(order="F"))
+                         if a is not None and np.size(a) else None)
+        xx, yy, e = ptr(magneticXX), ptr(magneticYY), ptr(electric)
+        out = C.c_void_p()
+        L.call("rtm_generators_create", cx, cy, xx.ctypes.data_as(C.c_void_p) if xx is not None else None,
+               yy.ctypes.data_as(C.c_void_p) if yy is not None else None, e.ctypes.data_as(C.c_void_p), L.HOST,
+               C.byref(out))
+        return Generators(out, mesh)
+
+
+class Problem:
+    """src/+rooftopMoM/Problem.m: the EFIE of a Mesh at one wavenumber; generators assembled lazily."""
+
+    minimumDensity = 10
+
+    def __init__(self, mesh: Mesh, wavenumber=None, electricalSize=None, quadratureOrder=(16, 8), chunkSize=None):
+        if (wavenumber is None) == (electricalSize is None):
+            raise _err("rooftopMoM:problem:invalidWavenumber",
+                       "A problem takes either the wavenumber or the 'electricalSize', not both or neither.")
+        if wavenumber is None:
+            wavenumber = electricalSize / mesh.radius()
+        if not (math.isfinite(wavenumber) and wavenumber > 0):
+            raise _err("rooftopMoM:problem:invalidWavenumber", "The wavenumber must be positive and finite.")
+        orders = np.atleast_1d(np.asarray(quadratureOrder))
+        if orders.size not in (1, 2):
+            raise _err("rooftopMoM:problem:invalidQuadratureOrder",
+                       "The quadrature order is one order or a pair [near, far].")
+        self._mesh = mesh
+        self._k = float(wavenumber)
+        self._orders = (int(orders[0]), int(orders[-1]))
+        self._generators = None
+
+    @staticmethod
+    def fromElectricalSize(electricalSize, density=10, aspect=1, quadratureOrder=(16, 8), chunkSize=None):
+        """Problem.m:159-206: the fewest faces reaching the density, rounded up to 7-smooth counts, k = 2 pi."""
+        sides = np.array([aspect, 1.0]) * (electricalSize / math.pi) / math.hypot(aspect, 1.0)
+        counts = np.maximum(1, np.ceil((1 - 4 * np.finfo(float).eps) * sides * density)).astype(int)
+        counts = [fast_fft_size(c) for c in counts]
+        if counts == [1, 1]:
+            raise _err("rooftopMoM:problem:singleFace", "The plate is a single face, which carries no rooftop.")
+        mesh = Mesh(counts[0], counts[1], sides[0] / counts[0], sides[1] / counts[1])
+        return Problem(mesh, 2 * math.pi, quadratureOrder=quadratureOrder)
+
+    def mesh(self):
+        return self._mesh
+
+    def wavenumber(self):
+        return self._k
+
+    def electricalSize(self):
+        return self._k * self._mesh.radius()
+
+    def density(self):
+        return 2 * math.pi / (self._k * max(self._mesh.faceSize()))
+
+    def rooftopCount(self):
+        return self._mesh.rooftopCount()
+
+    def quadratureOrder(self):
+        return self._orders
+
+    def generators(self) -> Generators:
+        """Problem.generators: assembled on the first call, on the GPU."""
+        if self._generators is None:
+            cx, cy = self._mesh.count()
+            a, b = self._mesh.faceSize()
+            out = C.c_void_p()
+            L.call("rtm_generators_assemble", cx, cy, a, b, self._k, self._orders[0], self._orders[1], None,
+                   C.byref(out))
+            self._generators = Generators(out, self._mesh)
+        return self._generators
+
+    def setGenerators(self, generators: Generators):
+        """Uses given generators instead of assembling them (e.g. the reference's stored ones)."""
+        self._generators = generators
+
+
+class _Product:
+    """Product.m: apply with the size check of the reference."""
+
+    _handle = None
+    _destroy = None
+    _apply_fn = None
+
+    def __del__(self):
+        if self._handle:
+            getattr(L.load(), self._destroy)(self._handle)
+            self._handle = None
+
+    def apply(self, x, nrhs: int = 1):
+        n = self._n
+        if _is_device(x):
+            total = x.numel()
+        else:
+            total = np.size(x)
+        if total != n * nrhs:
+            raise RtmError(L.ERR_SIZE, f"The input must be a numeric {n}x1 vector.", "rooftopMoM:product:sizeMismatch")
+        if _is_device(x):
+            import torch
+            y = torch.empty_like(x)
+            xp, where, keep = _vec_in(x, n)
+            L.call(self._apply_fn, self._handle, xp, C.c_void_p(y.data_ptr()), n, nrhs, where, None)
+            return y
+        xp, where, keep = _vec_in(x, n)
+        y = np.empty(n * nrhs, np.complex128)
+        L.call(self._apply_fn, self._handle, xp, y.ctypes.data_as(C.c_void_p), n, nrhs, where, None)
+        return y if nrhs > 1 else y.reshape(np.shape(x)) if np.ndim(x) else y
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def rooftopCount(self):
+        return self._n
+
+
+class Operator(_Product):
+    """src/+rooftopMoM/Operator.m: the matrix-free product with the Green's matrix.
+
+    product: 'fft' | 'splitFFT' (default) | 'leanSplitFFT'; modifier: None | 'real' | 'imag';
+    precision: 'double' (default) | 'single' (complex FP32 spectra and transforms).
+    """
+
+    _destroy = "rtm_operator_destroy"
+    _apply_fn = "rtm_operator_apply"
+
+    def __init__(self, problem: Problem, product="splitFFT", modifier=None, precision="double", maxRhs=1):
+        if product not in L.PRODUCTS:
+            raise _err("rooftopMoM:operator:invalidProduct", "The product is 'fft', 'splitFFT' or 'leanSplitFFT'.")
+        if precision not in L.PRECISIONS:
+            raise _err("rooftopMoM:operator:invalidPrecision", "The precision is 'double' or 'single'.")
+        gen = problem.generators()
+        if modifier is not None:
+            gen = gen.modify(modifier)
+        a, b = problem.mesh().faceSize()
+        out = C.c_void_p()
+        L.call("rtm_operator_create", gen.handle, a, b, L.PRODUCTS[product], L.PRECISIONS[precision], int(maxRhs),
+               C.byref(out))
+        self._handle = out
+        self._problem = problem
+        self._n = problem.rooftopCount()
+        self.product = product
+        self.precision = precision
+
+    def problem(self):
+        return self._problem
+
+    def info(self):
+        n = C.c_int64()
+        px, py = C.c_int(), C.c_int()
+        sb, wb = C.c_double(), C.c_double()
+        L.call("rtm_operator_info", self._handle, C.byref(n), C.byref(px), C.byref(py), C.byref(sb), C.byref(wb))
+        return {"n": n.value, "fft_x": px.value, "fft_y": py.value, "spectra_bytes": sb.value,
+                "working_bytes": wb.value}
+
+    def memory(self):
+        return self.info()["spectra_bytes"]
+
+    def spectra(self):
+        """The stored spectra as numpy arrays [block][x, y]."""
+        cnt = C.c_int()
+        L.call("rtm_operator_read_spectra", self._handle, None, C.byref(cnt))
+        inf = self.info()
+        P, Q = inf["fft_x"], inf["fft_y"]
+        buf = np.zeros(cnt.value * P * Q, np.complex128)
+        L.call("rtm_operator_read_spectra", self._handle, buf.ctypes.data_as(C.c_void_p), C.byref(cnt))
+        return buf.reshape(cnt.value, Q, P).transpose(0, 2, 1)
+
+
+class DenseOperator(_Product):
+    """A dense complex matrix as an operator of the solvers (IterativeMethod accepts matrices)."""
+
+    _destroy = "rtm_operator_destroy"
+    _apply_fn = "rtm_operator_apply"
+
+    def __init__(self, matrix):
+        A = np.asfortranarray(np.asarray(matrix, np.complex128))
+        if A.ndim != 2 or A.shape[0] != A.shape[1]:
+            raise _err("rooftopMoM:solver:invalidOperator", "An operator matrix is square.")
+        out = C.c_void_p()
+        L.call("rtm_operator_create_dense", A.ctypes.data_as(C.c_void_p), A.shape[0], L.HOST, C.byref(out))
+        self._handle = out
+        self._n = A.shape[0]
+        self.precision = "double"
+
+
+class Preconditioner(_Product):
+    """src/+rooftopMoM/Preconditioner.m: circulant preconditioner (inverse of a block-circulant approximation).
+
+    kernel: 'strang' | 'tChan' | 'rChan' (default) | 'huckle' | 'superoptimal';
+    builder: 'partwise' (default) | 'blockwise' | 'hybrid'.
+    """
+
+    _destroy = "rtm_preconditioner_destroy"
+    _apply_fn = "rtm_preconditioner_apply"
+
+    def __init__(self, problem: Problem, kernel="rChan", builder="partwise", bandwidth=None, modifier=None,
+                 precision="double"):
+        if kernel not in L.KERNELS:
+            raise _err("rooftopMoM:preconditioner:invalidKernel",
+                       "The kernel is 'strang', 'tChan', 'rChan', 'huckle' or 'superoptimal'.")
+        if builder not in L.BUILDERS:
+            raise _err("rooftopMoM:preconditioner:invalidBuilder", "The builder is 'partwise', 'blockwise' or 'hybrid'.")
+        bw = None
+        if bandwidth is not None:
+            if np.size(bandwidth) != 2:
+                raise _err("rooftopMoM:preconditioner:invalidBandwidth",
+                           "The bandwidth is a pair [bandwidthX, bandwidthY].")
+            bw = (C.c_int * 2)(int(bandwidth[0]), int(bandwidth[1]))
+        gen = problem.generators()
+        if modifier is not None:
+            gen = gen.modify(modifier)
+        a, b = problem.mesh().faceSize()
+        out = C.c_void_p()
+        L.call("rtm_preconditioner_create", gen.handle, a, b, L.KERNELS[kernel], L.BUILDERS[builder],
+               C.cast(bw, C.c_void_p) if bw is not None else None, L.PRECISIONS[precision], C.byref(out))
+        self._handle = out
+        self._problem = problem
+        self._n = problem.rooftopCount()
+        self.precision = precision
+
+    @classmethod
+    def blockJacobi(cls, problem: Problem, block=(2, 2), precision="double"):
+        """Block-Jacobi over blocks of block[0] x block[1] faces (not in the reference)."""
+        self = cls.__new__(cls)
+        gen = problem.generators()
+        a, b = problem.mesh().faceSize()
+        out = C.c_void_p()
+        L.call("rtm_preconditioner_create_block_jacobi", gen.handle, a, b, int(block[0]), int(block[1]),
+               L.PRECISIONS[precision], C.byref(out))
+        self._handle = out
+        self._problem = problem
+        self._n = problem.rooftopCount()
+        self.precision = precision
+        return self
+
+    def problem(self):
+        return self._problem
+
+
+@dataclass
+class _Params:
+    type: str
+    data: dict
+
+
+class Excitation:
+    """src/+rooftopMoM/Excitation.m: plane wave or delta gap, generated on the device."""
+
+    def __init__(self, problem, type_, vector, params):
+        self._problem = problem
+        self._type = type_
+        self._vector = vector
+        self._params = params
+
+    @staticmethod
+    def _normalize(v, name):
+        v = np.asarray(v, np.float64).reshape(3)
+        if not np.any(v):
+            raise _err("rooftopMoM:excitation:zeroVector", f"The {name} must not be zero.")
+        return v / np.linalg.norm(v)
+
+    @classmethod
+    def planeWave(cls, problem: Problem, direction=(0, 0, -1), polarization=(1, 0, 0), intensity=1.0):
+        d = cls._normalize(direction, "direction")
+        p = cls._normalize(polarization, "polarization")
+        dot = float(d @ p)
+        if abs(dot) > 10 * np.finfo(float).eps:
+            raise _err("rooftopMoM:excitation:notPerpendicular",
+                       f"The polarization must be perpendicular to the direction of propagation, their dot product "
+                       f"is {dot:.1e}.")
+        cx, cy = problem.mesh().count()
+        a, b = problem.mesh().faceSize()
+        n = problem.rooftopCount()
+        out = np.zeros(n, np.complex128)
+        inten = np.array([float(intensity)])
+        L.call("rtm_plane_wave", cx, cy, a, b, problem.quadratureOrder()[1], problem.wavenumber(),
+               d.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p), inten.ctypes.data_as(C.c_void_p), 1,
+               out.ctypes.data_as(C.c_void_p), L.HOST, None)
+        return cls(problem, "planeWave", out, {"direction": d, "polarization": p, "intensity": float(intensity)})
+
+    @classmethod
+    def deltaGap(cls, problem: Problem, port=None, direction="x", voltage=1.0):
+        """port: 0-based rooftop indices (default: the middle line of edges of the direction)."""
+        cx, cy = problem.mesh().count()
+        a, b = problem.mesh().faceSize()
+        n = problem.rooftopCount()
+        out = np.zeros(n, np.complex128)
+        if port is None:
+            if problem.mesh().gridSize(direction)[0] * problem.mesh().gridSize(direction)[1] == 0:
+                raise _err("rooftopMoM:excitation:noRooftops", f"The mesh has no {direction}-directed rooftops.")
+            pp = None
+            cnt = 0
+        else:
+            pp = np.ascontiguousarray(np.asarray(port, np.int64).ravel())
+            if np.any(pp >= n) or np.any(pp < 0) or np.unique(pp).size < pp.size:
+                raise _err("rooftopMoM:excitation:invalidPort",
+                           f"The port must hold distinct rooftop indices up to {n}.")
+            cnt = pp.size
+        L.call("rtm_delta_gap", cx, cy, a, b, pp.ctypes.data_as(C.c_void_p) if pp is not None else None, cnt,
+               0 if direction == "x" else 1, float(voltage), out.ctypes.data_as(C.c_void_p), L.HOST)
+        if port is None:
+            pp = np.flatnonzero(out)
+        return cls(problem, "deltaGap", out, {"port": pp, "voltage": float(voltage)})
+
+    def problem(self):
+        return self._problem
+
+    def type(self):
+        return self._type
+
+    def vector(self):
+        return self._vector
+
+    def parameters(self):
+        return self._params
+
+
+class Result:
+    """src/+rooftopMoM/Result.m."""
+
+    def __init__(self, solution, stats, history, excitation=None, inner_iterations=None):
+        self._x = solution
+        self._stats = stats
+        self._history = history
+        self._excitation = excitation
+
+    def solution(self):
+        return self._x
+
+    def converged(self):
+        return bool(self._stats.converged)
+
+    def iterationCount(self):
+        return int(self._stats.iteration_count)
+
+    def residualNorms(self):
+        h = self._history
+        return h[: np.count_nonzero(~np.isnan(h))]
+
+    def residualNorm(self):
+        return float(self._stats.residual_norm)
+
+    def time(self):
+        return float(self._stats.time_s)
+
+    def refinements(self):
+        return int(self._stats.refinements)
+
+    def excitation(self):
+        return self._excitation
+
+    def _parameters(self, type_):
+        if self._excitation is None or self._excitation.type() != type_:
+            raise _err("rooftopMoM:result:wrongExcitation", f"This quantity needs a {type_} excitation.")
+        return self._excitation.parameters()
+
+    def inputImpedance(self):
+        p = self._parameters("deltaGap")
+        prob = self._excitation.problem()
+        cx, cy = prob.mesh().count()
+        a, b = prob.mesh().faceSize()
+        xp, where, keep = _vec_in(self._x, prob.rooftopCount())
+        port = np.ascontiguousarray(np.asarray(p["port"], np.int64))
+        out = (C.c_double * 2)()
+        L.call("rtm_input_impedance", cx, cy, a, b, xp, port.ctypes.data_as(C.c_void_p), port.size, p["voltage"],
+               where, out)
+        return complex(out[0], out[1])
+
+    def radarCrossSection(self):
+        p = self._parameters("planeWave")
+        prob = self._excitation.problem()
+        ev = np.ascontiguousarray(self._excitation.vector())
+        if _is_device(self._x):
+            import torch
+            e_t = torch.from_numpy(ev).to(self._x.device)
+            ep, where, keep1 = _vec_in(e_t, prob.rooftopCount())
+        else:
+            ep, where, keep1 = _vec_in(ev, prob.rooftopCount())
+        xp, where2, keep2 = _vec_in(self._x, prob.rooftopCount())
+        out = C.c_double()
+        L.call("rtm_radar_cross_section", prob.wavenumber(), ep, xp, prob.rooftopCount(), p["intensity"], where,
+               C.byref(out))
+        return out.value
+
+    def normalizedRadarCrossSection(self):
+        wavelength = 2 * math.pi / self._excitation.problem().wavenumber()
+        return self.radarCrossSection() / wavelength**2
+
+
+class Solver:
+    """src/+rooftopMoM/Solver.m: 'cg' (COCG) or 'gmres' (restarted GMRES), plus the GPU-only
+    precision form 'fgmres' (FP32 flexible GMRES inside FP64 iterative refinement)."""
+
+    def __init__(self, method="cg", tolerance=1e-6, maxIterationCount=1000, restart=50, innerTolerance=1e-4,
+                 maxRefinements=20, checkEvery=0, innerMethod="fgmres"):
+        if method not in ("cg", "gmres", "fgmres"):
+            raise _err("rooftopMoM:solver:invalidMethod", "The method is 'cg', 'gmres' or 'fgmres'.")
+        if not (0 < tolerance < 1):
+            raise _err("rooftopMoM:solver:invalidTolerance", "The tolerance lies in (0, 1).")
+        if int(maxIterationCount) != maxIterationCount or maxIterationCount < 1:
+            raise _err("rooftopMoM:solver:invalidMaxIterationCount", "maxIterationCount is a positive integer.")
+        if not (restart == math.inf or (int(restart) == restart and restart > 0)):
+            raise _err("rooftopMoM:solver:invalidRestart", "The restart is a positive integer or Inf.")
+        self.method = method
+        self.tolerance = float(tolerance)
+        self.maxIterationCount = int(maxIterationCount)
+        self.restart = int(min(restart, 1 << 30))
+        self.innerTolerance = innerTolerance
+        self.maxRefinements = maxRefinements
+        self.checkEvery = checkEvery
+        self.innerMethod = innerMethod
+
+    def _config(self, method_id):
+        return L.SolveConfig(method_id, self.tolerance, self.maxIterationCount, self.restart, self.innerTolerance,
+                             self.maxRefinements, self.checkEvery)
+
+    def solve(self, operator, rightHandSide, preconditioner=None, initialGuess=None, innerOperator=None,
+              innerPreconditioner=None, nrhs: int = 1):
+        excitation = None
+        if isinstance(rightHandSide, Excitation):
+            excitation = rightHandSide
+            b = rightHandSide.vector()
+        else:
+            b = rightHandSide
+            if not _is_device(b) and not np.all(np.isfinite(np.asarray(b))):
+                raise _err("rooftopMoM:solver:invalidRightHandSide",
+                           "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+        if isinstance(operator, np.ndarray):
+            operator = DenseOperator(operator)
+        if isinstance(preconditioner, np.ndarray):
+            preconditioner = DenseOperator(preconditioner)
+        count = (b.numel() if _is_device(b) else np.size(b)) // nrhs
+        if operator.rooftopCount() != count:
+            raise RtmError(L.ERR_SIZE, f"The operator does not match the {count} unknowns of the right-hand side.",
+                           "rooftopMoM:solver:sizeMismatch")
+        if preconditioner is not None and preconditioner.rooftopCount() != count:
+            raise RtmError(L.ERR_SIZE,
+                           f"The preconditioner does not match the {count} unknowns of the right-hand side.",
+                           "rooftopMoM:solver:sizeMismatch")
+        if initialGuess is not None and np.size(initialGuess) != count * nrhs and not _is_device(initialGuess):
+            raise RtmError(L.ERR_SIZE, f"The initial guess must have {count} elements.", "rooftopMoM:solver:sizeMismatch")
+        device = _is_device(b)
+        single = getattr(operator, "precision", "double") == "single"
+        dt = np.complex64 if (single and device) else np.complex128
+        bp, where, keep_b = _vec_in(b, count, dt)
+        x0p = None
+        keep_x0 = None
+        if initialGuess is not None:
+            x0p, _, keep_x0 = _vec_in(initialGuess, count, dt)
+        if device:
+            import torch
+            x = torch.empty_like(b)
+            xp = C.c_void_p(x.data_ptr())
+        else:
+            x = np.empty(count * nrhs, np.complex128)
+            xp = x.ctypes.data_as(C.c_void_p)
+        hist = np.full((nrhs, self.maxIterationCount + 1), np.nan)
+        stats = (L.SolveStats * nrhs)()
+        if self.method == "fgmres" or innerOperator is not None:
+            method_id = L.METHODS["cg"] if self.innerMethod == "cg" else L.METHODS["fgmres"]
+            if innerOperator is None:
+                raise _err("rooftopMoM:solver:missingInnerOperator", "The precision form needs an FP32 operator.")
+            cfg = self._config(method_id)
+            L.call("rtm_solve_mixed", operator.handle, innerOperator.handle,
+                   innerPreconditioner.handle if innerPreconditioner is not None else None, C.byref(cfg), bp, x0p, xp,
+                   count, nrhs, where, hist.ctypes.data_as(C.c_void_p), stats, None)
+        else:
+            cfg = self._config(L.METHODS[self.method])
+            L.call("rtm_solve", operator.handle, preconditioner.handle if preconditioner is not None else None,
+                   C.byref(cfg), bp, x0p, xp, count, nrhs, where, hist.ctypes.data_as(C.c_void_p), stats, None)
+        if nrhs == 1:
+            return Result(x, stats[0], hist[0], excitation)
+        return [Result(x[k * count:(k + 1) * count], stats[k], hist[k], excitation) for k in range(nrhs)]
+
+
+class Resources:
+    """src/+rooftopMoM/Resources.m for device memory: the HBM ceiling and the byte models."""
+
+    @staticmethod
+    def configure(memory=math.inf):
+        L.call("rtm_budget_configure", 0.0 if memory == math.inf else float(memory))
+
+    @staticmethod
+    def reset():
+        Resources.configure()
+
+    @staticmethod
+    def ceiling():
+        c, h = C.c_double(), C.c_double()
+        L.call("rtm_budget_query", C.byref(c), C.byref(h))
+        return math.inf if c.value <= 0 else c.value
+
+    @staticmethod
+    def held():
+        c, h = C.c_double(), C.c_double()
+        L.call("rtm_budget_query", C.byref(c), C.byref(h))
+        return h.value
+
+    @staticmethod
+    def estimate(mesh: Mesh, product="splitFFT", method="cg", preconditioner=True, restart=50, maxIterationCount=1000):
+        out = (C.c_double * 6)()
+        cx, cy = mesh.count()
+        L.call("rtm_estimate_bytes", cx, cy, L.PRODUCTS[product], L.METHODS[method], int(bool(preconditioner)),
+               int(restart), int(maxIterationCount), out)
+        keys = ("generators", "product", "productWorking", "preconditioner", "preconditionerWorking", "solver")
+        return dict(zip(keys, list(out)))

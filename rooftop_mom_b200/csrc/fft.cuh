@@ -1,0 +1,244 @@
+// Shared-memory mixed-radix FFT engine for sm_100a (device code only).
+//
+// A CTA transforms `lines` lines of length n that sit in shared memory; element e of line l is at
+// buf[l * ls + e * es]. The transform is a Stockham autosort FFT (natural order in and out): at a
+// stage of radix R after sub-transforms of length Ns, butterfly j reads the R elements
+// j + t n/R, twiddles them by w^(t k n/(Ns R)) with k = j mod Ns, applies a radix-R DFT and writes
+// them to (j - k) R + k + q Ns. Radices 2, 4, 8 and 16 are hand-written, 3, 5 and 7 read their
+// roots from the twiddle table, larger primes up to kMaxGenericRadix use a direct DFT.
+// Twiddles are w^m = exp(-2 pi i m / n) (table of n entries); the inverse uses their conjugates
+// and does not scale.
+#pragma once
+
+#include "internal.h"
+
+namespace rtm {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+template <typename T2> __device__ __forceinline__ T2 czero();
+template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
+template <typename T2> __device__ __forceinline__ T2 cmake(double x, double y);
+template <> __device__ __forceinline__ double2 cmake<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 cmake<float2>(double x, double y) {
+    return make_float2((float)x, (float)y);
+}
+
+// v * (-i) for the forward transform, v * (+i) for the inverse.
+template <bool INV, typename T2> __device__ __forceinline__ T2 rot(T2 v) {
+    T2 r;
+    if (INV) { r.x = -v.y; r.y = v.x; } else { r.x = v.y; r.y = -v.x; }
+    return r;
+}
+
+// Multiplies by (c, s) for the forward transform and by (c, -s) for the inverse, where (c, s) is
+// a forward root of unity exp(-i theta) = (cos theta, -sin theta) given as c and s = -sin theta.
+template <bool INV, typename T2, typename S> __device__ __forceinline__ T2 twc(T2 v, S c, S s) {
+    if (INV) s = -s;
+    T2 r;
+    r.x = v.x * c - v.y * s;
+    r.y = v.x * s + v.y * c;
+    return r;
+}
+
+template <bool INV, typename T2> __device__ __forceinline__ void dft2(T2& a, T2& b) {
+    T2 t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <bool INV, typename T2> __device__ __forceinline__ void dft4(T2& a0, T2& a1, T2& a2, T2& a3) {
+    T2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = rot<INV>(csub(a1, a3));
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, t3);
+    a3 = csub(t1, t3);
+}
+
+// sqrt(1/2), cos(pi/8), sin(pi/8)
+#define RTM_R2 0.70710678118654752440084436210485
+#define RTM_C8 0.92387953251128675612818318939679
+#define RTM_S8 0.38268343236508977172845998403040
+
+template <bool INV, typename T2> __device__ __forceinline__ void dft8(T2* v) {
+    using S = decltype(v[0].x);
+    T2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    T2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    const S c = (S)RTM_R2;
+    o1 = twc<INV>(o1, c, -c);
+    o2 = rot<INV>(o2);
+    o3 = twc<INV>(o3, -c, -c);
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+template <bool INV, typename T2> __device__ __forceinline__ void dft16(T2* v) {
+    using S = decltype(v[0].x);
+    T2 e[8], o[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) { e[t] = v[2 * t]; o[t] = v[2 * t + 1]; }
+    dft8<INV>(e);
+    dft8<INV>(o);
+    const S c1 = (S)RTM_C8, s1 = (S)RTM_S8, r2 = (S)RTM_R2;
+    o[1] = twc<INV>(o[1], c1, -s1);
+    o[2] = twc<INV>(o[2], r2, -r2);
+    o[3] = twc<INV>(o[3], s1, -c1);
+    o[4] = rot<INV>(o[4]);
+    o[5] = twc<INV>(o[5], -s1, -c1);
+    o[6] = twc<INV>(o[6], -r2, -r2);
+    o[7] = twc<INV>(o[7], -c1, -s1);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        v[t] = cadd(e[t], o[t]);
+        v[t + 8] = csub(e[t], o[t]);
+    }
+}
+
+// Odd radix R by its definition, with the roots w_R^m = tw[m n / R] of the length-n table.
+template <int R, bool INV, typename T2> __device__ __forceinline__ void dft_odd(T2* v, const T2* __restrict__ tw, int n) {
+    const int st = n / R;
+    T2 w[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        T2 t = __ldg(&tw[m * st]);
+        w[m] = INV ? cconj(t) : t;
+    }
+    T2 out[R];
+    T2 s = v[0];
+#pragma unroll
+    for (int t = 1; t < R; ++t) s = cadd(s, v[t]);
+    out[0] = s;
+#pragma unroll
+    for (int q = 1; q < R; ++q) {
+        T2 acc = v[0];
+#pragma unroll
+        for (int t = 1; t < R; ++t) acc = cadd(acc, cmul(v[t], w[(t * q) % R]));
+        out[q] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = out[q];
+}
+
+template <int R, bool INV, typename T2> __device__ __forceinline__ void dft(T2* v, const T2* __restrict__ tw, int n) {
+    if constexpr (R == 2) dft2<INV>(v[0], v[1]);
+    else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 16) dft16<INV>(v);
+    else dft_odd<R, INV>(v, tw, n);
+}
+
+template <int R, bool INV, typename T2>
+__device__ __forceinline__ void stockham_pass(const T2* __restrict__ src, T2* __restrict__ dst, int n, int Ns,
+                                              int lines, int ls, int es, const T2* __restrict__ tw) {
+    const int nb = n / R;
+    const int stride = n / (Ns * R);
+    const int items = lines * nb;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int line = it % lines;
+        const int j = it / lines;
+        const int k = j % Ns;
+        const T2* s = src + line * ls;
+        T2 v[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) v[t] = s[(j + t * nb) * es];
+        if (Ns > 1) {
+#pragma unroll
+            for (int t = 1; t < R; ++t) {
+                const T2 w = __ldg(&tw[t * k * stride]);
+                v[t] = INV ? cmulc(v[t], w) : cmul(v[t], w);
+            }
+        }
+        dft<R, INV>(v, tw, n);
+        const int base = (j - k) * R + k;
+        T2* d = dst + line * ls;
+#pragma unroll
+        for (int q = 0; q < R; ++q) d[(base + q * Ns) * es] = v[q];
+    }
+}
+
+// Any radix up to kMaxGenericRadix by a direct DFT (rare: sizes with a prime factor above 7).
+template <bool INV, typename T2>
+__device__ void stockham_pass_generic(const T2* __restrict__ src, T2* __restrict__ dst, int n, int R, int Ns,
+                                      int lines, int ls, int es, const T2* __restrict__ tw) {
+    const int nb = n / R;
+    const int stride = n / (Ns * R);
+    const int st = n / R;
+    const int items = lines * nb;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int line = it % lines;
+        const int j = it / lines;
+        const int k = j % Ns;
+        const T2* s = src + line * ls;
+        T2 v[kMaxGenericRadix];
+        for (int t = 0; t < R; ++t) {
+            T2 x = s[(j + t * nb) * es];
+            if (Ns > 1 && t > 0) {
+                const T2 w = __ldg(&tw[t * k * stride]);
+                x = INV ? cmulc(x, w) : cmul(x, w);
+            }
+            v[t] = x;
+        }
+        const int base = (j - k) * R + k;
+        T2* d = dst + line * ls;
+        for (int q = 0; q < R; ++q) {
+            T2 acc = v[0];
+            for (int t = 1; t < R; ++t) {
+                const T2 w = __ldg(&tw[((t * q) % R) * st]);
+                acc = cadd(acc, INV ? cmulc(v[t], w) : cmul(v[t], w));
+            }
+            d[(base + q * Ns) * es] = acc;
+        }
+    }
+}
+
+// Transforms the lines in `a` (using `b` as scratch) and returns the buffer holding the result.
+// Call after a __syncthreads() that makes `a` visible; returns after a __syncthreads().
+template <bool INV, typename T2>
+__device__ T2* fft_smem(T2* a, T2* b, int lines, int ls, int es, const FftPlan& p, const T2* __restrict__ tw) {
+    int Ns = 1;
+    for (int s = 0; s < p.nstages; ++s) {
+        const int r = p.radix[s];
+        switch (r) {
+            case 2: stockham_pass<2, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 3: stockham_pass<3, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 4: stockham_pass<4, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 5: stockham_pass<5, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 7: stockham_pass<7, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 8: stockham_pass<8, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            case 16: stockham_pass<16, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
+            default: stockham_pass_generic<INV>(a, b, p.n, r, Ns, lines, ls, es, tw); break;
+        }
+        __syncthreads();
+        T2* t = a;
+        a = b;
+        b = t;
+        Ns *= r;
+    }
+    return a;
+}
+
+}  // namespace rtm

@@ -1,0 +1,870 @@
+// FFT products on the rooftop grid and the on-device spectra builders (see grid.h).
+//
+// Follows the reference's
+//   src/+rooftopMoM/+assembler/+greensMatrix/@SplitFFTApplicator/applyBothDirections_.m:14-85
+//   src/+rooftopMoM/+assembler/+greensMatrix/@SplitFFTApplicator/applySingleDirection_.m:14-26
+//   src/+rooftopMoM/+assembler/+greensMatrix/@LeanSplitFFTApplicator/applyBothDirections_.m:13-91
+//   src/+rooftopMoM/+assembler/+greensMatrix/FFTApplicator.m:52-87
+//   src/+rooftopMoM/+assembler/+greensMatrix/+utils/generateSubbandSpectra.m:20-77
+//   src/+rooftopMoM/+assembler/+greensMatrix/+utils/generateEmbeddingSpectra.m:15-40
+//   src/+rooftopMoM/+assembler/+greensMatrix/+utils/generateBlockSpectra.m:19-50
+//   src/+rooftopMoM/+assembler/+preconditioner/generatePartwiseSpectra.m:16-30 (+ kernels, foldGenerator.m)
+//   src/+rooftopMoM/+assembler/+greensMatrix/@Spectra/invert.m:12-20
+//
+// The subband spectra are computed as P x Q transforms of the folded, modulated embedding:
+// frequency 2m + p of a period-2P sequence e is the length-P DFT of (e(d) + (-1)^p e(d + P)) w^(p d),
+// w = exp(-i pi / P), which is the same number as subsampling the 2P x 2Q transform.
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "fft.cuh"
+#include "grid.h"
+
+namespace rtm {
+
+static constexpr int kSmemBudget = 200 * 1024;
+static constexpr int kThreads = 256;
+
+template <typename T> struct GridArgs {
+    using T2 = typename Cx<T>::T2;
+    int P, Q, nsx, nsy;
+    int rows[2], cols[2];
+    int64_t off[2];
+    int64_t n;
+    int ncomp;
+    int ti;          // x columns per y-tile
+    int py0, npy;    // y subbands handled by this launch (lean: one at a time)
+    int accumulate;  // y-inverse adds into y (second parity of the lean product)
+    FftPlan planP, planQ;
+    const T2* twP;
+    const T2* twQ;
+    const T2* modP;
+    const T2* modQ;
+    T2* work;
+    int64_t work_rhs;  // elements of W per right-hand side
+    int mode;
+    const T2* spec;
+    const T2* ux0;
+    const T2* ux1;
+    const T2* vy0;
+    const T2* vy1;
+    T inv_a2, inv_b2, inv_ab, scale;
+    const int* skip;  // per right-hand side, nonzero: leave it alone
+    int skip_stride;
+};
+
+template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rhs) {
+    return a.skip != nullptr && a.skip[(int64_t)rhs * a.skip_stride] != 0;
+}
+
+// --------------------------------------------------------------------------------------------
+// y-forward: W[py][c][j][i] = FFT_y( x_c(i, j) * mody(j)^py ), i in the tile.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+    using T2 = typename Cx<T>::T2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TI = a.ti, Q = a.Q;
+    T2* A = reinterpret_cast<T2*>(smem_raw);
+    T2* B = A + TI * Q;
+    const int i0 = blockIdx.x * TI;
+    const int rhs = blockIdx.y;
+    if (skipped(a, rhs)) return;
+    const T2* xr = x + (int64_t)rhs * a.n;
+    T2* wr = a.work + (int64_t)rhs * a.work_rhs;
+    for (int c = 0; c < a.ncomp; ++c) {
+        const int rows = a.rows[c], cols = a.cols[c];
+        if (i0 >= rows) continue;
+        for (int pyi = 0; pyi < a.npy; ++pyi) {
+            const int py = a.py0 + pyi;
+            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+                const int l = it % TI, j = it / TI, i = i0 + l;
+                T2 v = czero<T2>();
+                if (i < rows && j < cols) {
+                    v = xr[a.off[c] + i + (int64_t)j * rows];
+                    if (py) v = cmul(v, __ldg(&a.modQ[j]));
+                }
+                A[it] = v;
+            }
+            __syncthreads();
+            T2* out = fft_smem<false>(A, B, TI, 1, TI, a.planQ, a.twQ);
+            T2* dst = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
+            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+                const int l = it % TI, j = it / TI, i = i0 + l;
+                if (i < rows) dst[(int64_t)j * a.P + i] = out[it];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------------------
+// x-mix: per y frequency j of the y subband py, both components: sum over px of
+// demod_x^px * IFFT_x( B(px,py) * FFT_x( W * mod_x^px ) ), scaled by 1/(PQ), in place.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_grid_x_mix(const GridArgs<T> a) {
+    using T2 = typename Cx<T>::T2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int P = a.P, Q = a.Q, nc = a.ncomp;
+    T2* acc = reinterpret_cast<T2*>(smem_raw);
+    T2* A = acc + nc * P;
+    T2* B = A + nc * P;
+    const int j = blockIdx.x;
+    const int pyi = blockIdx.y;
+    const int py = a.py0 + pyi;
+    const int rhs = blockIdx.z;
+    if (skipped(a, rhs)) return;
+    T2* wr = a.work + (int64_t)rhs * a.work_rhs + (int64_t)pyi * nc * Q * P;
+    const T2* vy = py ? a.vy1 : a.vy0;
+    for (int px = 0; px < a.nsx; ++px) {
+        for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
+            const int c = it / P, i = it - c * P;
+            T2 v = czero<T2>();
+            if (i < a.rows[c]) {
+                v = wr[((int64_t)c * Q + j) * P + i];
+                if (px) v = cmul(v, __ldg(&a.modP[i]));
+            }
+            A[it] = v;
+        }
+        __syncthreads();
+        T2* U = fft_smem<false>(A, B, nc, P, 1, a.planP, a.twP);
+        T2* other = (U == A) ? B : A;
+        const int sub = px + a.nsx * py;
+        const T2* ux = px ? a.ux1 : a.ux0;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const T2 sx = U[i], sy = U[P + i];
+            T2 ox, oy;
+            if (a.mode == kGen3) {
+                const int64_t base = ((int64_t)(sub * 3) * Q + j) * P + i;
+                const T2 E = __ldg(&a.spec[base]);
+                const T2 Mx = __ldg(&a.spec[base + (int64_t)Q * P]);
+                const T2 My = __ldg(&a.spec[base + 2 * (int64_t)Q * P]);
+                const T2 u = __ldg(&ux[i]);
+                const T2 v = __ldg(&vy[j]);
+                const T cu = (u.x * u.x + u.y * u.y) * a.inv_a2;
+                const T cv = (v.x * v.x + v.y * v.y) * a.inv_b2;
+                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E.
+                T2 qc = cmulc(u, v);
+                qc.x = -qc.x * a.inv_ab;
+                qc.y = -qc.y * a.inv_ab;
+                const T2 Ex = cmul(E, sx), Ey = cmul(E, sy);
+                ox = csub(cmul(Mx, sx), cscale(Ex, cu));
+                ox = cadd(ox, cmul(qc, Ey));
+                oy = csub(cmul(My, sy), cscale(Ey, cv));
+                oy = cadd(oy, cmul(cconj(qc), Ex));
+            } else {
+                const int64_t base = (int64_t)j * P + i, blk = (int64_t)Q * P;
+                const T2 XX = __ldg(&a.spec[base]), XY = __ldg(&a.spec[base + blk]);
+                const T2 YX = __ldg(&a.spec[base + 2 * blk]), YY = __ldg(&a.spec[base + 3 * blk]);
+                ox = cadd(cmul(XX, sx), cmul(XY, sy));
+                oy = cadd(cmul(YX, sx), cmul(YY, sy));
+            }
+            U[i] = ox;
+            U[P + i] = oy;
+        }
+        __syncthreads();
+        T2* Y = fft_smem<true>(U, other, nc, P, 1, a.planP, a.twP);
+        for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
+            const int c = it / P, i = it - c * P;
+            T2 v = Y[it];
+            if (px) v = cmulc(v, __ldg(&a.modP[i]));
+            acc[it] = px ? cadd(acc[it], v) : v;
+        }
+        __syncthreads();
+    }
+    for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
+        const int c = it / P, i = it - c * P;
+        if (i < a.rows[c]) wr[((int64_t)c * Q + j) * P + i] = cscale(acc[it], a.scale);
+    }
+}
+
+// --------------------------------------------------------------------------------------------
+// y-inverse: y_c(i, j) = sum_py demod_y^py IFFT_y(W[py][c][:, i]) for the tile, cropped.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+    using T2 = typename Cx<T>::T2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TI = a.ti, Q = a.Q;
+    T2* acc = reinterpret_cast<T2*>(smem_raw);
+    T2* A = acc + TI * Q;
+    T2* B = A + TI * Q;
+    const int i0 = blockIdx.x * TI;
+    const int rhs = blockIdx.y;
+    if (skipped(a, rhs)) return;
+    T2* yr = y + (int64_t)rhs * a.n;
+    const T2* wr = a.work + (int64_t)rhs * a.work_rhs;
+    for (int c = 0; c < a.ncomp; ++c) {
+        const int rows = a.rows[c], cols = a.cols[c];
+        if (i0 >= rows) continue;
+        for (int pyi = 0; pyi < a.npy; ++pyi) {
+            const int py = a.py0 + pyi;
+            const T2* src = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
+            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+                const int l = it % TI, j = it / TI, i = i0 + l;
+                A[it] = (i < rows) ? src[(int64_t)j * a.P + i] : czero<T2>();
+            }
+            __syncthreads();
+            T2* R = fft_smem<true>(A, B, TI, 1, TI, a.planQ, a.twQ);
+            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+                const int j = it / TI;
+                T2 v = R[it];
+                if (py) v = cmulc(v, __ldg(&a.modQ[j]));
+                acc[it] = pyi ? cadd(acc[it], v) : v;
+            }
+            __syncthreads();
+        }
+        for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+            const int l = it % TI, j = it / TI, i = i0 + l;
+            if (i < rows && j < cols) {
+                const int64_t idx = a.off[c] + i + (int64_t)j * rows;
+                yr[idx] = a.accumulate ? cadd(yr[idx], acc[it]) : acc[it];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------------------------------------
+// Strip: y = sum_s demod^s IFFT( B_s * FFT( x * mod^s ) ) / L on one line per right-hand side.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
+                                                   typename Cx<T>::T2* __restrict__ y) {
+    using T2 = typename Cx<T>::T2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int L = a.P;
+    const int count = (int)a.n;
+    T2* acc = reinterpret_cast<T2*>(smem_raw);
+    T2* A = acc + L;
+    T2* B = A + L;
+    const int rhs = blockIdx.x;
+    if (skipped(a, rhs)) return;
+    const T2* xr = x + (int64_t)rhs * a.n;
+    T2* yr = y + (int64_t)rhs * a.n;
+    for (int s = 0; s < a.nsx; ++s) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            T2 v = czero<T2>();
+            if (i < count) {
+                v = xr[i];
+                if (s) v = cmul(v, __ldg(&a.modP[i]));
+            }
+            A[i] = v;
+        }
+        __syncthreads();
+        T2* U = fft_smem<false>(A, B, 1, L, 1, a.planP, a.twP);
+        T2* other = (U == A) ? B : A;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) U[i] = cmul(U[i], __ldg(&a.spec[(int64_t)s * L + i]));
+        __syncthreads();
+        T2* Y = fft_smem<true>(U, other, 1, L, 1, a.planP, a.twP);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            T2 v = Y[i];
+            if (s) v = cmulc(v, __ldg(&a.modP[i]));
+            acc[i] = s ? cadd(acc[i], v) : v;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < count; i += blockDim.x) yr[i] = cscale(acc[i], a.scale);
+}
+
+// --------------------------------------------------------------------------------------------
+template <typename T> static void set_smem_attrs() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (done[dev & 63]) return;
+    cudaFuncSetAttribute(k_grid_y_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_grid_x_mix<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_grid_y_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    done[dev & 63] = true;
+}
+
+static int tile_columns(int Q, int nbuf, size_t elem) {
+    int ti = 16;
+    while (ti > 1 && (size_t)nbuf * ti * Q * elem > (size_t)kSmemBudget) ti /= 2;
+    if ((size_t)nbuf * ti * Q * elem > (size_t)kSmemBudget) return 0;
+    return ti;
+}
+
+size_t GridApplicator::work_bytes_per_rhs() const {
+    if (mode == kStrip) return 0;
+    const size_t elem = precision == RTM_FP64 ? sizeof(double2) : sizeof(float2);
+    const int npy = lean ? 1 : nsy;
+    return (size_t)npy * 2 * P * Q * elem;
+}
+
+template <typename T>
+static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip) {
+    using T2 = typename Cx<T>::T2;
+    set_smem_attrs<T>();
+    const T2* x = static_cast<const T2*>(xv);
+    T2* y = static_cast<T2*>(yv);
+    GridArgs<T> a{};
+    a.skip = skip.ptr;
+    a.skip_stride = skip.stride;
+    a.P = g.P;
+    a.Q = g.Q;
+    a.nsx = g.nsx;
+    a.nsy = g.nsy;
+    for (int c = 0; c < 2; ++c) {
+        a.rows[c] = g.rows[c];
+        a.cols[c] = g.cols[c];
+        a.off[c] = g.off[c];
+    }
+    a.n = g.n;
+    a.ncomp = 2;
+    a.planP = g.tP->plan;
+    a.planQ = g.tQ->plan;
+    if constexpr (sizeof(T) == 8) {
+        a.twP = g.tP->tw64; a.twQ = g.tQ->tw64; a.modP = g.tP->mod64; a.modQ = g.tQ->mod64;
+    } else {
+        a.twP = g.tP->tw32; a.twQ = g.tQ->tw32; a.modP = g.tP->mod32; a.modQ = g.tQ->mod32;
+    }
+    a.spec = g.spec.as<T2>();
+    a.mode = g.mode;
+    a.ux0 = static_cast<const T2*>(g.ux[0]);
+    a.ux1 = static_cast<const T2*>(g.ux[1]);
+    a.vy0 = static_cast<const T2*>(g.vy[0]);
+    a.vy1 = static_cast<const T2*>(g.vy[1]);
+    a.inv_a2 = (T)(1.0 / (g.size_x * g.size_x));
+    a.inv_b2 = (T)(1.0 / (g.size_y * g.size_y));
+    a.inv_ab = (T)(1.0 / (g.size_x * g.size_y));
+    const size_t elem = sizeof(T2);
+    if (g.mode == kStrip) {
+        a.scale = (T)(1.0 / g.P);
+        const size_t smem = 3 * (size_t)g.P * elem;
+        if (smem > (size_t)kSmemBudget) return fail(RTM_ERR_UNSUPPORTED, "strip too long for this build");
+        k_strip<T><<<nrhs, kThreads, smem, s>>>(a, x, y);
+        count_launch();
+        RTM_CUDA(cudaGetLastError());
+        return RTM_OK;
+    }
+    a.scale = (T)(1.0 / ((double)g.P * g.Q));
+    a.work = g.work.as<T2>();
+    a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
+    const int ti_f = tile_columns(g.Q, 2, elem);
+    const int ti_i = tile_columns(g.Q, 3, elem);
+    const size_t smem_mix = 3 * 2 * (size_t)g.P * elem;
+    if (ti_f == 0 || ti_i == 0 || smem_mix > (size_t)kSmemBudget)
+        return fail(RTM_ERR_UNSUPPORTED, "FFT grid too large for this build");
+    const int rows_max = std::max(g.rows[0], g.rows[1]);
+    const int passes = g.lean ? g.nsy : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+        a.py0 = g.lean ? pass : 0;
+        a.npy = g.lean ? 1 : g.nsy;
+        a.accumulate = g.lean && pass > 0;
+        a.ti = ti_f;
+        dim3 gf((rows_max + ti_f - 1) / ti_f, nrhs);
+        k_grid_y_fwd<T><<<gf, kThreads, 2 * (size_t)ti_f * g.Q * elem, s>>>(a, x);
+        dim3 gm(g.Q, a.npy, nrhs);
+        k_grid_x_mix<T><<<gm, kThreads, smem_mix, s>>>(a);
+        a.ti = ti_i;
+        dim3 gi((rows_max + ti_i - 1) / ti_i, nrhs);
+        k_grid_y_inv<T><<<gi, kThreads, 3 * (size_t)ti_i * g.Q * elem, s>>>(a, y);
+        count_launch(3);
+        RTM_CUDA(cudaGetLastError());
+    }
+    return RTM_OK;
+}
+
+int GridApplicator::reserve(int nrhs) {
+    if (nrhs <= max_rhs && (mode == kStrip || work.bytes >= work_bytes_per_rhs() * (size_t)nrhs)) return RTM_OK;
+    if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
+    max_rhs = std::max(max_rhs, nrhs);
+    return RTM_OK;
+}
+
+int GridApplicator::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) {
+    if (nrhs < 1 || nrhs > max_rhs) return fail(RTM_ERR_ARG, "more right-hand sides than the product reserved");
+    return precision == RTM_FP64 ? apply_t<double>(*this, x, y, nrhs, s, skip)
+                                 : apply_t<float>(*this, x, y, nrhs, s, skip);
+}
+
+// ============================================================================================
+// Spectra builders: 2-D DFTs (P x Q) of generated inputs, in FP64.
+enum SourceKind { kSrcEmbed = 0, kSrcCirculant = 1 };
+enum Window { kWinStrang = 0, kWinTChan = 1, kWinRChan = 2, kWinHuckle = 3 };
+constexpr int kMaxItems = 12;
+
+struct GenItem {
+    const double2* g;  // generator, column-major rows x cols
+    int rows, cols;
+    int px, py;
+    double2* dst;      // P x Q output (column-major, x fastest)
+};
+
+struct GenArgs {
+    int P, Q;
+    int kind;
+    int Lx, Ly;        // mirror periods of the embedding
+    int nsx, nsy;      // folded copies (2 for split directions)
+    double scale;
+    int window, bw_x, bw_y;
+    int realify;
+    int ti;
+    FftPlan planP, planQ;
+    const double2* twP;
+    const double2* twQ;
+    const double2* modP;
+    const double2* modQ;
+    int nitems;
+    GenItem items[kMaxItems];
+};
+
+__device__ __forceinline__ int mirror_index(int i, int rows, int L) {
+    if (i < rows) return i;
+    const int m = L - i;
+    return (m >= 0 && m < rows) ? m : -1;
+}
+
+__device__ __forceinline__ double window_weight(int w, int o, int n, int bw) {
+    const int ao = o < 0 ? -o : o;
+    switch (w) {
+        case kWinStrang: return (2 * ao < n) ? 1.0 : (2 * ao == n ? 0.5 : 0.0);
+        case kWinTChan: return (double)(n - ao) / (double)n;
+        case kWinRChan: return 1.0;
+        default: return fmax(0.0, 1.0 - (double)ao / (double)bw);
+    }
+}
+
+__device__ double2 gen_value(const GenArgs& a, const GenItem& it, int i, int j) {
+    double re = 0, im = 0;
+    if (a.kind == kSrcEmbed) {
+        for (int ca = 0; ca < a.nsx; ++ca) {
+            const int mx = mirror_index(i + ca * a.P, it.rows, a.Lx);
+            if (mx < 0) continue;
+            const double sa = (it.px && ca) ? -1.0 : 1.0;
+            for (int cb = 0; cb < a.nsy; ++cb) {
+                const int my = mirror_index(j + cb * a.Q, it.cols, a.Ly);
+                if (my < 0) continue;
+                const double sb = (it.py && cb) ? -1.0 : 1.0;
+                const double2 g = it.g[mx + (int64_t)my * it.rows];
+                re += sa * sb * g.x;
+                im += sa * sb * g.y;
+            }
+        }
+        double2 v = make_double2(re * a.scale, im * a.scale);
+        if (it.px) v = cmul(v, a.modP[i]);
+        if (it.py) v = cmul(v, a.modQ[j]);
+        return v;
+    }
+    // Circulant fold of the even generator onto the face grid (foldGenerator.m:38-45).
+    for (int ca = 0; ca < 2; ++ca) {
+        if (ca == 1 && i == 0) continue;
+        const int mx = ca ? a.P - i : i;
+        if (mx >= it.rows) continue;
+        const double wa = window_weight(a.window, ca ? i - a.P : i, a.P, a.bw_x);
+        for (int cb = 0; cb < 2; ++cb) {
+            if (cb == 1 && j == 0) continue;
+            const int my = cb ? a.Q - j : j;
+            if (my >= it.cols) continue;
+            const double wb = window_weight(a.window, cb ? j - a.Q : j, a.Q, a.bw_y);
+            const double2 g = it.g[mx + (int64_t)my * it.rows];
+            re += wa * wb * g.x;
+            im += wa * wb * g.y;
+        }
+    }
+    return make_double2(re, im);
+}
+
+__global__ void __launch_bounds__(kThreads) k_gen_y(const GenArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TI = a.ti, Q = a.Q;
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    double2* B = A + TI * Q;
+    const GenItem& item = a.items[blockIdx.y];
+    const int i0 = blockIdx.x * TI;
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        A[it] = (i < a.P) ? gen_value(a, item, i, j) : make_double2(0, 0);
+    }
+    __syncthreads();
+    double2* out = fft_smem<false>(A, B, TI, 1, TI, a.planQ, a.twQ);
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        if (i < a.P) item.dst[(int64_t)j * a.P + i] = out[it];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_gen_x(const GenArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int P = a.P;
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    double2* B = A + P;
+    const GenItem& item = a.items[blockIdx.y];
+    const int j = blockIdx.x;
+    double2* col = item.dst + (int64_t)j * P;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) A[i] = col[i];
+    __syncthreads();
+    double2* out = fft_smem<false>(A, B, 1, P, 1, a.planP, a.twP);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        double2 v = out[i];
+        if (a.realify) v.y = 0.0;
+        col[i] = v;
+    }
+}
+
+static int run_gen(GenArgs& a, cudaStream_t s) {
+    static bool attrs = false;
+    if (!attrs) {
+        cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attrs = true;
+    }
+    if (a.nitems == 0) return RTM_OK;
+    a.ti = tile_columns(a.Q, 2, sizeof(double2));
+    if (a.ti == 0 || 2 * (size_t)a.P * sizeof(double2) > (size_t)kSmemBudget)
+        return fail(RTM_ERR_UNSUPPORTED, "spectra grid too large for this build");
+    dim3 gy((a.P + a.ti - 1) / a.ti, a.nitems);
+    k_gen_y<<<gy, kThreads, 2 * (size_t)a.ti * a.Q * sizeof(double2), s>>>(a);
+    dim3 gx(a.Q, a.nitems);
+    k_gen_x<<<gx, kThreads, 2 * (size_t)a.P * sizeof(double2), s>>>(a);
+    count_launch(2);
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
+// Explicit strip blocks B_s = M_s - |u_s|^2 / h^2 E_s on a line of length L (generateBlockSpectra.m:36-42).
+__global__ void k_strip_blocks(int L, int nsub, const double2* __restrict__ raw, const double2* __restrict__ u0,
+                               const double2* __restrict__ u1, double inv_h2, double2* __restrict__ out) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L * nsub) return;
+    const int s = idx / L, i = idx - s * L;
+    const double2 E = raw[(int64_t)(s * 2 + 0) * L + i];
+    const double2 M = raw[(int64_t)(s * 2 + 1) * L + i];
+    const double2 u = (s ? u1 : u0)[i];
+    const double c = (u.x * u.x + u.y * u.y) * inv_h2;
+    out[idx] = make_double2(M.x - c * E.x, M.y - c * E.y);
+}
+
+// Circulant blocks and their 2x2 inverse (generateBlockSpectra.m + Spectra.invert), flags any
+// non-finite value. raw: [E, MXX, MYY] on the face grid; out: [XX, XY, YX, YY].
+__global__ void k_circulant_invert(int P, int Q, int content, const double2* __restrict__ raw,
+                                   const double2* __restrict__ u, const double2* __restrict__ v, double inv_a2,
+                                   double inv_b2, double inv_ab, double2* __restrict__ out, int* __restrict__ bad) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t G = (int64_t)P * Q;
+    if (idx >= G) return;
+    const int i = (int)(idx % P), j = (int)(idx / P);
+    const double2 E = raw[idx], Mx = raw[G + idx], My = raw[2 * G + idx];
+    const double2 uu = u[i], vv = v[j];
+    const double cu = (uu.x * uu.x + uu.y * uu.y) * inv_a2;
+    const double cv = (vv.x * vv.x + vv.y * vv.y) * inv_b2;
+    double2 XX = make_double2(Mx.x - cu * E.x, Mx.y - cu * E.y);
+    double2 YY = make_double2(My.x - cv * E.x, My.y - cv * E.y);
+    double2 qc = cmulc(uu, vv);
+    qc.x = -qc.x * inv_ab;
+    qc.y = -qc.y * inv_ab;
+    double2 XY = cmul(qc, E), YX = cmul(cconj(qc), E);
+    double2 r[4];
+    if (content == RTM_XONLY) {
+        const double d = XX.x * XX.x + XX.y * XX.y;
+        r[0] = make_double2(XX.x / d, -XX.y / d);
+        r[1] = r[2] = r[3] = make_double2(0, 0);
+    } else if (content == RTM_YONLY) {
+        const double d = YY.x * YY.x + YY.y * YY.y;
+        r[3] = make_double2(YY.x / d, -YY.y / d);
+        r[0] = r[1] = r[2] = make_double2(0, 0);
+    } else {
+        const double2 det = csub(cmul(XX, YY), cmul(XY, YX));
+        const double dd = det.x * det.x + det.y * det.y;
+        const double2 inv = make_double2(det.x / dd, -det.y / dd);
+        r[0] = cmul(YY, inv);
+        r[1] = cmul(make_double2(-XY.x, -XY.y), inv);
+        r[2] = cmul(make_double2(-YX.x, -YX.y), inv);
+        r[3] = cmul(XX, inv);
+    }
+    for (int b = 0; b < 4; ++b) {
+        if (!isfinite(r[b].x) || !isfinite(r[b].y)) atomicExch(bad, 1);
+        out[b * G + idx] = r[b];
+    }
+}
+
+__global__ void k_to_fp32(int64_t n, const double2* __restrict__ in, float2* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+static int convert_spectra(const DeviceBuffer& src64, int precision, DeviceBuffer& dst, cudaStream_t s) {
+    const int64_t n = (int64_t)(src64.bytes / sizeof(double2));
+    if (precision == RTM_FP64) {
+        RTM_TRY(dst.alloc(src64.bytes));
+        RTM_CUDA(cudaMemcpyAsync(dst.ptr, src64.ptr, src64.bytes, cudaMemcpyDeviceToDevice, s));
+        return RTM_OK;
+    }
+    RTM_TRY(dst.alloc((size_t)n * sizeof(float2)));
+    k_to_fp32<<<592, 256, 0, s>>>(n, src64.as<double2>(), dst.as<float2>());
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
+static void fill_shift(GridApplicator& out, int n, int parity, bool x_dir, int slot) {
+    const double2* s64 = nullptr;
+    const float2* s32 = nullptr;
+    shift_factors(n, parity, &s64, &s32);
+    const void* p = out.precision == RTM_FP64 ? (const void*)s64 : (const void*)s32;
+    if (x_dir) out.ux[slot] = p; else out.vy[slot] = p;
+}
+
+static void layout(GridApplicator& o, int cx, int cy) {
+    o.count_x = cx;
+    o.count_y = cy;
+    o.rows[0] = cx - 1; o.cols[0] = cy;
+    o.rows[1] = cx;     o.cols[1] = cy - 1;
+    const int64_t nx = (int64_t)(cx - 1) * cy, ny = (int64_t)cx * (cy - 1);
+    o.off[0] = 0;
+    o.off[1] = nx;
+    o.n = nx + ny;
+    o.content = (nx > 0 && ny > 0) ? RTM_BOTH : nx > 0 ? RTM_XONLY : ny > 0 ? RTM_YONLY : RTM_NONE;
+}
+
+int build_product(const DeviceGenerators& g, double size_x, double size_y, int product, int precision, int max_rhs,
+                  GridApplicator& out, cudaStream_t s) {
+    const int cx = g.count_x, cy = g.count_y;
+    layout(out, cx, cy);
+    out.precision = precision;
+    out.size_x = size_x;
+    out.size_y = size_y;
+    out.max_rhs = std::max(1, max_rhs);
+    out.lean = product == RTM_PRODUCT_LEAN;
+    if (out.content == RTM_NONE) return fail(RTM_ERR_ARG, "a single face carries no rooftop");
+    GenArgs a{};
+    a.kind = kSrcEmbed;
+    if (product == RTM_PRODUCT_FFT) {
+        // generateEmbeddingSpectra.m: period 2n - 2 along every direction with more than one face.
+        out.P = cx > 1 ? 2 * cx - 2 : 1;
+        out.Q = cy > 1 ? 2 * cy - 2 : 1;
+        out.nsx = out.nsy = 1;
+        a.Lx = out.P;
+        a.Ly = out.Q;
+        a.nsx = a.nsy = 1;
+        a.scale = 1.0;
+    } else {
+        // generateSubbandSpectra.m: fast FFT size and 2 subbands along every direction with more than one face.
+        out.P = cx > 1 ? fast_fft_size(cx) : 1;
+        out.Q = cy > 1 ? fast_fft_size(cy) : 1;
+        out.nsx = cx > 1 ? 2 : 1;
+        out.nsy = cy > 1 ? 2 : 1;
+        a.Lx = out.nsx * out.P;
+        a.Ly = out.nsy * out.Q;
+        a.nsx = out.nsx;
+        a.nsy = out.nsy;
+        a.scale = 1.0 / (out.nsx * out.nsy);
+    }
+    const FftTables* tP = nullptr;
+    const FftTables* tQ = nullptr;
+    RTM_TRY(fft_tables(out.P, &tP));
+    RTM_TRY(fft_tables(out.Q, &tQ));
+    out.tP = tP;
+    out.tQ = tQ;
+    a.P = out.P;
+    a.Q = out.Q;
+    a.planP = tP->plan;
+    a.planQ = tQ->plan;
+    a.twP = tP->tw64;
+    a.twQ = tQ->tw64;
+    a.modP = tP->mod64;
+    a.modQ = tQ->mod64;
+    a.realify = g.is_real ? 1 : 0;
+    const int nsub = out.nsx * out.nsy;
+    const int64_t G = (int64_t)out.P * out.Q;
+    const double2* gens[3] = {g.e.as<double2>(), g.xx.as<double2>(), g.yy.as<double2>()};
+    const int grows[3] = {cx, cx - 1, cx};
+    const int gcols[3] = {cy, cy, cy - 1};
+
+    if (out.content == RTM_BOTH) {
+        out.mode = kGen3;
+        DeviceBuffer raw;
+        RTM_TRY(raw.alloc((size_t)nsub * 3 * G * sizeof(double2)));
+        RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
+        for (int sub = 0; sub < nsub; ++sub) {
+            for (int k = 0; k < 3; ++k) {
+                GenItem& it = a.items[a.nitems++];
+                it.g = gens[k];
+                it.rows = grows[k];
+                it.cols = gcols[k];
+                it.px = sub % out.nsx;
+                it.py = sub / out.nsx;
+                it.dst = raw.as<double2>() + (int64_t)(sub * 3 + k) * G;
+            }
+        }
+        RTM_TRY(run_gen(a, s));
+        RTM_TRY(convert_spectra(raw, precision, out.spec, s));
+        out.spec_blocks = nsub * 3;
+        for (int p = 0; p < out.nsx; ++p) fill_shift(out, out.P, p, true, p);
+        for (int p = 0; p < out.nsy; ++p) fill_shift(out, out.Q, p, false, p);
+        if (out.nsx == 1) fill_shift(out, out.P, 0, true, 1);
+        if (out.nsy == 1) fill_shift(out, out.Q, 0, false, 1);
+        RTM_TRY(out.work.alloc(out.work_bytes_per_rhs() * out.max_rhs));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        return RTM_OK;
+    }
+    // Strips: a line along the direction with rooftops; subbands along it (x strip: Q = 1).
+    out.mode = kStrip;
+    const bool xs = out.content == RTM_XONLY;
+    const int L = xs ? out.P : out.Q;
+    const int ns = xs ? out.nsx : out.nsy;
+    DeviceBuffer raw, blocks64;
+    RTM_TRY(raw.alloc((size_t)ns * 2 * G * sizeof(double2)));
+    RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
+    for (int sub = 0; sub < ns; ++sub) {
+        for (int k = 0; k < 2; ++k) {
+            GenItem& it = a.items[a.nitems++];
+            const int gi = k == 0 ? 0 : (xs ? 1 : 2);
+            it.g = gens[gi];
+            it.rows = grows[gi];
+            it.cols = gcols[gi];
+            it.px = xs ? sub : 0;
+            it.py = xs ? 0 : sub;
+            it.dst = raw.as<double2>() + (int64_t)(sub * 2 + k) * G;
+        }
+    }
+    RTM_TRY(run_gen(a, s));
+    RTM_TRY(blocks64.alloc((size_t)ns * L * sizeof(double2)));
+    const double2* u0 = nullptr;
+    const double2* u1 = nullptr;
+    const float2* f = nullptr;
+    RTM_TRY(shift_factors(L, 0, &u0, &f));
+    if (ns > 1) RTM_TRY(shift_factors(L, 1, &u1, &f));
+    const double h = xs ? size_x : size_y;
+    k_strip_blocks<<<(ns * L + 255) / 256, 256, 0, s>>>(L, ns, raw.as<double2>(), u0, u1 ? u1 : u0, 1.0 / (h * h),
+                                                         blocks64.as<double2>());
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    RTM_TRY(convert_spectra(blocks64, precision, out.spec, s));
+    out.spec_blocks = ns;
+    // The strip kernel runs on P (line length) with nsx subbands.
+    out.P = L;
+    out.Q = 1;
+    out.nsx = ns;
+    out.nsy = 1;
+    RTM_TRY(fft_tables(L, &out.tP));
+    RTM_TRY(fft_tables(1, &out.tQ));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    return RTM_OK;
+}
+
+int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int kernel, int builder,
+                    const int* bandwidth, int precision, GridApplicator& out, cudaStream_t s) {
+    if (builder != RTM_BUILDER_PARTWISE || kernel == RTM_KERNEL_SUPEROPTIMAL)
+        return fail(RTM_ERR_UNSUPPORTED, "only the partwise builder with the strang, tChan, rChan and huckle kernels "
+                                         "is built on the device in this version");
+    const int cx = g.count_x, cy = g.count_y;
+    layout(out, cx, cy);
+    out.precision = precision;
+    out.size_x = size_x;
+    out.size_y = size_y;
+    out.max_rhs = 1;
+    out.P = cx;
+    out.Q = cy;
+    out.nsx = out.nsy = 1;
+    RTM_TRY(fft_tables(out.P, &out.tP));
+    RTM_TRY(fft_tables(out.Q, &out.tQ));
+    GenArgs a{};
+    a.kind = kSrcCirculant;
+    a.P = cx;
+    a.Q = cy;
+    a.window = kernel == RTM_KERNEL_STRANG ? kWinStrang : kernel == RTM_KERNEL_TCHAN ? kWinTChan
+               : kernel == RTM_KERNEL_RCHAN ? kWinRChan : kWinHuckle;
+    a.bw_x = bandwidth ? bandwidth[0] : cx;
+    a.bw_y = bandwidth ? bandwidth[1] : cy;
+    a.planP = out.tP->plan;
+    a.planQ = out.tQ->plan;
+    a.twP = out.tP->tw64;
+    a.twQ = out.tQ->tw64;
+    a.realify = 0;
+    const int64_t G = (int64_t)cx * cy;
+    DeviceBuffer raw;
+    RTM_TRY(raw.alloc(3 * (size_t)G * sizeof(double2)));
+    RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
+    const double2* gens[3] = {g.e.as<double2>(), g.xx.as<double2>(), g.yy.as<double2>()};
+    const int grows[3] = {cx, cx - 1, cx};
+    const int gcols[3] = {cy, cy, cy - 1};
+    for (int k = 0; k < 3; ++k) {
+        if (!gens[k]) continue;
+        GenItem& it = a.items[a.nitems++];
+        it.g = gens[k];
+        it.rows = grows[k];
+        it.cols = gcols[k];
+        it.px = it.py = 0;
+        it.dst = raw.as<double2>() + k * G;
+    }
+    RTM_TRY(run_gen(a, s));
+    DeviceBuffer inv, flag;
+    RTM_TRY(inv.alloc(4 * (size_t)G * sizeof(double2)));
+    RTM_TRY(flag.alloc(sizeof(int)));
+    RTM_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(int), s));
+    const double2* u = nullptr;
+    const double2* v = nullptr;
+    const float2* f = nullptr;
+    RTM_TRY(shift_factors(cx, 0, &u, &f));
+    RTM_TRY(shift_factors(cy, 0, &v, &f));
+    k_circulant_invert<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(cx, cy, out.content, raw.as<double2>(), u, v,
+                                                                   1.0 / (size_x * size_x), 1.0 / (size_y * size_y),
+                                                                   1.0 / (size_x * size_y), inv.as<double2>(),
+                                                                   flag.as<int>());
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    int bad = 0;
+    RTM_CUDA(cudaMemcpyAsync(&bad, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    if (bad)
+        return fail(RTM_ERR_SINGULAR, "The circulant approximation is singular at some frequency. Use another kernel "
+                                      "or builder.");
+    if (out.content == RTM_BOTH) {
+        out.mode = kBlock4;
+        RTM_TRY(convert_spectra(inv, precision, out.spec, s));
+        out.spec_blocks = 4;
+        out.max_rhs = 0;
+        RTM_TRY(out.reserve(1));
+    } else {
+        // A strip: 1-D FFT of the face line with the single inverted block (FFTApplicator.m:52-59).
+        out.mode = kStrip;
+        const bool xs = out.content == RTM_XONLY;
+        const int L = xs ? cx : cy;
+        DeviceBuffer line;
+        RTM_TRY(line.alloc((size_t)L * sizeof(double2)));
+        RTM_CUDA(cudaMemcpyAsync(line.ptr, inv.as<double2>() + (xs ? 0 : 3 * G), L * sizeof(double2),
+                                 cudaMemcpyDeviceToDevice, s));
+        RTM_TRY(convert_spectra(line, precision, out.spec, s));
+        out.spec_blocks = 1;
+        out.P = L;
+        out.Q = 1;
+        out.nsx = 1;
+        out.nsy = 1;
+        RTM_TRY(fft_tables(L, &out.tP));
+        RTM_TRY(fft_tables(1, &out.tQ));
+        out.max_rhs = 1 << 20;  // a strip needs no working grid
+    }
+    RTM_CUDA(cudaStreamSynchronize(s));
+    return RTM_OK;
+}
+
+__global__ void k_modify(int64_t n, const double2* __restrict__ in, double2* __restrict__ out, int modifier) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = in[i];
+        out[i] = modifier == RTM_MODIFY_REAL ? make_double2(v.x, 0.0)
+                 : modifier == RTM_MODIFY_IMAG ? make_double2(v.y, 0.0) : v;
+    }
+}
+
+int modify_generators(const DeviceGenerators& in, int modifier, DeviceGenerators& out, cudaStream_t s) {
+    out.count_x = in.count_x;
+    out.count_y = in.count_y;
+    out.content = in.content;
+    out.is_real = in.is_real || modifier != RTM_MODIFY_NONE;
+    const DeviceBuffer* src[3] = {&in.xx, &in.yy, &in.e};
+    DeviceBuffer* dst[3] = {&out.xx, &out.yy, &out.e};
+    for (int k = 0; k < 3; ++k) {
+        if (!src[k]->ptr) continue;
+        RTM_TRY(dst[k]->alloc(src[k]->bytes));
+        const int64_t n = (int64_t)(src[k]->bytes / sizeof(double2));
+        k_modify<<<256, 256, 0, s>>>(n, src[k]->as<double2>(), dst[k]->as<double2>(), modifier);
+        count_launch();
+        RTM_CUDA(cudaGetLastError());
+    }
+    RTM_CUDA(cudaStreamSynchronize(s));
+    return RTM_OK;
+}
+
+}  // namespace rtm

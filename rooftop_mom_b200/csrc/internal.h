@@ -1,0 +1,93 @@
+// Internal declarations shared by the CUDA and C++ sources of librtm.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rtm.h"
+
+namespace rtm {
+
+// ---------------------------------------------------------------------------------------------
+// Errors: every entry point returns a status and records a thread-local message.
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define RTM_CUDA(call)                                        \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return ::rtm::cuda_fail(e_, #call); \
+    } while (0)
+
+#define RTM_TRY(call)                   \
+    do {                                \
+        int s_ = (call);                \
+        if (s_ != RTM_OK) return s_;    \
+    } while (0)
+
+extern int64_t g_launches;  // launches of this library's kernels (incremented by the launchers)
+inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (int64_t)n, __ATOMIC_RELAXED); }
+
+// ---------------------------------------------------------------------------------------------
+// Budget ledger of device bytes (Budget.m). Thread-safe.
+int budget_require(double bytes, const char* what);
+void budget_hold(double bytes);
+void budget_release(double bytes);
+
+// Device buffer owned by a handle; its bytes are held in the budget while it lives.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { reset(); }
+    int alloc(size_t n);
+    void reset();
+    template <typename T> T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+// ---------------------------------------------------------------------------------------------
+// FFT plans: a length n factorised into radices; twiddle tables exp(-2 pi i m / n), m < n, in
+// FP64 and FP32, computed on the host in long double and kept on the device for the life of the
+// process (one table per length and device).
+constexpr int kMaxStages = 20;
+constexpr int kMaxGenericRadix = 64;  // largest prime factor this build transforms
+
+struct FftPlan {
+    int n;
+    int nstages;
+    int radix[kMaxStages];
+};
+
+struct FftTables {
+    FftPlan plan;
+    const double2* tw64;   // n entries
+    const float2* tw32;
+    const double2* mod64;  // exp(-i pi d / n), d < n (the odd-subband modulation)
+    const float2* mod32;
+};
+
+// Returns the cached tables of length n on the current device (RTM_ERR_UNSUPPORTED if n has a
+// prime factor above kMaxGenericRadix).
+int fft_tables(int n, const FftTables** out);
+
+// Shift-phase factors of generateShiftPhases.m: u(m) = 1 - exp(i pi (2m + parity) / n).
+int shift_factors(int n, int parity, const double2** out64, const float2** out32);
+
+template <typename T> struct Cx;
+template <> struct Cx<double> { using T2 = double2; };
+template <> struct Cx<float> { using T2 = float2; };
+
+// Host FP64 helpers used by the assembler set-up.
+void gauss_legendre(int order, double a, double b, std::vector<double>& points, std::vector<double>& weights);
+void power_moments(double size_x, double size_y, int power, double out[7][4]);
+void extracted_moments(double size_x, double size_y, double k, double out[7][4]);
+
+int fast_fft_size(int count);
+
+}  // namespace rtm

@@ -1,0 +1,1032 @@
+// COCG, preconditioned COCG and restarted left-preconditioned GMRES on the device.
+//
+// Follows the reference's
+//   src/+rooftopMoM/+solver/IterativeMethod.m:27-70        (zero right-hand side, true residual)
+//   src/+rooftopMoM/+solver/ConjugateGradient.m:12-62       (COCG: r^T z, alpha = rho / d^T A d)
+//   src/+rooftopMoM/+solver/PreconditionedConjugateGradient.m:18-23
+//   src/+rooftopMoM/+solver/@GeneralizedMinimumResidual/iterate_.m:1-85
+//   src/+rooftopMoM/+solver/@GeneralizedMinimumResidual/private/orthogonalize_.m:15-23 (CGS2)
+//   src/+rooftopMoM/+solver/@GeneralizedMinimumResidual/private/generateRotation_.m:11-18
+//
+// Every scalar of an iteration lives on the device. Each reduction is one kernel whose last CTA to
+// arrive (atomic counter, no waiting) sums the per-CTA partials in a fixed order and updates the
+// solver state, so results do not depend on scheduling. Every kernel of an iteration first reads
+// the state of its right-hand side and does nothing once that solve is done; the host launches
+// `check_every` iterations, then reads the done flags once. Converged systems thus stop exactly at
+// the reference's iteration, and the extra launched iterations are no-ops.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fft.cuh"
+#include "krylov.h"
+
+namespace rtm {
+
+constexpr int kRT = 256;  // threads of the vector kernels
+
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
+template <typename T2> __device__ __forceinline__ T2 from_d2(double2 v);
+template <> __device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 from_d2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ double2 dmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 dmulc(double2 a, double2 b) {  // conj(a) * b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double dabs(double2 a) { return hypot(a.x, a.y); }
+
+// Sums K double2 values over the CTA into out[0..K-1] (thread 0..K-1 write).
+template <int K> __device__ __forceinline__ void block_sum(double2 (&v)[K], double2* out) {
+    __shared__ double2 sm[K][kRT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double r = v[k].x, i = v[k].y;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, o);
+            i += __shfl_down_sync(0xffffffffu, i, o);
+        }
+        if (lane == 0) sm[k][warp] = make_double2(r, i);
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double2 s = make_double2(0, 0);
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s = dadd(s, sm[threadIdx.x][w]);
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Returns true in the last CTA of this right-hand side to arrive; its partials are then visible.
+__device__ __forceinline__ bool arrive(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int prev = atomicAdd(counter, 1u);
+        last = prev == gridDim.x - 1;
+        if (last) *counter = 0;  // ready for the next reduction
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// ============================================================================================
+// COCG
+struct CgState {
+    double2 rho, beta, alpha;
+    double bnorm, tol;
+    int iteration, max_iterations;
+    int done;        // nonzero: this solve is finished (also the operators' skip flag)
+    int converged;
+    int zero_rhs;
+    unsigned int counter;
+};
+
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_cg_start(const T2* __restrict__ b, const T2* __restrict__ r, int64_t n,
+                                                  CgState* st, double2* part, double* hist, int hist_stride) {
+    const int rhs = blockIdx.y;
+    const T2* br = b + rhs * n;
+    const T2* rr = r + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 bv = to_d2(br[i]), rv = to_d2(rr[i]);
+        acc[0].x += bv.x * bv.x + bv.y * bv.y;
+        acc[0].y += rv.x * rv.x + rv.y * rv.y;
+    }
+    double2* mine = part + ((int64_t)rhs * gridDim.x + blockIdx.x);
+    block_sum<1>(acc, mine);
+    if (!arrive(&st[rhs].counter)) return;
+    if (threadIdx.x == 0) {
+        double2 s = make_double2(0, 0);
+        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
+        CgState& S = st[rhs];
+        S.bnorm = sqrt(s.x);
+        S.iteration = 0;
+        S.rho = S.beta = S.alpha = make_double2(0, 0);
+        if (S.bnorm == 0.0) {
+            // IterativeMethod.m:53-56: the solution of a zero right-hand side is zero.
+            S.zero_rhs = 1;
+            S.converged = 1;
+            S.done = 1;
+            hist[(int64_t)rhs * hist_stride] = 0.0;
+            return;
+        }
+        S.zero_rhs = 0;
+        const double h0 = sqrt(s.y) / S.bnorm;
+        hist[(int64_t)rhs * hist_stride] = h0;
+        S.converged = h0 < S.tol;
+        S.done = S.converged || S.max_iterations <= 0;
+    }
+}
+
+// rho = r^T z (no conjugate); beta = rho / rho_previous from the second iteration on.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_cg_rz(const T2* __restrict__ r, const T2* __restrict__ z, int64_t n,
+                                               CgState* st, double2* part) {
+    const int rhs = blockIdx.y;
+    if (st[rhs].done) return;
+    const T2* rr = r + rhs * n;
+    const T2* zr = z + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc[0] = dadd(acc[0], dmul(to_d2(rr[i]), to_d2(zr[i])));
+    block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
+    if (!arrive(&st[rhs].counter)) return;
+    if (threadIdx.x == 0) {
+        double2 s = make_double2(0, 0);
+        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
+        CgState& S = st[rhs];
+        S.beta = S.iteration == 0 ? make_double2(0, 0) : ddiv(s, S.rho);
+        S.rho = s;
+    }
+}
+
+// d = z + beta d (d = z in the first iteration).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_cg_dir(const T2* __restrict__ z, T2* __restrict__ d, int64_t n,
+                                                const CgState* st) {
+    const int rhs = blockIdx.y;
+    const CgState& S = st[rhs];
+    if (S.done) return;
+    const T2* zr = z + rhs * n;
+    T2* dr = d + rhs * n;
+    const bool first = S.iteration == 0;
+    const double2 beta = S.beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 zv = to_d2(zr[i]);
+        dr[i] = first ? zr[i] : from_d2<T2>(dadd(zv, dmul(beta, to_d2(dr[i]))));
+    }
+}
+
+// alpha = rho / (d^T q).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_cg_dq(const T2* __restrict__ d, const T2* __restrict__ q, int64_t n,
+                                               CgState* st, double2* part) {
+    const int rhs = blockIdx.y;
+    if (st[rhs].done) return;
+    const T2* dr = d + rhs * n;
+    const T2* qr = q + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc[0] = dadd(acc[0], dmul(to_d2(dr[i]), to_d2(qr[i])));
+    block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
+    if (!arrive(&st[rhs].counter)) return;
+    if (threadIdx.x == 0) {
+        double2 s = make_double2(0, 0);
+        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
+        st[rhs].alpha = ddiv(st[rhs].rho, s);
+    }
+}
+
+// x += alpha d, r -= alpha q, then the relative residual, the history and the stopping tests.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_cg_update(T2* __restrict__ x, T2* __restrict__ r, const T2* __restrict__ d,
+                                                   const T2* __restrict__ q, int64_t n, CgState* st, double2* part,
+                                                   double* hist, int hist_stride) {
+    const int rhs = blockIdx.y;
+    if (st[rhs].done) return;
+    const double2 alpha = st[rhs].alpha;
+    T2* xr = x + rhs * n;
+    T2* rr = r + rhs * n;
+    const T2* dr = d + rhs * n;
+    const T2* qr = q + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 xv = dadd(to_d2(xr[i]), dmul(alpha, to_d2(dr[i])));
+        const double2 aq = dmul(alpha, to_d2(qr[i]));
+        const double2 rv0 = to_d2(rr[i]);
+        const double2 rv = make_double2(rv0.x - aq.x, rv0.y - aq.y);
+        const T2 rs = from_d2<T2>(rv);
+        xr[i] = from_d2<T2>(xv);
+        rr[i] = rs;
+        const double2 rd = to_d2(rs);
+        acc[0].x += rd.x * rd.x + rd.y * rd.y;
+    }
+    block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
+    if (!arrive(&st[rhs].counter)) return;
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < (int)gridDim.x; ++k) s += part[(int64_t)rhs * gridDim.x + k].x;
+        CgState& S = st[rhs];
+        S.iteration += 1;
+        const double h = sqrt(s) / S.bnorm;
+        hist[(int64_t)rhs * hist_stride + S.iteration] = h;
+        S.converged = h < S.tol;
+        // A breakdown (d^T A d = 0) leaves Inf or NaN (ConjugateGradient.m:55-58).
+        S.done = S.converged || !isfinite(h) || S.iteration >= S.max_iterations;
+    }
+}
+
+// ============================================================================================
+// GMRES
+struct GmState {
+    double ref;       // || P b ||
+    double rn;        // norm of the residual a cycle starts from
+    double tol;
+    double inv_sub;
+    int iteration, max_iterations, m, step;
+    int active;       // inside a cycle
+    int skip_step;    // = !active: the operators' skip flag within a cycle
+    int done;         // converged or out of iterations: the skip flag of the restart
+    int converged;
+    int zero_rhs;
+    int cycle_ran;
+    unsigned int counter;
+};
+
+struct GmArrays {
+    double2* H;      // [rhs][(m+1) * m], column-major
+    double2* g;      // [rhs][m+1]
+    double2* cs;     // [rhs][m]
+    double2* sn;     // [rhs][m]
+    double2* h;      // [rhs][m+1] accumulated Gram-Schmidt coefficients
+    double2* c;      // [rhs][m+1] coefficients of the current pass
+    double2* y;      // [rhs][m]
+    double2* part;   // [rhs][blocks][m+1]
+    double* hist;
+    int hist_stride;
+    int m;
+};
+
+// ||w||: mode 0 sets ref = ||P b||; mode 1 starts a cycle from w (first: the history's first entry).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_norm(const T2* __restrict__ w, int64_t n, GmState* st, GmArrays ar,
+                                                 int mode, int first) {
+    const int rhs = blockIdx.y;
+    GmState& S = st[rhs];
+    if (mode == 1 && S.done) return;
+    const T2* wr = w + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = to_d2(wr[i]);
+        acc[0].x += v.x * v.x + v.y * v.y;
+    }
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
+    block_sum<1>(acc, part + blockIdx.x);
+    if (!arrive(&S.counter)) return;
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < (int)gridDim.x; ++k) s += part[k].x;
+        const double nrm = sqrt(s);
+        if (mode == 0) {
+            S.ref = nrm;
+            S.iteration = 0;
+            S.zero_rhs = nrm == 0.0;
+            S.done = S.zero_rhs;
+            S.converged = S.zero_rhs;
+            S.active = 0;
+            S.skip_step = 1;
+            if (S.zero_rhs) ar.hist[(int64_t)rhs * ar.hist_stride] = 0.0;
+            return;
+        }
+        S.rn = nrm;
+        if (first) {
+            const double h0 = nrm / S.ref;
+            ar.hist[(int64_t)rhs * ar.hist_stride] = h0;
+            S.converged = h0 < S.tol;
+            S.done = S.converged || S.max_iterations <= 0;
+        }
+        double2* g = ar.g + (int64_t)rhs * (ar.m + 1);
+        for (int k = 0; k <= ar.m; ++k) g[k] = make_double2(0, 0);
+        g[0] = make_double2(nrm, 0);
+        S.step = 0;
+        S.active = !S.done;
+        S.skip_step = !S.active;
+        S.cycle_ran = S.active;
+    }
+}
+
+// V[:, 0] = w / rn.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_v0(const T2* __restrict__ w, T2* __restrict__ V, int64_t n, int nrhs,
+                                               const GmState* st) {
+    const int rhs = blockIdx.y;
+    const GmState& S = st[rhs];
+    if (!S.active) return;
+    const double inv = 1.0 / S.rn;
+    const T2* wr = w + rhs * n;
+    T2* v0 = V + (int64_t)rhs * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = to_d2(wr[i]);
+        v0[i] = from_d2<T2>(make_double2(v.x * inv, v.y * inv));
+    }
+}
+
+// c_k = V_k^H w for k <= step (pass 0: h = c; pass 1: h += c).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_dot(const T2* __restrict__ V, const T2* __restrict__ w, int64_t n, int nrhs,
+                                                GmState* st, GmArrays ar, int pass) {
+    const int rhs = blockIdx.y;
+    GmState& S = st[rhs];
+    if (!S.active) return;
+    const int cols = S.step + 1;
+    const T2* wr = w + rhs * n;
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
+    for (int k0 = 0; k0 < cols; k0 += 8) {
+        double2 acc[8];
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) acc[kk] = make_double2(0, 0);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const double2 wv = to_d2(wr[i]);
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                if (k0 + kk < cols) {
+                    const double2 v = to_d2(V[((int64_t)(k0 + kk) * nrhs + rhs) * n + i]);
+                    acc[kk] = dadd(acc[kk], dmulc(v, wv));
+                }
+            }
+        }
+        double2 out[8];
+        block_sum<8>(acc, out);
+        if (threadIdx.x < 8 && k0 + threadIdx.x < cols)
+            part[(int64_t)blockIdx.x * (ar.m + 1) + k0 + threadIdx.x] = out[threadIdx.x];
+    }
+    if (!arrive(&S.counter)) return;
+    for (int k = threadIdx.x; k < cols; k += blockDim.x) {
+        double2 s = make_double2(0, 0);
+        for (int b = 0; b < (int)gridDim.x; ++b) s = dadd(s, part[(int64_t)b * (ar.m + 1) + k]);
+        double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
+        ar.c[(int64_t)rhs * (ar.m + 1) + k] = s;
+        h[k] = pass == 0 ? s : dadd(h[k], s);
+    }
+}
+
+// w -= V c; with finish, also ||w|| and the rest of the Arnoldi step: the Hessenberg column, its
+// rotations, the new rotation, the rotated right-hand side, the history and the stopping tests.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_update(T2* __restrict__ w, const T2* __restrict__ V, int64_t n, int nrhs,
+                                                   GmState* st, GmArrays ar, int finish) {
+    const int rhs = blockIdx.y;
+    GmState& S = st[rhs];
+    if (!S.active) return;
+    const int cols = S.step + 1;
+    const double2* c = ar.c + (int64_t)rhs * (ar.m + 1);
+    T2* wr = w + rhs * n;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = to_d2(wr[i]);
+        for (int k = 0; k < cols; ++k) {
+            const double2 p = dmul(to_d2(V[((int64_t)k * nrhs + rhs) * n + i]), c[k]);
+            v.x -= p.x;
+            v.y -= p.y;
+        }
+        const T2 vs = from_d2<T2>(v);
+        wr[i] = vs;
+        const double2 vd = to_d2(vs);
+        acc[0].x += vd.x * vd.x + vd.y * vd.y;
+    }
+    if (!finish) return;
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
+    block_sum<1>(acc, part + blockIdx.x);
+    if (!arrive(&S.counter)) return;
+    if (threadIdx.x != 0) return;
+    double s = 0;
+    for (int k = 0; k < (int)gridDim.x; ++k) s += part[k].x;
+    const double sub = sqrt(s);
+    const int m = ar.m, j = S.step;
+    double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
+    double2* g = ar.g + (int64_t)rhs * (m + 1);
+    double2* cs = ar.cs + (int64_t)rhs * m;
+    double2* sn = ar.sn + (int64_t)rhs * m;
+    const double2* h = ar.h + (int64_t)rhs * (m + 1);
+    double2* col = H + (int64_t)j * (m + 1);
+    for (int k = 0; k <= j; ++k) col[k] = h[k];
+    col[j + 1] = make_double2(sub, 0);
+    for (int k = 0; k < j; ++k) {
+        const double2 a0 = col[k], a1 = col[k + 1];
+        col[k] = dadd(dmulc(cs[k], a0), dmulc(sn[k], a1));
+        const double2 t = dmul(sn[k], a0);
+        const double2 u = dmul(cs[k], a1);
+        col[k + 1] = make_double2(u.x - t.x, u.y - t.y);
+    }
+    // generateRotation_.m:11-18
+    const double2 a = col[j], bsub = col[j + 1];
+    const double radius = sqrt(a.x * a.x + a.y * a.y + bsub.x * bsub.x + bsub.y * bsub.y);
+    double2 cj = make_double2(1, 0), sj = make_double2(0, 0);
+    if (radius > 0) {
+        cj = make_double2(a.x / radius, a.y / radius);
+        sj = make_double2(bsub.x / radius, bsub.y / radius);
+    }
+    cs[j] = cj;
+    sn[j] = sj;
+    col[j] = dadd(dmulc(cj, a), dmulc(sj, bsub));
+    col[j + 1] = make_double2(0, 0);
+    const double2 gj = g[j];
+    const double2 t = dmul(sj, gj);
+    g[j + 1] = make_double2(-t.x, -t.y);
+    g[j] = dmulc(cj, gj);
+    S.iteration += 1;
+    const double hres = dabs(g[j + 1]) / S.ref;
+    ar.hist[(int64_t)rhs * ar.hist_stride + S.iteration] = hres;
+    S.converged = hres < S.tol;
+    S.step = j + 1;
+    S.inv_sub = sub != 0 ? 1.0 / sub : 0.0;
+    const bool more = !S.converged && sub != 0 && S.step < m && S.iteration < S.max_iterations;
+    // A zero subdiagonal means the basis spans the solution (iterate_.m:65-68).
+    S.active = more;
+    S.skip_step = !more;
+    S.done = S.converged || S.iteration >= S.max_iterations;
+}
+
+// V[:, step] = w / H(step, step - 1) while the cycle goes on.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_next(const T2* __restrict__ w, T2* __restrict__ V, int64_t n, int nrhs,
+                                                 const GmState* st) {
+    const int rhs = blockIdx.y;
+    const GmState& S = st[rhs];
+    if (!S.active) return;
+    const double inv = S.inv_sub;
+    const T2* wr = w + rhs * n;
+    T2* v = V + ((int64_t)S.step * nrhs + rhs) * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 x = to_d2(wr[i]);
+        v[i] = from_d2<T2>(make_double2(x.x * inv, x.y * inv));
+    }
+}
+
+// y = H(1:step, 1:step) \ g(1:step) (upper triangular after the rotations; iterate_.m:73-74).
+__global__ void k_gm_solve(GmState* st, GmArrays ar, int nrhs) {
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs) return;
+    GmState& S = st[rhs];
+    if (!S.cycle_ran) return;
+    const int m = ar.m, k = S.step;
+    const double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
+    const double2* g = ar.g + (int64_t)rhs * (m + 1);
+    double2* y = ar.y + (int64_t)rhs * m;
+    for (int i = k - 1; i >= 0; --i) {
+        double2 s = g[i];
+        for (int l = i + 1; l < k; ++l) {
+            const double2 p = dmul(H[(int64_t)l * (m + 1) + i], y[l]);
+            s.x -= p.x;
+            s.y -= p.y;
+        }
+        y[i] = ddiv(s, H[(int64_t)i * (m + 1) + i]);
+    }
+}
+
+// x += V(:, 1:step) y.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_xupdate(T2* __restrict__ x, const T2* __restrict__ V, int64_t n, int nrhs,
+                                                    GmState* st, GmArrays ar) {
+    const int rhs = blockIdx.y;
+    const GmState& S = st[rhs];
+    if (!S.cycle_ran) return;
+    const int k = S.step;
+    const double2* y = ar.y + (int64_t)rhs * ar.m;
+    T2* xr = x + rhs * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = to_d2(xr[i]);
+        for (int l = 0; l < k; ++l) v = dadd(v, dmul(to_d2(V[((int64_t)l * nrhs + rhs) * n + i]), y[l]));
+        xr[i] = from_d2<T2>(v);
+    }
+}
+
+__global__ void k_gm_cycle_end(GmState* st, int nrhs) {
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs) return;
+    st[rhs].cycle_ran = 0;
+    st[rhs].active = 0;
+    st[rhs].skip_step = 1;
+}
+
+// ============================================================================================
+// Shared helpers
+// out = b - t where flag (stride) is zero.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_residual(const T2* __restrict__ b, const T2* __restrict__ t, T2* __restrict__ out,
+                                                  int64_t n, const int* skip, int stride) {
+    const int rhs = blockIdx.y;
+    if (skip && skip[(int64_t)rhs * stride]) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 bv = to_d2(b[rhs * n + i]), tv = to_d2(t[rhs * n + i]);
+        out[rhs * n + i] = from_d2<T2>(make_double2(bv.x - tv.x, bv.y - tv.y));
+    }
+}
+
+// ||b - t||^2 and ||b||^2 per right-hand side into res[rhs] = (||b - t||, ||b||).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_true_residual(const T2* __restrict__ b, const T2* __restrict__ t, int64_t n,
+                                                       double2* part, unsigned int* counters, double2* res) {
+    const int rhs = blockIdx.y;
+    double2 acc[1] = {make_double2(0, 0)};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 bv = to_d2(b[rhs * n + i]), tv = to_d2(t[rhs * n + i]);
+        const double dx = bv.x - tv.x, dy = bv.y - tv.y;
+        acc[0].x += dx * dx + dy * dy;
+        acc[0].y += bv.x * bv.x + bv.y * bv.y;
+    }
+    block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
+    if (!arrive(&counters[rhs])) return;
+    if (threadIdx.x == 0) {
+        double2 s = make_double2(0, 0);
+        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
+        res[rhs] = make_double2(sqrt(s.x), sqrt(s.y));
+    }
+}
+
+template <typename T2>
+__global__ void k_zero_where(T2* __restrict__ x, int64_t n, const int* flag, int stride) {
+    const int rhs = blockIdx.y;
+    if (!flag[(int64_t)rhs * stride]) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[rhs * n + i] = from_d2<T2>(make_double2(0, 0));
+}
+
+__global__ void k_fill(double* p, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+__global__ void k_d2f(const double2* __restrict__ in, float2* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+__global__ void k_f2d(const float2* __restrict__ in, double2* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = make_double2(in[i].x, in[i].y);
+}
+
+void convert_to_fp32(const double2* in, float2* out, int64_t n, cudaStream_t s) {
+    k_d2f<<<592, 256, 0, s>>>(in, out, n);
+    count_launch();
+}
+void convert_to_fp64(const float2* in, double2* out, int64_t n, cudaStream_t s) {
+    k_f2d<<<592, 256, 0, s>>>(in, out, n);
+    count_launch();
+}
+
+static int reduce_blocks(int64_t n) {
+    const int64_t b = (n + (int64_t)kRT * 4 - 1) / ((int64_t)kRT * 4);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 296));
+}
+
+// ============================================================================================
+template <typename T>
+static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv, const void* x0v, void* xv, int64_t n,
+                int nrhs, SolveResult& res, cudaStream_t s) {
+    using T2 = typename Cx<T>::T2;
+    const T2* b = static_cast<const T2*>(bv);
+    const T2* x0 = static_cast<const T2*>(x0v);
+    T2* x = static_cast<T2*>(xv);
+    const int nb = reduce_blocks(n);
+    const size_t vec = (size_t)n * nrhs * sizeof(T2);
+    DeviceBuffer r, z, d, q, stb, part, hist, resb, cnt;
+    RTM_TRY(r.alloc(vec));
+    if (M) RTM_TRY(z.alloc(vec));
+    RTM_TRY(d.alloc(vec));
+    RTM_TRY(q.alloc(vec));
+    RTM_TRY(stb.alloc(sizeof(CgState) * nrhs));
+    RTM_TRY(part.alloc(sizeof(double2) * nb * nrhs));
+    const int hs = cfg.max_iterations + 1;
+    RTM_TRY(hist.alloc(sizeof(double) * hs * nrhs));
+    RTM_TRY(resb.alloc(sizeof(double2) * nrhs));
+    RTM_TRY(cnt.alloc(sizeof(unsigned int) * nrhs));
+    std::vector<CgState> init(nrhs);
+    for (auto& st : init) {
+        memset(&st, 0, sizeof st);
+        st.tol = cfg.tolerance;
+        st.max_iterations = cfg.max_iterations;
+    }
+    RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, s));
+    RTM_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes, s));
+    k_fill<<<64, 256, 0, s>>>(hist.as<double>(), (int64_t)hs * nrhs, NAN);
+    count_launch();
+    RTM_TRY(A->reserve(nrhs));
+    if (M) RTM_TRY(M->reserve(nrhs));
+    CgState* st = stb.as<CgState>();
+    SkipFlags skip{&st[0].done, (int)(sizeof(CgState) / sizeof(int))};
+    const dim3 grid(nb, nrhs);
+    if (x0) {
+        RTM_CUDA(cudaMemcpyAsync(x, x0, vec, cudaMemcpyDeviceToDevice, s));
+        RTM_TRY(A->apply(x, q.ptr, nrhs, s, SkipFlags{}));
+        k_residual<T2><<<grid, kRT, 0, s>>>(b, q.as<T2>(), r.as<T2>(), n, nullptr, 0);
+        count_launch();
+    } else {
+        RTM_CUDA(cudaMemsetAsync(x, 0, vec, s));
+        RTM_CUDA(cudaMemcpyAsync(r.ptr, b, vec, cudaMemcpyDeviceToDevice, s));
+    }
+    k_cg_start<T2><<<grid, kRT, 0, s>>>(b, r.as<T2>(), n, st, part.as<double2>(), hist.as<double>(), hs);
+    count_launch();
+    T2* zp = M ? z.as<T2>() : r.as<T2>();
+    const int every = cfg.check_every > 0 ? cfg.check_every : 16;
+    std::vector<CgState> host(nrhs);
+    int launched = 0;
+    res.matvecs = x0 ? 1 : 0;
+    while (true) {
+        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        bool all = true;
+        for (auto& h : host) all = all && h.done;
+        if (all || launched >= cfg.max_iterations) break;
+        const int chunk = std::min(every, cfg.max_iterations - launched);
+        for (int it = 0; it < chunk; ++it) {
+            if (M) RTM_TRY(M->apply(r.ptr, z.ptr, nrhs, s, skip));
+            k_cg_rz<T2><<<grid, kRT, 0, s>>>(r.as<T2>(), zp, n, st, part.as<double2>());
+            k_cg_dir<T2><<<grid, kRT, 0, s>>>(zp, d.as<T2>(), n, st);
+            RTM_TRY(A->apply(d.ptr, q.ptr, nrhs, s, skip));
+            k_cg_dq<T2><<<grid, kRT, 0, s>>>(d.as<T2>(), q.as<T2>(), n, st, part.as<double2>());
+            k_cg_update<T2><<<grid, kRT, 0, s>>>(x, r.as<T2>(), d.as<T2>(), q.as<T2>(), n, st, part.as<double2>(),
+                                                 hist.as<double>(), hs);
+            count_launch(4);
+        }
+        RTM_CUDA(cudaGetLastError());
+        launched += chunk;
+    }
+    // IterativeMethod.m:52: the true residual costs one more product.
+    RTM_TRY(A->apply(x, q.ptr, nrhs, s, SkipFlags{}));
+    k_zero_where<T2><<<grid, kRT, 0, s>>>(x, n, &st[0].zero_rhs, (int)(sizeof(CgState) / sizeof(int)));
+    k_true_residual<T2><<<grid, kRT, 0, s>>>(b, q.as<T2>(), n, part.as<double2>(), cnt.as<unsigned int>(),
+                                             resb.as<double2>());
+    count_launch(2);
+    std::vector<double2> rb(nrhs);
+    RTM_CUDA(cudaMemcpyAsync(rb.data(), resb.ptr, sizeof(double2) * nrhs, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, s));
+    res.history.resize((size_t)hs * nrhs);
+    RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    res.hist_stride = hs;
+    res.stats.resize(nrhs);
+    for (int k = 0; k < nrhs; ++k) {
+        rtm_solve_stats& o = res.stats[k];
+        o.converged = host[k].converged;
+        o.iteration_count = host[k].zero_rhs ? 0 : host[k].iteration;
+        o.residual_norm = host[k].zero_rhs ? 0.0 : rb[k].x / rb[k].y;
+        o.refinements = 0;
+        o.matvecs = res.matvecs + host[k].iteration + 1;
+    }
+    return RTM_OK;
+}
+
+template <typename T>
+static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv, const void* x0v, void* xv, int64_t n,
+                 int nrhs, SolveResult& res, cudaStream_t s) {
+    using T2 = typename Cx<T>::T2;
+    const T2* b = static_cast<const T2*>(bv);
+    const T2* x0 = static_cast<const T2*>(x0v);
+    T2* x = static_cast<T2*>(xv);
+    const int m = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)cfg.restart, n, (int64_t)cfg.max_iterations}));
+    const int nb = reduce_blocks(n);
+    const size_t vec = (size_t)n * nrhs * sizeof(T2);
+    DeviceBuffer V, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
+    RTM_TRY(V.alloc(vec * (m + 1)));
+    RTM_TRY(w.alloc(vec));
+    RTM_TRY(t.alloc(vec));
+    RTM_TRY(stb.alloc(sizeof(GmState) * nrhs));
+    RTM_TRY(H.alloc(sizeof(double2) * (m + 1) * m * nrhs));
+    RTM_TRY(g.alloc(sizeof(double2) * (m + 1) * nrhs));
+    RTM_TRY(cs.alloc(sizeof(double2) * m * nrhs));
+    RTM_TRY(sn.alloc(sizeof(double2) * m * nrhs));
+    RTM_TRY(h.alloc(sizeof(double2) * (m + 1) * nrhs));
+    RTM_TRY(c.alloc(sizeof(double2) * (m + 1) * nrhs));
+    RTM_TRY(y.alloc(sizeof(double2) * m * nrhs));
+    RTM_TRY(part.alloc(sizeof(double2) * (size_t)nb * (m + 1) * nrhs));
+    const int hs = cfg.max_iterations + 1;
+    RTM_TRY(hist.alloc(sizeof(double) * hs * nrhs));
+    RTM_TRY(resb.alloc(sizeof(double2) * nrhs));
+    RTM_TRY(cnt.alloc(sizeof(unsigned int) * nrhs));
+    RTM_CUDA(cudaMemsetAsync(H.ptr, 0, H.bytes, s));
+    RTM_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes, s));
+    std::vector<GmState> init(nrhs);
+    for (auto& st : init) {
+        memset(&st, 0, sizeof st);
+        st.tol = cfg.tolerance;
+        st.max_iterations = cfg.max_iterations;
+        st.m = m;
+        st.skip_step = 1;
+    }
+    RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(GmState) * nrhs, cudaMemcpyHostToDevice, s));
+    k_fill<<<64, 256, 0, s>>>(hist.as<double>(), (int64_t)hs * nrhs, NAN);
+    count_launch();
+    RTM_TRY(A->reserve(nrhs));
+    if (M) RTM_TRY(M->reserve(nrhs));
+    GmState* st = stb.as<GmState>();
+    GmArrays ar{H.as<double2>(), g.as<double2>(), cs.as<double2>(), sn.as<double2>(), h.as<double2>(),
+                c.as<double2>(), y.as<double2>(), part.as<double2>(), hist.as<double>(), hs, m};
+    const int stride = (int)(sizeof(GmState) / sizeof(int));
+    SkipFlags skip_step{&st[0].skip_step, stride};
+    SkipFlags skip_done{&st[0].done, stride};
+    const dim3 grid(nb, nrhs);
+    // reference = ||P b|| (iterate_.m:9)
+    if (M) RTM_TRY(M->apply(b, w.ptr, nrhs, s, SkipFlags{}));
+    else RTM_CUDA(cudaMemcpyAsync(w.ptr, b, vec, cudaMemcpyDeviceToDevice, s));
+    k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 0, 0);
+    count_launch();
+    res.matvecs = 0;
+    if (x0) {
+        RTM_CUDA(cudaMemcpyAsync(x, x0, vec, cudaMemcpyDeviceToDevice, s));
+        RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
+        k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
+        count_launch();
+        if (M) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
+        else RTM_CUDA(cudaMemcpyAsync(w.ptr, t.ptr, vec, cudaMemcpyDeviceToDevice, s));
+        res.matvecs += 1;
+    } else {
+        RTM_CUDA(cudaMemsetAsync(x, 0, vec, s));
+    }
+    k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 1);
+    count_launch();
+    std::vector<GmState> host(nrhs);
+    T2* Vp = V.as<T2>();
+    while (true) {
+        k_gm_v0<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
+        count_launch();
+        for (int j = 0; j < m; ++j) {
+            T2* vj = Vp + (int64_t)j * nrhs * n;
+            if (M) {
+                RTM_TRY(A->apply(vj, t.ptr, nrhs, s, skip_step));
+                RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_step));
+            } else {
+                RTM_TRY(A->apply(vj, w.ptr, nrhs, s, skip_step));
+            }
+            k_gm_dot<T2><<<grid, kRT, 0, s>>>(Vp, w.as<T2>(), n, nrhs, st, ar, 0);
+            k_gm_update<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st, ar, 0);
+            k_gm_dot<T2><<<grid, kRT, 0, s>>>(Vp, w.as<T2>(), n, nrhs, st, ar, 1);
+            k_gm_update<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st, ar, 1);
+            k_gm_next<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
+            count_launch(5);
+            RTM_CUDA(cudaGetLastError());
+            if (cfg.check_every > 0 && (j + 1) % cfg.check_every == 0 && j + 1 < m) {
+                RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
+                RTM_CUDA(cudaStreamSynchronize(s));
+                bool any = false;
+                for (auto& hh : host) any = any || hh.active;
+                if (!any) break;
+            }
+        }
+        k_gm_solve<<<(nrhs + 31) / 32, 32, 0, s>>>(st, ar, nrhs);
+        k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, Vp, n, nrhs, st, ar);
+        k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
+        count_launch(3);
+        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        bool all = true;
+        for (auto& hh : host) all = all && hh.done;
+        if (all) break;
+        // The next cycle starts from the true residual (iterate_.m:77-81).
+        RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
+        k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
+        count_launch();
+        if (M) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
+        else RTM_CUDA(cudaMemcpyAsync(w.ptr, t.ptr, vec, cudaMemcpyDeviceToDevice, s));
+        k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 0);
+        count_launch();
+        res.matvecs += 1;
+    }
+    RTM_TRY(A->apply(x, t.ptr, nrhs, s, SkipFlags{}));
+    k_zero_where<T2><<<grid, kRT, 0, s>>>(x, n, &st[0].zero_rhs, stride);
+    k_true_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), n, part.as<double2>(), cnt.as<unsigned int>(),
+                                             resb.as<double2>());
+    count_launch(2);
+    std::vector<double2> rb(nrhs);
+    RTM_CUDA(cudaMemcpyAsync(rb.data(), resb.ptr, sizeof(double2) * nrhs, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
+    res.history.resize((size_t)hs * nrhs);
+    RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    res.hist_stride = hs;
+    res.stats.resize(nrhs);
+    for (int k = 0; k < nrhs; ++k) {
+        rtm_solve_stats& o = res.stats[k];
+        o.converged = host[k].converged;
+        o.iteration_count = host[k].zero_rhs ? 0 : host[k].iteration;
+        o.residual_norm = host[k].zero_rhs ? 0.0 : rb[k].x / rb[k].y;
+        o.refinements = 0;
+        o.matvecs = res.matvecs + host[k].iteration + 1;
+    }
+    return RTM_OK;
+}
+
+// ============================================================================================
+// Mixed precision: FP64 iterative refinement around an FP32 inner solve.
+//   r = b - A64 x (FP64); r32 = r / ||r||; d32 ~ A32^-1 r32 (one FP32 FGMRES cycle, or FP32 COCG);
+//   x += ||r|| d32; repeat until ||b - A64 x|| / ||b|| < tolerance. The outer residual is always
+//   the true FP64 residual, so the stopping test holds for the FP64 operator.
+
+__global__ void k_ir_to32(const double2* __restrict__ r, float2* __restrict__ r32, int64_t n, const double2* res,
+                          const int* done) {
+    const int rhs = blockIdx.y;
+    const bool off = done[rhs] != 0;
+    const double inv = off ? 0.0 : 1.0 / res[rhs].x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = r[rhs * n + i];
+        r32[rhs * n + i] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+    }
+}
+
+__global__ void k_ir_update(double2* __restrict__ x, const float2* __restrict__ d, int64_t n, const double2* res,
+                            const int* done) {
+    const int rhs = blockIdx.y;
+    if (done[rhs]) return;
+    const double s = res[rhs].x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = d[rhs * n + i];
+        double2 xv = x[rhs * n + i];
+        xv.x += s * v.x;
+        xv.y += s * v.y;
+        x[rhs * n + i] = xv;
+    }
+}
+
+// res = (||r||, ||b||): history entry and stopping test of refinement step `step`.
+__global__ void k_ir_check(const double2* res, int* done, int* converged, double* hist, int hist_stride, int step,
+                           double tol, int nrhs) {
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs || done[rhs]) return;
+    const double2 v = res[rhs];
+    const double rel = v.y == 0.0 ? 0.0 : v.x / v.y;
+    if (step < hist_stride) hist[(int64_t)rhs * hist_stride + step] = rel;
+    converged[rhs] = rel < tol;
+    done[rhs] = converged[rhs] || !isfinite(rel);
+}
+
+// One FGMRES(m) cycle in FP32 from x = 0 for the right-hand sides r32 (right preconditioning, the
+// preconditioned directions z_j = M v_j are kept, x = Z y). Returns the inner iterations done.
+static int fgmres_cycle(LinearOp* A, LinearOp* M, const float2* r32, float2* x32, int64_t n, int nrhs, int m,
+                        double tol, DeviceBuffer& V, DeviceBuffer& Z, DeviceBuffer& w, DeviceBuffer& stb,
+                        GmArrays& ar, std::vector<GmState>& host, cudaStream_t s) {
+    const int nb = reduce_blocks(n);
+    const dim3 grid(nb, nrhs);
+    std::vector<GmState> init(nrhs);
+    for (auto& st : init) {
+        memset(&st, 0, sizeof st);
+        st.tol = tol;
+        st.max_iterations = m;
+        st.m = m;
+        st.skip_step = 1;
+    }
+    RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(GmState) * nrhs, cudaMemcpyHostToDevice, s));
+    GmState* st = stb.as<GmState>();
+    const int stride = (int)(sizeof(GmState) / sizeof(int));
+    SkipFlags skip_step{&st[0].skip_step, stride};
+    const size_t vec = (size_t)n * nrhs * sizeof(float2);
+    RTM_CUDA(cudaMemcpyAsync(w.ptr, r32, vec, cudaMemcpyDeviceToDevice, s));
+    RTM_CUDA(cudaMemsetAsync(x32, 0, vec, s));
+    k_gm_norm<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), n, st, ar, 0, 0);
+    k_gm_norm<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), n, st, ar, 1, 1);
+    k_gm_v0<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), V.as<float2>(), n, nrhs, st);
+    count_launch(3);
+    float2* Vp = V.as<float2>();
+    float2* Zp = M ? Z.as<float2>() : Vp;
+    for (int j = 0; j < m; ++j) {
+        float2* vj = Vp + (int64_t)j * nrhs * n;
+        float2* zj = Zp + (int64_t)j * nrhs * n;
+        if (M) RTM_TRY(M->apply(vj, zj, nrhs, s, skip_step));
+        RTM_TRY(A->apply(zj, w.ptr, nrhs, s, skip_step));
+        k_gm_dot<float2><<<grid, kRT, 0, s>>>(Vp, w.as<float2>(), n, nrhs, st, ar, 0);
+        k_gm_update<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st, ar, 0);
+        k_gm_dot<float2><<<grid, kRT, 0, s>>>(Vp, w.as<float2>(), n, nrhs, st, ar, 1);
+        k_gm_update<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st, ar, 1);
+        k_gm_next<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st);
+        count_launch(5);
+        RTM_CUDA(cudaGetLastError());
+    }
+    k_gm_solve<<<(nrhs + 31) / 32, 32, 0, s>>>(st, ar, nrhs);
+    k_gm_xupdate<float2><<<grid, kRT, 0, s>>>(x32, Zp, n, nrhs, st, ar);
+    k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
+    count_launch(3);
+    RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    int most = 0;
+    for (auto& h : host) most = std::max(most, h.iteration);
+    return most;
+}
+
+int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& cfg, const void* bv, const void* x0v,
+                void* xv, int64_t n, int nrhs, SolveResult& res, cudaStream_t s) {
+    const double2* b = static_cast<const double2*>(bv);
+    const double2* x0 = static_cast<const double2*>(x0v);
+    double2* x = static_cast<double2*>(xv);
+    const int nb = reduce_blocks(n);
+    const dim3 grid(nb, nrhs);
+    const size_t vec64 = (size_t)n * nrhs * sizeof(double2), vec32 = (size_t)n * nrhs * sizeof(float2);
+    const int m = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)cfg.restart, n));
+    DeviceBuffer r64, t64, r32, d32, part, resb, cnt, done, conv, hist;
+    RTM_TRY(r64.alloc(vec64));
+    RTM_TRY(t64.alloc(vec64));
+    RTM_TRY(r32.alloc(vec32));
+    RTM_TRY(d32.alloc(vec32));
+    RTM_TRY(part.alloc(sizeof(double2) * (size_t)nb * (m + 1) * nrhs));
+    RTM_TRY(resb.alloc(sizeof(double2) * nrhs));
+    RTM_TRY(cnt.alloc(sizeof(unsigned int) * nrhs));
+    RTM_TRY(done.alloc(sizeof(int) * nrhs));
+    RTM_TRY(conv.alloc(sizeof(int) * nrhs));
+    const int hs = cfg.max_iterations + 1;
+    RTM_TRY(hist.alloc(sizeof(double) * hs * nrhs));
+    RTM_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes, s));
+    RTM_CUDA(cudaMemsetAsync(done.ptr, 0, done.bytes, s));
+    RTM_CUDA(cudaMemsetAsync(conv.ptr, 0, conv.bytes, s));
+    k_fill<<<64, 256, 0, s>>>(hist.as<double>(), (int64_t)hs * nrhs, NAN);
+    count_launch();
+    RTM_TRY(A64->reserve(nrhs));
+    RTM_TRY(A32->reserve(nrhs));
+    if (M32) RTM_TRY(M32->reserve(nrhs));
+    // FGMRES buffers (inner state, FP32 basis and preconditioned directions).
+    DeviceBuffer V, Z, w, stb, H, g, cs, sn, h, c, y, ipart, ihist;
+    const bool inner_cg = cfg.method == RTM_METHOD_CG;
+    GmArrays ar{};
+    std::vector<GmState> ghost(nrhs);
+    if (!inner_cg) {
+        RTM_TRY(V.alloc(vec32 * (m + 1)));
+        if (M32) RTM_TRY(Z.alloc(vec32 * m));
+        RTM_TRY(w.alloc(vec32));
+        RTM_TRY(stb.alloc(sizeof(GmState) * nrhs));
+        RTM_TRY(H.alloc(sizeof(double2) * (m + 1) * m * nrhs));
+        RTM_TRY(g.alloc(sizeof(double2) * (m + 1) * nrhs));
+        RTM_TRY(cs.alloc(sizeof(double2) * m * nrhs));
+        RTM_TRY(sn.alloc(sizeof(double2) * m * nrhs));
+        RTM_TRY(h.alloc(sizeof(double2) * (m + 1) * nrhs));
+        RTM_TRY(c.alloc(sizeof(double2) * (m + 1) * nrhs));
+        RTM_TRY(y.alloc(sizeof(double2) * m * nrhs));
+        RTM_TRY(ipart.alloc(sizeof(double2) * (size_t)nb * (m + 1) * nrhs));
+        RTM_TRY(ihist.alloc(sizeof(double) * (m + 1) * nrhs));
+        RTM_CUDA(cudaMemsetAsync(H.ptr, 0, H.bytes, s));
+        ar = GmArrays{H.as<double2>(), g.as<double2>(), cs.as<double2>(), sn.as<double2>(), h.as<double2>(),
+                      c.as<double2>(), y.as<double2>(), ipart.as<double2>(), ihist.as<double>(), m + 1, m};
+    }
+    if (x0) RTM_CUDA(cudaMemcpyAsync(x, x0, vec64, cudaMemcpyDeviceToDevice, s));
+    else RTM_CUDA(cudaMemsetAsync(x, 0, vec64, s));
+    int inner_total = 0, steps = 0;
+    res.matvecs = 0;
+    std::vector<int> hd(nrhs);
+    for (int step = 0;; ++step) {
+        RTM_TRY(A64->apply(x, t64.ptr, nrhs, s, SkipFlags{}));
+        k_residual<double2><<<grid, kRT, 0, s>>>(b, t64.as<double2>(), r64.as<double2>(), n, nullptr, 0);
+        k_true_residual<double2><<<grid, kRT, 0, s>>>(b, t64.as<double2>(), n, part.as<double2>(),
+                                                      cnt.as<unsigned int>(), resb.as<double2>());
+        k_ir_check<<<(nrhs + 31) / 32, 32, 0, s>>>(resb.as<double2>(), done.as<int>(), conv.as<int>(),
+                                                   hist.as<double>(), hs, step, cfg.tolerance, nrhs);
+        count_launch(3);
+        res.matvecs += 1;
+        RTM_CUDA(cudaMemcpyAsync(hd.data(), done.ptr, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        steps = step;
+        bool all = true;
+        for (int v : hd) all = all && v;
+        if (all || step >= cfg.max_refinements || inner_total >= cfg.max_iterations) break;
+        k_ir_to32<<<grid, kRT, 0, s>>>(r64.as<double2>(), r32.as<float2>(), n, resb.as<double2>(), done.as<int>());
+        count_launch();
+        if (inner_cg) {
+            SolveConfig ic;
+            ic.method = RTM_METHOD_CG;
+            ic.tolerance = cfg.inner_tolerance;
+            ic.max_iterations = std::max(1, cfg.restart);
+            ic.check_every = cfg.check_every;
+            SolveResult ir;
+            RTM_TRY(cocg<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
+            int most = 0;
+            for (auto& st : ir.stats) most = std::max(most, st.iteration_count);
+            inner_total += most;
+            res.matvecs += ir.matvecs + most + 1;
+        } else {
+            const int it = fgmres_cycle(A32, M32, r32.as<float2>(), d32.as<float2>(), n, nrhs, m, cfg.inner_tolerance,
+                                        V, Z, w, stb, ar, ghost, s);
+            if (it < 0) return it;
+            inner_total += it;
+            res.matvecs += it;
+        }
+        k_ir_update<<<grid, kRT, 0, s>>>(x, d32.as<float2>(), n, resb.as<double2>(), done.as<int>());
+        count_launch();
+    }
+    std::vector<double2> rb(nrhs);
+    std::vector<int> hc(nrhs);
+    RTM_CUDA(cudaMemcpyAsync(rb.data(), resb.ptr, sizeof(double2) * nrhs, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaMemcpyAsync(hc.data(), conv.ptr, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, s));
+    res.history.resize((size_t)hs * nrhs);
+    RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    res.hist_stride = hs;
+    res.stats.resize(nrhs);
+    for (int k = 0; k < nrhs; ++k) {
+        rtm_solve_stats& o = res.stats[k];
+        o.converged = hc[k];
+        o.iteration_count = inner_total;
+        o.residual_norm = rb[k].y == 0 ? 0.0 : rb[k].x / rb[k].y;
+        o.refinements = steps;
+        o.matvecs = res.matvecs;
+    }
+    return RTM_OK;
+}
+
+int solve(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b, const void* x0, void* x, int64_t n, int nrhs,
+          SolveResult& res, cudaStream_t s) {
+    if (cfg.method == RTM_METHOD_CG)
+        return A->precision == RTM_FP64 ? cocg<double>(A, M, cfg, b, x0, x, n, nrhs, res, s)
+                                        : cocg<float>(A, M, cfg, b, x0, x, n, nrhs, res, s);
+    if (cfg.method == RTM_METHOD_GMRES)
+        return A->precision == RTM_FP64 ? gmres<double>(A, M, cfg, b, x0, x, n, nrhs, res, s)
+                                        : gmres<float>(A, M, cfg, b, x0, x, n, nrhs, res, s);
+    return fail(RTM_ERR_ARG, "unknown solver method");
+}
+
+}  // namespace rtm

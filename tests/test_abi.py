@@ -1,0 +1,78 @@
+"""The C-ABI library loads and exports every entry point include/rtm.h declares (no GPU needed)."""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "rtm.h")).read()
+    return sorted(set(re.findall(r"RTM_API int (rtm_\w+)\(", text)))
+
+
+@pytest.fixture(scope="module")
+def library():
+    from rooftop_mom_b200 import build
+
+    return build.build()
+
+
+def test_library_exports_every_declared_symbol(library):
+    out = subprocess.run(["nm", "-D", "--defined-only", library], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (rtm_\w+)", out))
+    declared = _declared()
+    assert declared, "no declarations found"
+    assert set(declared) <= exported
+    # nothing else leaks out of the library
+    assert exported == set(declared)
+
+
+def test_library_loads_and_binds_every_symbol(library):
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    for name in _declared():
+        assert hasattr(lib, name)
+    assert set(_lib.exported_symbols()) == set(_declared())
+
+
+def test_version_and_errors_without_a_gpu(library):
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    assert lib.rtm_version(C.byref(a), C.byref(b), C.byref(c)) == 0
+    assert (a.value, b.value, c.value) == (3, 5, 0)
+    # argument errors are reported without touching a device
+    assert lib.rtm_generators_destroy(None) == 0
+    out = (C.c_double * 6)()
+    assert lib.rtm_estimate_bytes(0, 4, 1, 0, 0, 50, 1000, out) == _lib.ERR_ARG
+    assert "invalid grid" in _lib.last_error()
+
+
+def test_byte_models_match_the_oracle(library):
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+    from oracle import excitation as EX, geometry as G
+
+    lib = _lib.load()
+    for (cx, cy) in [(5, 4), (256, 256), (9, 1), (1, 6), (1024, 1024), (37, 11)]:
+        rt = G.Rooftops(cx, cy, 0.1, 0.1)
+        for pname, pid in _lib.PRODUCTS.items():
+            for method, mid in (("cg", 0), ("gmres", 1)):
+                out = (C.c_double * 6)()
+                assert lib.rtm_estimate_bytes(cx, cy, pid, mid, 1, 50, 1000, out) == 0
+                stored, working = EX.estimate_product(rt, pname)
+                assert out[0] == EX.estimate_generators(rt)
+                assert out[1] == stored and out[2] == working
+                ps, pw = EX.estimate_preconditioner(rt)
+                assert out[3] == ps and out[4] == pw
+                assert out[5] == EX.estimate_solver(rt.count, method, True, 50, 1000)

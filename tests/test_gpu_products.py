@@ -1,0 +1,175 @@
+"""GPU products, spectra, preconditioners and excitations against the reference's golden data and
+the oracle (the reference's tests: +reference/+assembler/+greensMatrix/ApplicatorTest.m,
++reference/+assembler/+preconditioner/GenerateCirculantTest.m, +reference/+operator/GeneratePlaneWaveTest.m,
++unit/+assembler/+greensMatrix/ApplicatorTest.m)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import reference_case, rel, random_vector
+
+pytestmark = pytest.mark.gpu
+
+PRODUCTS = ("fft", "splitFFT", "leanSplitFFT")
+FIELDS = {"fft": "productFFT", "splitFFT": "productSplit", "leanSplitFFT": "productLean"}
+
+
+def _problem_from_reference(d):
+    import rooftop_mom_b200 as R
+
+    mesh = R.Mesh(d["countX"], d["countY"], d["sizeX"], d["sizeY"])
+    prob = R.Problem(mesh, d["wavenumber"], quadratureOrder=d["order"])
+    prob.setGenerators(R.Generators.fromArrays(mesh, d["magneticXX"], d["magneticYY"], d["electric"]))
+    return prob
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+@pytest.mark.parametrize("product", PRODUCTS)
+def test_products_match_the_reference(golden, case, product):
+    import rooftop_mom_b200 as R
+
+    d = reference_case(golden, case)
+    op = R.Operator(_problem_from_reference(d), product=product)
+    assert rel(op.apply(d["vector"]), d[FIELDS[product]]) < 1e-13
+
+
+def test_product_matches_the_reference_dense_matrix(golden):
+    import rooftop_mom_b200 as R
+
+    d = reference_case(golden, 0)
+    op = R.Operator(_problem_from_reference(d), product="fft")
+    assert rel(op.apply(d["vector"]), d["impedanceMatrix"] @ d["vector"]) < 1e-10
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+@pytest.mark.parametrize("k", [0, 1])
+def test_partwise_preconditioners_match_the_reference(golden, case, k):
+    import rooftop_mom_b200 as R
+
+    d = reference_case(golden, case)
+    pc = R.Preconditioner(_problem_from_reference(d), kernel=["strang", "tChan"][k], builder="partwise")
+    assert rel(pc.apply(d["vector"]), d["preconditioned"][k]) < 1e-12
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_plane_wave_matches_the_reference(golden, case):
+    import rooftop_mom_b200 as R
+
+    d = reference_case(golden, case)
+    prob = _problem_from_reference(d)
+    exc = R.Excitation.planeWave(prob, direction=d["direction"], polarization=d["polarization"],
+                                 intensity=d["intensity"])
+    assert rel(exc.vector(), d["planeWave"]) < 1e-13
+
+
+GRIDS = {
+    "plate": (5, 4, 0.1, 0.15),
+    "oddPlate": (11, 7, 0.1, 0.1),
+    "twoFacesWide": (2, 5, 0.1, 0.1),
+    "stripX": (9, 1, 0.1, 0.02),
+    "stripY": (1, 6, 0.03, 0.1),
+    "square32": (32, 32, 0.05, 0.05),
+    "prime": (13, 17, 0.07, 0.05),
+}
+
+
+@pytest.mark.parametrize("name", sorted(GRIDS))
+@pytest.mark.parametrize("product", PRODUCTS)
+def test_products_match_the_dense_matrix(name, product):
+    """+unit/+assembler/+greensMatrix/ApplicatorTest.m: product of the assembled generators vs the
+    dense matrix of the same generators (oracle), rel 1e-12; the GPU generators vs the oracle's."""
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, excitation as EX, geometry as G
+
+    cx, cy, a, b = GRIDS[name]
+    mesh = R.Mesh(cx, cy, a, b)
+    prob = R.Problem(mesh, 2 * np.pi, quadratureOrder=3)
+    gen_gpu = prob.generators()
+    xx, yy, e = gen_gpu.arrays()
+    ref = A.generate(cx, cy, a, b, 2 * np.pi, (3, 3))
+    assert rel(e, ref.electric) < 1e-12
+    if ref.magnetic_xx is not None:
+        assert rel(xx, ref.magnetic_xx) < 1e-12
+    if ref.magnetic_yy is not None:
+        assert rel(yy, ref.magnetic_yy) < 1e-12
+    rt = G.Rooftops(cx, cy, a, b, 3)
+    dense = EX.dense_matrix(A.Generators(xx, yy, e, rt.content), rt)
+    v = random_vector(rt.count, seed=1)
+    assert rel(R.Operator(prob, product=product).apply(v), dense @ v) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["plate", "oddPlate", "stripX", "stripY", "square32"])
+def test_spectra_match_the_oracle(name):
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, spectra as S
+
+    cx, cy, a, b = GRIDS[name]
+    prob = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3)
+    op = R.Operator(prob, product="splitFFT")
+    xx, yy, e = prob.generators().arrays()
+    content = 3 if (cx > 1 and cy > 1) else (1 if cy == 1 else 2)
+    sub = S.subband_spectra(A.Generators(xx, yy, e, content), a, b)
+    got = op.spectra()
+    if content == 3:
+        for s in range(4):
+            # E, MXX, MYY per subband: rebuild the reference blocks from the raw spectra
+            blk = sub[s]
+            P, Q = got.shape[1:]
+            sx, sy = S.shift_phases(P, Q, s % 2, s // 2)
+            mine = S.block_spectra(got[3 * s + 1], got[3 * s + 2], got[3 * s], content, a, b, sx, sy)
+            for f in ("xx", "xy", "yx", "yy"):
+                assert rel(getattr(mine, f), getattr(blk, f)) < 1e-13
+    else:
+        for s in range(2):
+            want = sub[s].xx if content == 1 else sub[s].yy
+            assert rel(got[s].ravel(), want.ravel()) < 1e-13
+
+
+@pytest.mark.parametrize("kernel", ["strang", "tChan", "rChan", "huckle"])
+@pytest.mark.parametrize("name", ["plate", "oddPlate", "stripX", "stripY", "prime"])
+def test_circulant_preconditioners_match_the_oracle(kernel, name):
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, geometry as G, preconditioner as PC, spectra as S
+
+    cx, cy, a, b = GRIDS[name]
+    prob = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3)
+    bw = (max(1, cx // 2), max(1, cy // 2)) if kernel == "huckle" else None
+    pc = R.Preconditioner(prob, kernel=kernel, bandwidth=bw)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, a, b, 3)
+    inv = PC.circulant(A.Generators(xx, yy, e, rt.content), a, b, kernel, "partwise", bw)
+    v = random_vector(rt.count, seed=3)
+    assert rel(pc.apply(v), S.fft_apply(rt, inv, rt.content, v)) < 1e-12
+
+
+def test_single_precision_product_is_within_fp32_rounding():
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(64, 48, 0.05, 0.05), 2 * np.pi)
+    v = random_vector(prob.rooftopCount(), seed=4)
+    y64 = R.Operator(prob, precision="double").apply(v)
+    y32 = R.Operator(prob, precision="single").apply(v)
+    assert rel(y32, y64) < 2e-5
+
+
+def test_size_mismatch_raises_the_reference_error():
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(5, 4, 0.1, 0.15), 2 * np.pi)
+    op = R.Operator(prob)
+    with pytest.raises(R.RtmError) as e:
+        op.apply(np.zeros(prob.rooftopCount() + 1, complex))
+    assert e.value.identifier == "rooftopMoM:product:sizeMismatch"
+
+
+def test_batched_product_equals_single_products():
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(40, 24, 0.05, 0.05), 2 * np.pi)
+    n = prob.rooftopCount()
+    op = R.Operator(prob, maxRhs=4)
+    vs = [random_vector(n, seed=10 + k) for k in range(4)]
+    ys = op.apply(np.concatenate(vs), nrhs=4)
+    for k in range(4):
+        assert rel(ys[k * n:(k + 1) * n], op.apply(vs[k])) < 1e-15 + 1e-14

@@ -1,0 +1,153 @@
+"""GPU solvers against the oracle and the reference's solver tests
+(+unit/+solver/{ConjugateGradientTest,GeneralizedMinimumResidualTest,IterativeMethodTest}.m,
++unit/SolverTest.m, +unit/ResultTest.m, +unit/+operator/ComputeInputImpedanceTest.m)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _symmetric(count, seed=1):
+    rng = np.random.default_rng(seed)
+    r = (rng.standard_normal((count, count)) + 1j * rng.standard_normal((count, count))) / np.sqrt(count)
+    A = 4 * np.eye(count) + (r + r.T) / 2
+    b = rng.standard_normal(count) + 1j * rng.standard_normal(count)
+    return A, b
+
+
+def _nonsymmetric(count, seed=2):
+    rng = np.random.default_rng(seed)
+    A = 4 * np.eye(count) + (rng.standard_normal((count, count)) + 1j * rng.standard_normal((count, count))) / np.sqrt(count)
+    b = rng.standard_normal(count) + 1j * rng.standard_normal(count)
+    return A, b
+
+
+@pytest.mark.parametrize("method", ["cg", "gmres"])
+def test_dense_system_matches_the_oracle_history(method):
+    import rooftop_mom_b200 as R
+    from oracle import solvers as OS
+
+    A, b = _symmetric(60) if method == "cg" else _nonsymmetric(60)
+    res = R.Solver(method=method, tolerance=1e-10, restart=7).solve(A, b)
+    ref = OS.solve(method, A, b, tol=1e-10, restart=7)
+    assert res.converged() and ref.converged
+    assert res.iterationCount() == ref.iteration_count
+    np.testing.assert_allclose(res.residualNorms(), ref.residual_norms, rtol=1e-8, atol=1e-14)
+    assert rel(res.solution(), ref.solution) < 1e-9
+    assert res.residualNorm() < 1e-10
+
+
+def test_preconditioned_cg_matches_the_oracle():
+    import rooftop_mom_b200 as R
+    from oracle import solvers as OS
+
+    A, b = _symmetric(50, seed=5)
+    P = np.diag(1 / np.diag(A))
+    res = R.Solver(method="cg", tolerance=1e-10).solve(A, b, preconditioner=P)
+    ref = OS.solve("cg", A, b, tol=1e-10, precond=P)
+    assert res.iterationCount() == ref.iteration_count
+    assert rel(res.solution(), ref.solution) < 1e-9
+
+
+def test_zero_rhs_gives_zero_solution():
+    import rooftop_mom_b200 as R
+
+    A, _ = _symmetric(20)
+    for method in ("cg", "gmres"):
+        res = R.Solver(method=method).solve(A, np.zeros(20, complex), initialGuess=np.ones(20, complex))
+        assert res.converged() and res.iterationCount() == 0 and res.residualNorm() == 0
+        assert np.all(res.solution() == 0)
+        np.testing.assert_array_equal(res.residualNorms(), [0.0])
+
+
+def test_exact_initial_guess_converges_at_once():
+    import rooftop_mom_b200 as R
+
+    A, b = _symmetric(30)
+    x = np.linalg.solve(A, b)
+    res = R.Solver(method="cg", tolerance=1e-8).solve(A, b, initialGuess=x)
+    assert res.converged() and res.iterationCount() == 0
+
+
+def test_iteration_limit_is_not_an_error():
+    import rooftop_mom_b200 as R
+
+    A, b = _nonsymmetric(80)
+    res = R.Solver(method="gmres", tolerance=1e-14, maxIterationCount=5, restart=3).solve(A, b)
+    assert not res.converged() and res.iterationCount() == 5
+    assert len(res.residualNorms()) == 6
+
+
+@pytest.mark.parametrize("method", ["cg", "gmres"])
+def test_plate_solve_matches_the_oracle(method):
+    """SolverTest.m:9-21 style: a plane wave on a small plate, residual vs the dense matrix."""
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, excitation as EX, geometry as G, solvers as OS, spectra as S
+
+    cx = cy = 12
+    h = 1.0 / 20
+    prob = R.Problem(R.Mesh(cx, cy, h, h), 2 * np.pi)
+    op = R.Operator(prob)
+    exc = R.Excitation.planeWave(prob)
+    res = R.Solver(method=method, tolerance=1e-12, restart=30).solve(op, exc)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, h, h, 8)
+    gen = A.Generators(xx, yy, e, rt.content)
+    dense = EX.dense_matrix(gen, rt)
+    b = exc.vector()
+    assert np.linalg.norm(dense @ res.solution() - b) / np.linalg.norm(b) < 1e-10
+    sub = S.subband_spectra(gen, h, h)
+    ref = OS.solve(method, lambda v: S.split_apply(rt, sub, rt.content, v), b, tol=1e-12, restart=30)
+    assert res.iterationCount() == ref.iteration_count
+    assert rel(res.solution(), ref.solution) < 1e-10
+
+
+def test_rcs_and_impedance_match_the_oracle():
+    import rooftop_mom_b200 as R
+    from oracle import excitation as EX, geometry as G
+
+    prob = R.Problem(R.Mesh(16, 16, 0.05, 0.05), 2 * np.pi)
+    op = R.Operator(prob)
+    exc = R.Excitation.planeWave(prob)
+    res = R.Solver(tolerance=1e-10).solve(op, exc)
+    rcs = EX.radar_cross_section(2 * np.pi, exc.vector(), res.solution())
+    assert abs(res.radarCrossSection() - rcs) / rcs < 1e-12
+    strip = R.Problem(R.Mesh(21, 1, 0.025, 0.005), 2 * np.pi)
+    gap = R.Excitation.deltaGap(strip)
+    rt = G.Rooftops(21, 1, 0.025, 0.005, 8)
+    np.testing.assert_array_equal(np.flatnonzero(gap.vector()), EX.middle_port(rt, "x"))
+    r2 = R.Solver(tolerance=1e-10).solve(R.Operator(strip), gap)
+    z = EX.input_impedance(rt, r2.solution(), EX.middle_port(rt, "x"))
+    assert abs(r2.inputImpedance() - z) / abs(z) < 1e-12
+
+
+def test_block_jacobi_gmres_converges_on_a_plate():
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(48, 48, 0.05, 0.05), 2 * np.pi)
+    op = R.Operator(prob)
+    exc = R.Excitation.planeWave(prob, direction=[0.5, 0, -np.sqrt(3) / 2], polarization=[0, 1, 0])
+    plain = R.Solver(method="gmres", tolerance=1e-6, restart=50).solve(op, exc)
+    pc = R.Preconditioner.blockJacobi(prob, (2, 2))
+    pre = R.Solver(method="gmres", tolerance=1e-6, restart=50).solve(op, exc, preconditioner=pc)
+    assert pre.converged() and plain.converged()
+    assert pre.residualNorm() < 1e-5
+    assert rel(pre.solution(), plain.solution()) < 1e-4
+
+
+def test_mixed_precision_refinement_reaches_fp64_tolerance():
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(64, 64, 1 / 15, 1 / 15), 2 * np.pi)
+    op64 = R.Operator(prob)
+    op32 = R.Operator(prob, precision="single")
+    exc = R.Excitation.planeWave(prob, direction=[0.5, 0, -np.sqrt(3) / 2], polarization=[0, 1, 0])
+    ref = R.Solver(method="gmres", tolerance=1e-10, restart=100, maxIterationCount=5000).solve(op64, exc)
+    mix = R.Solver(method="fgmres", tolerance=1e-8, restart=30, innerTolerance=1e-4,
+                   maxIterationCount=5000).solve(op64, exc, innerOperator=op32)
+    assert mix.converged() and mix.residualNorm() < 1e-8
+    assert rel(mix.solution(), ref.solution()) < 1e-6
