@@ -171,6 +171,8 @@ typedef struct rtm_solve_config {
     double inner_tolerance;/* FGMRES_IR: relative residual of one FP32 inner solve */
     int max_refinements;   /* FGMRES_IR: bound on the FP64 outer refinement steps */
     int check_every;       /* iterations between host convergence checks (0: library default) */
+    int right_preconditioned; /* GMRES: 0 left preconditioning (GeneralizedMinimumResidual.m:2-5), 1 right
+                                 (flexible GMRES: the monitored residual is that of op * x = b) */
 } rtm_solve_config;
 
 typedef struct rtm_solve_stats {

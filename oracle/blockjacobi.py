@@ -54,22 +54,20 @@ def entry(gen, rt: Rooftops, dp, fp, dq, fq):
 
 
 class BlockJacobi:
+    """Block-Jacobi preconditioner: the inverses of the diagonal blocks, applied per block."""
+
     def __init__(self, gen, rt: Rooftops, bx=2, by=2):
-        self.blocks = []
+        groups = {}
         for idx, dirs, faces in block_indices(rt, bx, by):
-            n = idx.size
-            M = np.empty((n, n), dtype=np.complex128)
-            for r in range(n):
-                for c in range(n):
-                    M[r, c] = entry(gen, rt, dirs[r], faces[r], dirs[c], faces[c])
-            self.blocks.append((idx, np.linalg.inv(M)))
-        # group blocks of one size for a vectorised apply
+            if idx.size:  # a block at the edge of a strip can hold no rooftop
+                groups.setdefault(idx.size, []).append((idx, dirs, faces))
         self.groups = {}
-        for idx, inv in self.blocks:
-            self.groups.setdefault(idx.size, ([], []))
-            self.groups[idx.size][0].append(idx)
-            self.groups[idx.size][1].append(inv)
-        self.groups = {k: (np.array(v[0]), np.array(v[1])) for k, v in self.groups.items()}
+        for size, items in groups.items():
+            idx = np.array([it[0] for it in items])          # [B, n]
+            dirs = np.array([it[1] for it in items])         # [B, n]
+            faces = np.array([it[2] for it in items])        # [B, n, 2]
+            M = _entries(gen, rt, dirs, faces)               # [B, n, n]
+            self.groups[size] = (idx, np.linalg.inv(M))
 
     def apply(self, x):
         x = np.asarray(x)
@@ -77,3 +75,29 @@ class BlockJacobi:
         for idx, inv in self.groups.values():
             y[idx] = np.einsum("brc,bc->br", inv, x[idx])
         return y
+
+
+def _entries(gen, rt: Rooftops, dirs, faces):
+    """entry() for all pairs of all blocks at once: dirs [B, n], faces [B, n, 2] -> [B, n, n]."""
+    dp, dq = dirs[:, :, None], dirs[:, None, :]
+    fp, fq = faces[:, :, None, :], faces[:, None, :, :]
+    dx = np.abs(fp[..., 0] - fq[..., 0])
+    dy = np.abs(fp[..., 1] - fq[..., 1])
+    z = np.zeros(dx.shape, dtype=np.complex128)
+    if gen.magnetic_xx is not None:
+        m = (dp == 0) & (dq == 0)
+        z[m] = gen.magnetic_xx[dx[m], dy[m]]
+    if gen.magnetic_yy is not None:
+        m = (dp == 1) & (dq == 1)
+        z[m] = gen.magnetic_yy[dx[m], dy[m]]
+    hp = np.where(dp == 0, rt.size_x, rt.size_y)
+    hq = np.where(dq == 0, rt.size_x, rt.size_y)
+    for s in range(2):
+        fi = fp[..., 0] + (s * (dp == 0))
+        fj = fp[..., 1] + (s * (dp == 1))
+        for t in range(2):
+            gi = fq[..., 0] + (t * (dq == 0))
+            gj = fq[..., 1] + (t * (dq == 1))
+            w = (1.0 if s == t else -1.0) / (hp * hq)
+            z -= w * gen.electric[np.abs(fi - gi), np.abs(fj - gj)]
+    return z

@@ -95,7 +95,10 @@ class Generators:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            L.load().rtm_generators_destroy(self._h)
+            try:
+                L.load().rtm_generators_destroy(self._h)
+            except Exception:  # interpreter shutdown
+                pass
             self._h = None
 
     @property
@@ -221,7 +224,10 @@ class _Product:
 
     def __del__(self):
         if self._handle:
-            getattr(L.load(), self._destroy)(self._handle)
+            try:
+                getattr(L.load(), self._destroy)(self._handle)
+            except Exception:  # interpreter shutdown
+                pass
             self._handle = None
 
     def apply(self, x, nrhs: int = 1):
@@ -398,7 +404,9 @@ class Excitation:
         return v / np.linalg.norm(v)
 
     @classmethod
-    def planeWave(cls, problem: Problem, direction=(0, 0, -1), polarization=(1, 0, 0), intensity=1.0):
+    def planeWave(cls, problem: Problem, direction=(0, 0, -1), polarization=(1, 0, 0), intensity=1.0,
+                  device=False):
+        """device=True keeps the vector on the GPU (a complex128 CUDA tensor)."""
         d = cls._normalize(direction, "direction")
         p = cls._normalize(polarization, "polarization")
         dot = float(d @ p)
@@ -409,11 +417,17 @@ class Excitation:
         cx, cy = problem.mesh().count()
         a, b = problem.mesh().faceSize()
         n = problem.rooftopCount()
-        out = np.zeros(n, np.complex128)
         inten = np.array([float(intensity)])
+        if device:
+            import torch
+            out = torch.empty(n, dtype=torch.complex128, device="cuda")
+            ptr, where = C.c_void_p(out.data_ptr()), L.DEVICE
+        else:
+            out = np.zeros(n, np.complex128)
+            ptr, where = out.ctypes.data_as(C.c_void_p), L.HOST
         L.call("rtm_plane_wave", cx, cy, a, b, problem.quadratureOrder()[1], problem.wavenumber(),
                d.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p), inten.ctypes.data_as(C.c_void_p), 1,
-               out.ctypes.data_as(C.c_void_p), L.HOST, None)
+               ptr, where, None)
         return cls(problem, "planeWave", out, {"direction": d, "polarization": p, "intensity": float(intensity)})
 
     @classmethod
@@ -507,13 +521,13 @@ class Result:
     def radarCrossSection(self):
         p = self._parameters("planeWave")
         prob = self._excitation.problem()
-        ev = np.ascontiguousarray(self._excitation.vector())
-        if _is_device(self._x):
+        ev = self._excitation.vector()
+        if _is_device(self._x) and not _is_device(ev):
             import torch
-            e_t = torch.from_numpy(ev).to(self._x.device)
-            ep, where, keep1 = _vec_in(e_t, prob.rooftopCount())
-        else:
-            ep, where, keep1 = _vec_in(ev, prob.rooftopCount())
+            ev = torch.from_numpy(np.ascontiguousarray(ev)).to(self._x.device)
+        elif not _is_device(self._x) and _is_device(ev):
+            ev = ev.cpu().numpy()
+        ep, where, keep1 = _vec_in(ev, prob.rooftopCount())
         xp, where2, keep2 = _vec_in(self._x, prob.rooftopCount())
         out = C.c_double()
         L.call("rtm_radar_cross_section", prob.wavenumber(), ep, xp, prob.rooftopCount(), p["intensity"], where,
@@ -530,7 +544,7 @@ class Solver:
     precision form 'fgmres' (FP32 flexible GMRES inside FP64 iterative refinement)."""
 
     def __init__(self, method="cg", tolerance=1e-6, maxIterationCount=1000, restart=50, innerTolerance=1e-4,
-                 maxRefinements=20, checkEvery=0, innerMethod="fgmres"):
+                 maxRefinements=20, checkEvery=0, innerMethod="fgmres", side="left"):
         if method not in ("cg", "gmres", "fgmres"):
             raise _err("rooftopMoM:solver:invalidMethod", "The method is 'cg', 'gmres' or 'fgmres'.")
         if not (0 < tolerance < 1):
@@ -547,10 +561,13 @@ class Solver:
         self.maxRefinements = maxRefinements
         self.checkEvery = checkEvery
         self.innerMethod = innerMethod
+        if side not in ("left", "right"):
+            raise _err("rooftopMoM:solver:invalidSide", "The preconditioning side is 'left' or 'right'.")
+        self.side = side
 
     def _config(self, method_id):
         return L.SolveConfig(method_id, self.tolerance, self.maxIterationCount, self.restart, self.innerTolerance,
-                             self.maxRefinements, self.checkEvery)
+                             self.maxRefinements, self.checkEvery, int(self.side == "right"))
 
     def solve(self, operator, rightHandSide, preconditioner=None, initialGuess=None, innerOperator=None,
               innerPreconditioner=None, nrhs: int = 1):

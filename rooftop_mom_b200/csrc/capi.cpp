@@ -479,6 +479,7 @@ int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_config* 
     cfg.max_iterations = config->max_iterations;
     cfg.restart = config->restart;
     cfg.check_every = config->check_every;
+    cfg.right_preconditioned = config->right_preconditioned;
     cudaEvent_t e0, e1;
     RTM_CUDA(cudaEventCreate(&e0));
     RTM_CUDA(cudaEventCreate(&e1));

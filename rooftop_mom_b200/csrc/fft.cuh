@@ -1,10 +1,11 @@
 // Shared-memory mixed-radix FFT engine for sm_100a (device code only).
 //
-// A CTA transforms `lines` lines of length n that sit in shared memory; element e of line l is at
-// buf[l * ls + e * es]. The transform is a Stockham autosort FFT (natural order in and out): at a
-// stage of radix R after sub-transforms of length Ns, butterfly j reads the R elements
+// A CTA transforms, in place, `lines` lines of length n that sit in shared memory; element e of
+// line l is at buf[l * ls + e * es]. The transform is a Stockham autosort FFT (natural order in and
+// out): at a stage of radix R after sub-transforms of length Ns, butterfly j reads the R elements
 // j + t n/R, twiddles them by w^(t k n/(Ns R)) with k = j mod Ns, applies a radix-R DFT and writes
-// them to (j - k) R + k + q Ns. Radices 2, 4, 8 and 16 are hand-written, 3, 5 and 7 read their
+// them to (j - k) R + k + q Ns. Butterflies are numbered line-fastest, so a warp touches the same
+// position of consecutive lines (the callers pad or interleave lines to spread the banks). Radices 2, 4, 8 and 16 are hand-written, 3, 5 and 7 read their
 // roots from the twiddle table, larger primes up to kMaxGenericRadix use a direct DFT.
 // Twiddles are w^m = exp(-2 pi i m / n) (table of n entries); the inverse uses their conjugates
 // and does not scale.
@@ -151,49 +152,80 @@ template <int R, bool INV, typename T2> __device__ __forceinline__ void dft(T2* 
     else dft_odd<R, INV>(v, tw, n);
 }
 
-template <int R, bool INV, typename T2>
-__device__ __forceinline__ void stockham_pass(const T2* __restrict__ src, T2* __restrict__ dst, int n, int Ns,
-                                              int lines, int ls, int es, const T2* __restrict__ tw) {
+// Butterflies per thread of a stage of radix R (at most about 16 complex values in registers).
+__host__ __device__ constexpr int fft_ipt(int r) {
+    return r == 2 ? 8 : r == 3 ? 6 : r == 4 ? 4 : r == 5 ? 4 : r == 7 ? 3 : r == 8 ? 2 : 1;
+}
+
+// Threads a CTA needs to transform `lines` lines of plan p in place (a multiple of 32).
+__host__ __device__ inline int fft_threads(int lines, const FftPlan& p) {
+    int t = 32;
+    for (int s = 0; s < p.nstages; ++s) {
+        const int r = p.radix[s];
+        const int per = fft_ipt(r);
+        const int need = (lines * (p.n / r) + per - 1) / per;
+        t = need > t ? need : t;
+    }
+    return (t + 31) / 32 * 32;
+}
+
+// One in-place Stockham stage: every thread loads its butterflies into registers, the CTA
+// synchronises, then every thread stores them. Needs items = lines n / R <= IPT blockDim.x.
+template <int R, int IPT, bool INV, typename T2>
+__device__ __noinline__ void pass_ip(T2* buf, int n, int Ns, int lines, int ls, int es, const T2* __restrict__ tw) {
     const int nb = n / R;
     const int stride = n / (Ns * R);
     const int items = lines * nb;
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int line = it % lines;
-        const int j = it / lines;
-        const int k = j % Ns;
-        const T2* s = src + line * ls;
-        T2 v[R];
+    T2 v[IPT][R];
 #pragma unroll
-        for (int t = 0; t < R; ++t) v[t] = s[(j + t * nb) * es];
-        if (Ns > 1) {
+    for (int q = 0; q < IPT; ++q) {
+        const int it = threadIdx.x + q * blockDim.x;
+        if (it < items) {
+            const int line = it % lines, j = it / lines, k = j % Ns;
+            const T2* s = buf + line * ls;
 #pragma unroll
-            for (int t = 1; t < R; ++t) {
-                const T2 w = __ldg(&tw[t * k * stride]);
-                v[t] = INV ? cmulc(v[t], w) : cmul(v[t], w);
+            for (int t = 0; t < R; ++t) v[q][t] = s[(j + t * nb) * es];
+            if (Ns > 1) {
+#pragma unroll
+                for (int t = 1; t < R; ++t) {
+                    const T2 w = __ldg(&tw[t * k * stride]);
+                    v[q][t] = INV ? cmulc(v[q][t], w) : cmul(v[q][t], w);
+                }
             }
+            dft<R, INV>(v[q], tw, n);
         }
-        dft<R, INV>(v, tw, n);
-        const int base = (j - k) * R + k;
-        T2* d = dst + line * ls;
-#pragma unroll
-        for (int q = 0; q < R; ++q) d[(base + q * Ns) * es] = v[q];
     }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+        const int it = threadIdx.x + q * blockDim.x;
+        if (it < items) {
+            const int line = it % lines, j = it / lines, k = j % Ns;
+            const int base = (j - k) * R + k;
+            T2* d = buf + line * ls;
+#pragma unroll
+            for (int t = 0; t < R; ++t) d[(base + t * Ns) * es] = v[q][t];
+        }
+    }
+    __syncthreads();
 }
 
-// Any radix up to kMaxGenericRadix by a direct DFT (rare: sizes with a prime factor above 7).
+// Any radix up to kMaxGenericRadix (rare: sizes with a prime factor above 7) by a direct DFT; one
+// butterfly per thread suffices since R > 16.
 template <bool INV, typename T2>
-__device__ void stockham_pass_generic(const T2* __restrict__ src, T2* __restrict__ dst, int n, int R, int Ns,
-                                      int lines, int ls, int es, const T2* __restrict__ tw) {
+__device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int lines, int ls, int es, const T2* __restrict__ tw) {
     const int nb = n / R;
     const int stride = n / (Ns * R);
     const int st = n / R;
     const int items = lines * nb;
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int line = it % lines;
-        const int j = it / lines;
-        const int k = j % Ns;
-        const T2* s = src + line * ls;
-        T2 v[kMaxGenericRadix];
+    const int it = threadIdx.x;
+    T2 v[kMaxGenericRadix];
+    int line = 0, j = 0, k = 0;
+    if (it < items) {
+        line = it % lines;
+        j = it / lines;
+        k = j % Ns;
+        const T2* s = buf + line * ls;
         for (int t = 0; t < R; ++t) {
             T2 x = s[(j + t * nb) * es];
             if (Ns > 1 && t > 0) {
@@ -202,8 +234,11 @@ __device__ void stockham_pass_generic(const T2* __restrict__ src, T2* __restrict
             }
             v[t] = x;
         }
+    }
+    __syncthreads();
+    if (it < items) {
         const int base = (j - k) * R + k;
-        T2* d = dst + line * ls;
+        T2* d = buf + line * ls;
         for (int q = 0; q < R; ++q) {
             T2 acc = v[0];
             for (int t = 1; t < R; ++t) {
@@ -213,32 +248,29 @@ __device__ void stockham_pass_generic(const T2* __restrict__ src, T2* __restrict
             d[(base + q * Ns) * es] = acc;
         }
     }
+    __syncthreads();
 }
 
-// Transforms the lines in `a` (using `b` as scratch) and returns the buffer holding the result.
-// Call after a __syncthreads() that makes `a` visible; returns after a __syncthreads().
+// Transforms, in place, the `lines` lines of length p.n in buf (element e of line l at
+// buf[l * ls + e * es]). Needs blockDim.x >= fft_threads(lines, p.n); call it after a
+// __syncthreads() that makes buf visible; it returns after one.
 template <bool INV, typename T2>
-__device__ T2* fft_smem(T2* a, T2* b, int lines, int ls, int es, const FftPlan& p, const T2* __restrict__ tw) {
+__device__ void fft_inplace(T2* buf, int lines, int ls, int es, const FftPlan& p, const T2* __restrict__ tw) {
     int Ns = 1;
     for (int s = 0; s < p.nstages; ++s) {
         const int r = p.radix[s];
         switch (r) {
-            case 2: stockham_pass<2, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 3: stockham_pass<3, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 4: stockham_pass<4, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 5: stockham_pass<5, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 7: stockham_pass<7, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 8: stockham_pass<8, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            case 16: stockham_pass<16, INV>(a, b, p.n, Ns, lines, ls, es, tw); break;
-            default: stockham_pass_generic<INV>(a, b, p.n, r, Ns, lines, ls, es, tw); break;
+            case 2: pass_ip<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 3: pass_ip<3, 6, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 4: pass_ip<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 5: pass_ip<5, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 7: pass_ip<7, 3, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 8: pass_ip<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            case 16: pass_ip<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            default: pass_ip_generic<INV>(buf, p.n, r, Ns, lines, ls, es, tw); break;
         }
-        __syncthreads();
-        T2* t = a;
-        a = b;
-        b = t;
         Ns *= r;
     }
-    return a;
 }
 
 }  // namespace rtm

@@ -24,7 +24,7 @@
 namespace rtm {
 
 static constexpr int kSmemBudget = 200 * 1024;
-static constexpr int kThreads = 256;
+static constexpr int kMaxThreads = 256;  // CTA size of the FFT kernels (up to 255 registers a thread)
 
 template <typename T> struct GridArgs {
     using T2 = typename Cx<T>::T2;
@@ -52,6 +52,7 @@ template <typename T> struct GridArgs {
     T inv_a2, inv_b2, inv_ab, scale;
     const int* skip;  // per right-hand side, nonzero: leave it alone
     int skip_stride;
+    int cb, ls;  // x-mix: y frequencies per CTA and the padded line stride
 };
 
 template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rhs) {
@@ -59,80 +60,80 @@ template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rh
 }
 
 // --------------------------------------------------------------------------------------------
-// y-forward: W[py][c][j][i] = FFT_y( x_c(i, j) * mody(j)^py ), i in the tile.
+// y-forward: W[py][c][j][i] = FFT_y( x_c(i, j) * mody(j)^py ) for a tile of TI x columns of one
+// component c and one y subband py (grid: tiles x (component, subband) x right-hand sides).
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* B = A + TI * Q;
+    const int c = blockIdx.y % a.ncomp, pyi = blockIdx.y / a.ncomp, py = a.py0 + pyi;
+    const int rhs = blockIdx.z;
+    const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
-    const int rhs = blockIdx.y;
-    if (skipped(a, rhs)) return;
-    const T2* xr = x + (int64_t)rhs * a.n;
-    T2* wr = a.work + (int64_t)rhs * a.work_rhs;
-    for (int c = 0; c < a.ncomp; ++c) {
-        const int rows = a.rows[c], cols = a.cols[c];
-        if (i0 >= rows) continue;
-        for (int pyi = 0; pyi < a.npy; ++pyi) {
-            const int py = a.py0 + pyi;
-            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-                const int l = it % TI, j = it / TI, i = i0 + l;
-                T2 v = czero<T2>();
-                if (i < rows && j < cols) {
-                    v = xr[a.off[c] + i + (int64_t)j * rows];
-                    if (py) v = cmul(v, __ldg(&a.modQ[j]));
-                }
-                A[it] = v;
-            }
-            __syncthreads();
-            T2* out = fft_smem<false>(A, B, TI, 1, TI, a.planQ, a.twQ);
-            T2* dst = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
-            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-                const int l = it % TI, j = it / TI, i = i0 + l;
-                if (i < rows) dst[(int64_t)j * a.P + i] = out[it];
-            }
-            __syncthreads();
+    if (i0 >= rows || skipped(a, rhs)) return;
+    const T2* xr = x + (int64_t)rhs * a.n + a.off[c];
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        T2 v = czero<T2>();
+        if (i < rows && j < cols) {
+            v = xr[i + (int64_t)j * rows];
+            if (py) v = cmul(v, __ldg(&a.modQ[j]));
         }
+        A[it] = v;
+    }
+    __syncthreads();
+    fft_inplace<false>(A, TI, 1, TI, a.planQ, a.twQ);
+    T2* dst = a.work + (int64_t)rhs * a.work_rhs + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        if (i < rows) dst[(int64_t)j * a.P + i] = A[it];
     }
 }
 
 // --------------------------------------------------------------------------------------------
-// x-mix: per y frequency j of the y subband py, both components: sum over px of
-// demod_x^px * IFFT_x( B(px,py) * FFT_x( W * mod_x^px ) ), scaled by 1/(PQ), in place.
+// x-mix: for CB y frequencies j of the y subband py and both components: sum over px of
+// demod_x^px IFFT_x( B(px, py) FFT_x( W mod_x^px ) ), scaled by 1/(PQ), in place in W. The
+// 2 CB lines sit in shared memory with an odd line stride (a.ls) so that consecutive lines fall on
+// different banks.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_grid_x_mix(const GridArgs<T> a) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_x_mix(const GridArgs<T> a) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int P = a.P, Q = a.Q, nc = a.ncomp;
-    T2* acc = reinterpret_cast<T2*>(smem_raw);
-    T2* A = acc + nc * P;
-    T2* B = A + nc * P;
-    const int j = blockIdx.x;
+    const int P = a.P, Q = a.Q, nc = a.ncomp, CB = a.cb, ls = a.ls;
+    const int lines = nc * CB;
+    T2* A = reinterpret_cast<T2*>(smem_raw);
+    T2* acc = A + lines * ls;
+    const int j0 = blockIdx.x * CB;
     const int pyi = blockIdx.y;
     const int py = a.py0 + pyi;
     const int rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
     T2* wr = a.work + (int64_t)rhs * a.work_rhs + (int64_t)pyi * nc * Q * P;
     const T2* vy = py ? a.vy1 : a.vy0;
+    // line l = jj * nc + c: column j0 + jj of component c
     for (int px = 0; px < a.nsx; ++px) {
-        for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
-            const int c = it / P, i = it - c * P;
+        for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
+            const int l = it / P, i = it - l * P;
+            const int c = l % nc, j = j0 + l / nc;
             T2 v = czero<T2>();
-            if (i < a.rows[c]) {
+            if (i < a.rows[c] && j < Q) {
                 v = wr[((int64_t)c * Q + j) * P + i];
                 if (px) v = cmul(v, __ldg(&a.modP[i]));
             }
-            A[it] = v;
+            A[l * ls + i] = v;
         }
         __syncthreads();
-        T2* U = fft_smem<false>(A, B, nc, P, 1, a.planP, a.twP);
-        T2* other = (U == A) ? B : A;
+        fft_inplace<false>(A, lines, ls, 1, a.planP, a.twP);
         const int sub = px + a.nsx * py;
         const T2* ux = px ? a.ux1 : a.ux0;
-        for (int i = threadIdx.x; i < P; i += blockDim.x) {
-            const T2 sx = U[i], sy = U[P + i];
+        for (int it = threadIdx.x; it < CB * P; it += blockDim.x) {
+            const int jj = it / P, i = it - jj * P, j = j0 + jj;
+            if (j >= Q) continue;
+            T2* lx = A + (jj * nc) * ls;
+            T2* ly = lx + ls;
+            const T2 sx = lx[i], sy = ly[i];
             T2 ox, oy;
             if (a.mode == kGen3) {
                 const int64_t base = ((int64_t)(sub * 3) * Q + j) * P + i;
@@ -159,83 +160,79 @@ __global__ void __launch_bounds__(kThreads) k_grid_x_mix(const GridArgs<T> a) {
                 ox = cadd(cmul(XX, sx), cmul(XY, sy));
                 oy = cadd(cmul(YX, sx), cmul(YY, sy));
             }
-            U[i] = ox;
-            U[P + i] = oy;
+            lx[i] = ox;
+            ly[i] = oy;
         }
         __syncthreads();
-        T2* Y = fft_smem<true>(U, other, nc, P, 1, a.planP, a.twP);
-        for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
-            const int c = it / P, i = it - c * P;
-            T2 v = Y[it];
-            if (px) v = cmulc(v, __ldg(&a.modP[i]));
-            acc[it] = px ? cadd(acc[it], v) : v;
+        fft_inplace<true>(A, lines, ls, 1, a.planP, a.twP);
+        for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
+            const int l = it / P, i = it - l * P;
+            T2 v = A[l * ls + i];
+            if (px) v = cadd(acc[l * ls + i], cmulc(v, __ldg(&a.modP[i])));
+            acc[l * ls + i] = v;
         }
         __syncthreads();
     }
-    for (int it = threadIdx.x; it < nc * P; it += blockDim.x) {
-        const int c = it / P, i = it - c * P;
-        if (i < a.rows[c]) wr[((int64_t)c * Q + j) * P + i] = cscale(acc[it], a.scale);
+    for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
+        const int l = it / P, i = it - l * P;
+        const int c = l % nc, j = j0 + l / nc;
+        if (i < a.rows[c] && j < Q) wr[((int64_t)c * Q + j) * P + i] = cscale(acc[l * ls + i], a.scale);
     }
 }
 
 // --------------------------------------------------------------------------------------------
-// y-inverse: y_c(i, j) = sum_py demod_y^py IFFT_y(W[py][c][:, i]) for the tile, cropped.
+// y-inverse: y_c(i, j) = sum_py demod_y^py IFFT_y(W[py][c][:, i]) for a tile of TI columns of one
+// component, cropped to the rooftop grid (grid: tiles x components x right-hand sides).
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q;
-    T2* acc = reinterpret_cast<T2*>(smem_raw);
-    T2* A = acc + TI * Q;
-    T2* B = A + TI * Q;
+    T2* A = reinterpret_cast<T2*>(smem_raw);
+    T2* acc = A + TI * Q;
+    const int c = blockIdx.y, rhs = blockIdx.z;
+    const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
-    const int rhs = blockIdx.y;
-    if (skipped(a, rhs)) return;
-    T2* yr = y + (int64_t)rhs * a.n;
+    if (i0 >= rows || skipped(a, rhs)) return;
     const T2* wr = a.work + (int64_t)rhs * a.work_rhs;
-    for (int c = 0; c < a.ncomp; ++c) {
-        const int rows = a.rows[c], cols = a.cols[c];
-        if (i0 >= rows) continue;
-        for (int pyi = 0; pyi < a.npy; ++pyi) {
-            const int py = a.py0 + pyi;
-            const T2* src = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
-            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-                const int l = it % TI, j = it / TI, i = i0 + l;
-                A[it] = (i < rows) ? src[(int64_t)j * a.P + i] : czero<T2>();
-            }
-            __syncthreads();
-            T2* R = fft_smem<true>(A, B, TI, 1, TI, a.planQ, a.twQ);
-            for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-                const int j = it / TI;
-                T2 v = R[it];
-                if (py) v = cmulc(v, __ldg(&a.modQ[j]));
-                acc[it] = pyi ? cadd(acc[it], v) : v;
-            }
-            __syncthreads();
-        }
+    for (int pyi = 0; pyi < a.npy; ++pyi) {
+        const int py = a.py0 + pyi;
+        const T2* src = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
         for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
             const int l = it % TI, j = it / TI, i = i0 + l;
-            if (i < rows && j < cols) {
-                const int64_t idx = a.off[c] + i + (int64_t)j * rows;
-                yr[idx] = a.accumulate ? cadd(yr[idx], acc[it]) : acc[it];
-            }
+            A[it] = (i < rows) ? src[(int64_t)j * a.P + i] : czero<T2>();
         }
         __syncthreads();
+        fft_inplace<true>(A, TI, 1, TI, a.planQ, a.twQ);
+        for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+            const int j = it / TI;
+            T2 v = A[it];
+            if (py) v = cmulc(v, __ldg(&a.modQ[j]));
+            acc[it] = pyi ? cadd(acc[it], v) : v;
+        }
+        __syncthreads();
+    }
+    T2* yr = y + (int64_t)rhs * a.n + a.off[c];
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        if (i < rows && j < cols) {
+            const int64_t idx = i + (int64_t)j * rows;
+            yr[idx] = a.accumulate ? cadd(yr[idx], acc[it]) : acc[it];
+        }
     }
 }
 
 // --------------------------------------------------------------------------------------------
 // Strip: y = sum_s demod^s IFFT( B_s * FFT( x * mod^s ) ) / L on one line per right-hand side.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
-                                                   typename Cx<T>::T2* __restrict__ y) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
+                                               typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L = a.P;
     const int count = (int)a.n;
-    T2* acc = reinterpret_cast<T2*>(smem_raw);
-    T2* A = acc + L;
-    T2* B = A + L;
+    T2* A = reinterpret_cast<T2*>(smem_raw);
+    T2* acc = A + L;
     const int rhs = blockIdx.x;
     if (skipped(a, rhs)) return;
     const T2* xr = x + (int64_t)rhs * a.n;
@@ -250,15 +247,14 @@ __global__ void __launch_bounds__(kThreads) k_strip(const GridArgs<T> a, const t
             A[i] = v;
         }
         __syncthreads();
-        T2* U = fft_smem<false>(A, B, 1, L, 1, a.planP, a.twP);
-        T2* other = (U == A) ? B : A;
-        for (int i = threadIdx.x; i < L; i += blockDim.x) U[i] = cmul(U[i], __ldg(&a.spec[(int64_t)s * L + i]));
+        fft_inplace<false>(A, 1, L, 1, a.planP, a.twP);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) A[i] = cmul(A[i], __ldg(&a.spec[(int64_t)s * L + i]));
         __syncthreads();
-        T2* Y = fft_smem<true>(U, other, 1, L, 1, a.planP, a.twP);
+        fft_inplace<true>(A, 1, L, 1, a.planP, a.twP);
         for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            T2 v = Y[i];
-            if (s) v = cmulc(v, __ldg(&a.modP[i]));
-            acc[i] = s ? cadd(acc[i], v) : v;
+            T2 v = A[i];
+            if (s) v = cadd(acc[i], cmulc(v, __ldg(&a.modP[i])));
+            acc[i] = v;
         }
         __syncthreads();
     }
@@ -276,13 +272,6 @@ template <typename T> static void set_smem_attrs() {
     cudaFuncSetAttribute(k_grid_y_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     cudaFuncSetAttribute(k_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     done[dev & 63] = true;
-}
-
-static int tile_columns(int Q, int nbuf, size_t elem) {
-    int ti = 16;
-    while (ti > 1 && (size_t)nbuf * ti * Q * elem > (size_t)kSmemBudget) ti /= 2;
-    if ((size_t)nbuf * ti * Q * elem > (size_t)kSmemBudget) return 0;
-    return ti;
 }
 
 size_t GridApplicator::work_bytes_per_rhs() const {
@@ -331,9 +320,11 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     const size_t elem = sizeof(T2);
     if (g.mode == kStrip) {
         a.scale = (T)(1.0 / g.P);
-        const size_t smem = 3 * (size_t)g.P * elem;
-        if (smem > (size_t)kSmemBudget) return fail(RTM_ERR_UNSUPPORTED, "strip too long for this build");
-        k_strip<T><<<nrhs, kThreads, smem, s>>>(a, x, y);
+        const size_t smem = 2 * (size_t)g.P * elem;
+        const int thr = fft_threads(1, g.tP->plan);
+        if (smem > (size_t)kSmemBudget || thr > kMaxThreads)
+            return fail(RTM_ERR_UNSUPPORTED, "strip too long for this build");
+        k_strip<T><<<nrhs, thr, smem, s>>>(a, x, y);
         count_launch();
         RTM_CUDA(cudaGetLastError());
         return RTM_OK;
@@ -341,25 +332,38 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     a.scale = (T)(1.0 / ((double)g.P * g.Q));
     a.work = g.work.as<T2>();
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
-    const int ti_f = tile_columns(g.Q, 2, elem);
-    const int ti_i = tile_columns(g.Q, 3, elem);
-    const size_t smem_mix = 3 * 2 * (size_t)g.P * elem;
-    if (ti_f == 0 || ti_i == 0 || smem_mix > (size_t)kSmemBudget)
-        return fail(RTM_ERR_UNSUPPORTED, "FFT grid too large for this build");
-    const int rows_max = std::max(g.rows[0], g.rows[1]);
     const int passes = g.lean ? g.nsy : 1;
+    const int npy = g.lean ? 1 : g.nsy;
+    // y passes: TI x columns per CTA (rows of 64 bytes), fewer if two tiles would not fit.
+    int ti = sizeof(T) == 8 ? 4 : 8;
+    while (ti > 1 && (2 * (size_t)ti * g.Q * elem > (size_t)kSmemBudget || fft_threads(ti, g.tQ->plan) > kMaxThreads))
+        ti /= 2;
+    const int thr_y = fft_threads(ti, g.tQ->plan);
+    // x-mix: CB y frequencies per CTA (2 CB lines), as many as keep about 256 threads busy while
+    // the grid still has two waves of CTAs.
+    int cb = std::max(1, std::min(16, 2048 / g.P));
+    while (cb > 1 && (int64_t)((g.Q + cb - 1) / cb) * npy * nrhs < 2 * 148) cb /= 2;
+    const int ls = g.P | 1;
+    while (cb > 1 && (2 * (size_t)(2 * cb) * ls * elem > (size_t)kSmemBudget ||
+                      fft_threads(2 * cb, g.tP->plan) > kMaxThreads))
+        cb /= 2;
+    const size_t smem_mix = 2 * (size_t)(2 * cb) * ls * elem;
+    const int thr_x = fft_threads(2 * cb, g.tP->plan);
+    if (2 * (size_t)ti * g.Q * elem > (size_t)kSmemBudget || smem_mix > (size_t)kSmemBudget ||
+        thr_y > kMaxThreads || thr_x > kMaxThreads)
+        return fail(RTM_ERR_UNSUPPORTED, "FFT grid too large for this build");
+    a.ti = ti;
+    a.cb = cb;
+    a.ls = ls;
+    const int rows_max = std::max(g.rows[0], g.rows[1]);
+    const unsigned tiles = (unsigned)((rows_max + ti - 1) / ti);
     for (int pass = 0; pass < passes; ++pass) {
         a.py0 = g.lean ? pass : 0;
-        a.npy = g.lean ? 1 : g.nsy;
+        a.npy = npy;
         a.accumulate = g.lean && pass > 0;
-        a.ti = ti_f;
-        dim3 gf((rows_max + ti_f - 1) / ti_f, nrhs);
-        k_grid_y_fwd<T><<<gf, kThreads, 2 * (size_t)ti_f * g.Q * elem, s>>>(a, x);
-        dim3 gm(g.Q, a.npy, nrhs);
-        k_grid_x_mix<T><<<gm, kThreads, smem_mix, s>>>(a);
-        a.ti = ti_i;
-        dim3 gi((rows_max + ti_i - 1) / ti_i, nrhs);
-        k_grid_y_inv<T><<<gi, kThreads, 3 * (size_t)ti_i * g.Q * elem, s>>>(a, y);
+        k_grid_y_fwd<T><<<dim3(tiles, 2 * npy, nrhs), thr_y, (size_t)ti * g.Q * elem, s>>>(a, x);
+        k_grid_x_mix<T><<<dim3((g.Q + cb - 1) / cb, npy, nrhs), thr_x, smem_mix, s>>>(a);
+        k_grid_y_inv<T><<<dim3(tiles, 2, nrhs), thr_y, 2 * (size_t)ti * g.Q * elem, s>>>(a, y);
         count_launch(3);
         RTM_CUDA(cudaGetLastError());
     }
@@ -466,11 +470,10 @@ __device__ double2 gen_value(const GenArgs& a, const GenItem& it, int i, int j) 
     return make_double2(re, im);
 }
 
-__global__ void __launch_bounds__(kThreads) k_gen_y(const GenArgs a) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_gen_y(const GenArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q;
     double2* A = reinterpret_cast<double2*>(smem_raw);
-    double2* B = A + TI * Q;
     const GenItem& item = a.items[blockIdx.y];
     const int i0 = blockIdx.x * TI;
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
@@ -478,26 +481,25 @@ __global__ void __launch_bounds__(kThreads) k_gen_y(const GenArgs a) {
         A[it] = (i < a.P) ? gen_value(a, item, i, j) : make_double2(0, 0);
     }
     __syncthreads();
-    double2* out = fft_smem<false>(A, B, TI, 1, TI, a.planQ, a.twQ);
+    fft_inplace<false>(A, TI, 1, TI, a.planQ, a.twQ);
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
-        if (i < a.P) item.dst[(int64_t)j * a.P + i] = out[it];
+        if (i < a.P) item.dst[(int64_t)j * a.P + i] = A[it];
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_gen_x(const GenArgs a) {
+__global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = a.P;
     double2* A = reinterpret_cast<double2*>(smem_raw);
-    double2* B = A + P;
     const GenItem& item = a.items[blockIdx.y];
     const int j = blockIdx.x;
     double2* col = item.dst + (int64_t)j * P;
     for (int i = threadIdx.x; i < P; i += blockDim.x) A[i] = col[i];
     __syncthreads();
-    double2* out = fft_smem<false>(A, B, 1, P, 1, a.planP, a.twP);
+    fft_inplace<false>(A, 1, P, 1, a.planP, a.twP);
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        double2 v = out[i];
+        double2 v = A[i];
         if (a.realify) v.y = 0.0;
         col[i] = v;
     }
@@ -511,13 +513,18 @@ static int run_gen(GenArgs& a, cudaStream_t s) {
         attrs = true;
     }
     if (a.nitems == 0) return RTM_OK;
-    a.ti = tile_columns(a.Q, 2, sizeof(double2));
-    if (a.ti == 0 || 2 * (size_t)a.P * sizeof(double2) > (size_t)kSmemBudget)
+    a.ti = 4;
+    while (a.ti > 1 && ((size_t)a.ti * a.Q * sizeof(double2) > (size_t)kSmemBudget ||
+                        fft_threads(a.ti, a.planQ) > kMaxThreads))
+        a.ti /= 2;
+    const int thr_y = fft_threads(a.ti, a.planQ), thr_x = fft_threads(1, a.planP);
+    if ((size_t)a.ti * a.Q * sizeof(double2) > (size_t)kSmemBudget ||
+        (size_t)a.P * sizeof(double2) > (size_t)kSmemBudget || thr_y > kMaxThreads || thr_x > kMaxThreads)
         return fail(RTM_ERR_UNSUPPORTED, "spectra grid too large for this build");
     dim3 gy((a.P + a.ti - 1) / a.ti, a.nitems);
-    k_gen_y<<<gy, kThreads, 2 * (size_t)a.ti * a.Q * sizeof(double2), s>>>(a);
+    k_gen_y<<<gy, thr_y, (size_t)a.ti * a.Q * sizeof(double2), s>>>(a);
     dim3 gx(a.Q, a.nitems);
-    k_gen_x<<<gx, kThreads, 2 * (size_t)a.P * sizeof(double2), s>>>(a);
+    k_gen_x<<<gx, thr_x, (size_t)a.P * sizeof(double2), s>>>(a);
     count_launch(2);
     RTM_CUDA(cudaGetLastError());
     return RTM_OK;

@@ -80,6 +80,15 @@ __device__ __forceinline__ bool arrive(unsigned int* counter) {
     return last;
 }
 
+// Sum of nb partials by the whole CTA in a fixed order (every thread gets the total).
+__device__ __forceinline__ double2 cta_total(const double2* p, int nb) {
+    __shared__ double2 total;
+    double2 v[1] = {make_double2(0, 0)};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v[0] = dadd(v[0], p[b]);
+    block_sum<1>(v, &total);
+    return total;
+}
+
 // ============================================================================================
 // COCG
 struct CgState {
@@ -107,9 +116,8 @@ __global__ void __launch_bounds__(kRT) k_cg_start(const T2* __restrict__ b, cons
     double2* mine = part + ((int64_t)rhs * gridDim.x + blockIdx.x);
     block_sum<1>(acc, mine);
     if (!arrive(&st[rhs].counter)) return;
+    const double2 s = cta_total(part + (int64_t)rhs * gridDim.x, gridDim.x);
     if (threadIdx.x == 0) {
-        double2 s = make_double2(0, 0);
-        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
         CgState& S = st[rhs];
         S.bnorm = sqrt(s.x);
         S.iteration = 0;
@@ -143,9 +151,8 @@ __global__ void __launch_bounds__(kRT) k_cg_rz(const T2* __restrict__ r, const T
         acc[0] = dadd(acc[0], dmul(to_d2(rr[i]), to_d2(zr[i])));
     block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
     if (!arrive(&st[rhs].counter)) return;
+    const double2 s = cta_total(part + (int64_t)rhs * gridDim.x, gridDim.x);
     if (threadIdx.x == 0) {
-        double2 s = make_double2(0, 0);
-        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
         CgState& S = st[rhs];
         S.beta = S.iteration == 0 ? make_double2(0, 0) : ddiv(s, S.rho);
         S.rho = s;
@@ -182,11 +189,8 @@ __global__ void __launch_bounds__(kRT) k_cg_dq(const T2* __restrict__ d, const T
         acc[0] = dadd(acc[0], dmul(to_d2(dr[i]), to_d2(qr[i])));
     block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
     if (!arrive(&st[rhs].counter)) return;
-    if (threadIdx.x == 0) {
-        double2 s = make_double2(0, 0);
-        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
-        st[rhs].alpha = ddiv(st[rhs].rho, s);
-    }
+    const double2 s = cta_total(part + (int64_t)rhs * gridDim.x, gridDim.x);
+    if (threadIdx.x == 0) st[rhs].alpha = ddiv(st[rhs].rho, s);
 }
 
 // x += alpha d, r -= alpha q, then the relative residual, the history and the stopping tests.
@@ -215,9 +219,8 @@ __global__ void __launch_bounds__(kRT) k_cg_update(T2* __restrict__ x, T2* __res
     }
     block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
     if (!arrive(&st[rhs].counter)) return;
+    const double s = cta_total(part + (int64_t)rhs * gridDim.x, gridDim.x).x;
     if (threadIdx.x == 0) {
-        double s = 0;
-        for (int k = 0; k < (int)gridDim.x; ++k) s += part[(int64_t)rhs * gridDim.x + k].x;
         CgState& S = st[rhs];
         S.iteration += 1;
         const double h = sqrt(s) / S.bnorm;
@@ -275,9 +278,8 @@ __global__ void __launch_bounds__(kRT) k_gm_norm(const T2* __restrict__ w, int64
     double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
     block_sum<1>(acc, part + blockIdx.x);
     if (!arrive(&S.counter)) return;
+    const double s = cta_total(part, gridDim.x).x;
     if (threadIdx.x == 0) {
-        double s = 0;
-        for (int k = 0; k < (int)gridDim.x; ++k) s += part[k].x;
         const double nrm = sqrt(s);
         if (mode == 0) {
             S.ref = nrm;
@@ -350,15 +352,24 @@ __global__ void __launch_bounds__(kRT) k_gm_dot(const T2* __restrict__ V, const 
         double2 out[8];
         block_sum<8>(acc, out);
         if (threadIdx.x < 8 && k0 + threadIdx.x < cols)
-            part[(int64_t)blockIdx.x * (ar.m + 1) + k0 + threadIdx.x] = out[threadIdx.x];
+            part[(int64_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = out[threadIdx.x];
     }
     if (!arrive(&S.counter)) return;
-    for (int k = threadIdx.x; k < cols; k += blockDim.x) {
-        double2 s = make_double2(0, 0);
-        for (int b = 0; b < (int)gridDim.x; ++b) s = dadd(s, part[(int64_t)b * (ar.m + 1) + k]);
-        double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
-        ar.c[(int64_t)rhs * (ar.m + 1) + k] = s;
-        h[k] = pass == 0 ? s : dadd(h[k], s);
+    // One warp per column: lanes sum strided partials, then a shuffle tree (fixed order).
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = warp; k < cols; k += nw) {
+        double2 v = make_double2(0, 0);
+        const double2* pk = part + (int64_t)k * gridDim.x;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v = dadd(v, pk[b]);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+        }
+        if (lane == 0) {
+            double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
+            ar.c[(int64_t)rhs * (ar.m + 1) + k] = v;
+            h[k] = pass == 0 ? v : dadd(h[k], v);
+        }
     }
 }
 
@@ -390,9 +401,8 @@ __global__ void __launch_bounds__(kRT) k_gm_update(T2* __restrict__ w, const T2*
     double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
     block_sum<1>(acc, part + blockIdx.x);
     if (!arrive(&S.counter)) return;
+    const double s = cta_total(part, gridDim.x).x;
     if (threadIdx.x != 0) return;
-    double s = 0;
-    for (int k = 0; k < (int)gridDim.x; ++k) s += part[k].x;
     const double sub = sqrt(s);
     const int m = ar.m, j = S.step;
     double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
@@ -456,24 +466,59 @@ __global__ void __launch_bounds__(kRT) k_gm_next(const T2* __restrict__ w, T2* _
 }
 
 // y = H(1:step, 1:step) \ g(1:step) (upper triangular after the rotations; iterate_.m:73-74).
-__global__ void k_gm_solve(GmState* st, GmArrays ar, int nrhs) {
-    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
-    if (rhs >= nrhs) return;
+// One CTA per right-hand side: H and g are staged in shared memory, then column-oriented back
+// substitution (y_c = g_c / H_cc; g_i -= H_ic y_c for i < c, in parallel over i).
+__global__ void k_gm_solve(GmState* st, GmArrays ar, int staged) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int rhs = blockIdx.x;
     GmState& S = st[rhs];
     if (!S.cycle_ran) return;
     const int m = ar.m, k = S.step;
     const double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
     const double2* g = ar.g + (int64_t)rhs * (m + 1);
     double2* y = ar.y + (int64_t)rhs * m;
-    for (int i = k - 1; i >= 0; --i) {
-        double2 s = g[i];
-        for (int l = i + 1; l < k; ++l) {
-            const double2 p = dmul(H[(int64_t)l * (m + 1) + i], y[l]);
-            s.x -= p.x;
-            s.y -= p.y;
+    // staged: H (k x k, leading dimension k) and g in shared memory; otherwise read H in place and
+    // run the substitution in y.
+    const double2* Hs = H;
+    int ld = m + 1;
+    double2* gs = y;
+    if (staged) {
+        double2* hs = reinterpret_cast<double2*>(smem_raw);
+        for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+            const int r = t % k, c = t / k;
+            hs[t] = H[(int64_t)c * (m + 1) + r];
         }
-        y[i] = ddiv(s, H[(int64_t)i * (m + 1) + i]);
+        Hs = hs;
+        ld = k;
+        gs = hs + (int64_t)k * k;
     }
+    for (int t = threadIdx.x; t < k; t += blockDim.x) gs[t] = g[t];
+    __syncthreads();
+    for (int c = k - 1; c >= 0; --c) {
+        const double2 yc = ddiv(gs[c], Hs[(int64_t)c * ld + c]);
+        for (int i = threadIdx.x; i < c; i += blockDim.x) {
+            const double2 p = dmul(Hs[(int64_t)c * ld + i], yc);
+            gs[i].x -= p.x;
+            gs[i].y -= p.y;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) gs[c] = yc;
+        __syncthreads();
+    }
+    if (staged)
+        for (int t = threadIdx.x; t < k; t += blockDim.x) y[t] = gs[t];
+}
+
+static void launch_gm_solve(GmState* st, const GmArrays& ar, int nrhs, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    const size_t bytes = ((size_t)ar.m * ar.m + ar.m) * sizeof(double2);
+    const bool staged = bytes <= 200 * 1024;
+    k_gm_solve<<<nrhs, 128, staged ? bytes : 0, s>>>(st, ar, staged ? 1 : 0);
+    count_launch();
 }
 
 // x += V(:, 1:step) y.
@@ -529,11 +574,8 @@ __global__ void __launch_bounds__(kRT) k_true_residual(const T2* __restrict__ b,
     }
     block_sum<1>(acc, part + ((int64_t)rhs * gridDim.x + blockIdx.x));
     if (!arrive(&counters[rhs])) return;
-    if (threadIdx.x == 0) {
-        double2 s = make_double2(0, 0);
-        for (int k = 0; k < (int)gridDim.x; ++k) s = dadd(s, part[(int64_t)rhs * gridDim.x + k]);
-        res[rhs] = make_double2(sqrt(s.x), sqrt(s.y));
-    }
+    const double2 s = cta_total(part + (int64_t)rhs * gridDim.x, gridDim.x);
+    if (threadIdx.x == 0) res[rhs] = make_double2(sqrt(s.x), sqrt(s.y));
 }
 
 template <typename T2>
@@ -566,9 +608,10 @@ void convert_to_fp64(const float2* in, double2* out, int64_t n, cudaStream_t s) 
     count_launch();
 }
 
+// CTAs of the vector kernels: about two elements per thread, at most 4 waves of the 148 SMs.
 static int reduce_blocks(int64_t n) {
-    const int64_t b = (n + (int64_t)kRT * 4 - 1) / ((int64_t)kRT * 4);
-    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 296));
+    const int64_t b = (n + (int64_t)kRT * 2 - 1) / ((int64_t)kRT * 2);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 592));
 }
 
 // ============================================================================================
@@ -678,8 +721,12 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     const int m = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)cfg.restart, n, (int64_t)cfg.max_iterations}));
     const int nb = reduce_blocks(n);
     const size_t vec = (size_t)n * nrhs * sizeof(T2);
-    DeviceBuffer V, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
+    // Right (flexible) preconditioning keeps z_j = M v_j and solves A M u = b, x = Z y: the monitored
+    // residual is the residual of A x = b itself. Left preconditioning is the reference's form.
+    const bool right = M != nullptr && cfg.right_preconditioned;
+    DeviceBuffer V, Z, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
     RTM_TRY(V.alloc(vec * (m + 1)));
+    if (right) RTM_TRY(Z.alloc(vec * m));
     RTM_TRY(w.alloc(vec));
     RTM_TRY(t.alloc(vec));
     RTM_TRY(stb.alloc(sizeof(GmState) * nrhs));
@@ -717,8 +764,8 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     SkipFlags skip_step{&st[0].skip_step, stride};
     SkipFlags skip_done{&st[0].done, stride};
     const dim3 grid(nb, nrhs);
-    // reference = ||P b|| (iterate_.m:9)
-    if (M) RTM_TRY(M->apply(b, w.ptr, nrhs, s, SkipFlags{}));
+    // reference = ||P b|| (iterate_.m:9); ||b|| with right preconditioning
+    if (M && !right) RTM_TRY(M->apply(b, w.ptr, nrhs, s, SkipFlags{}));
     else RTM_CUDA(cudaMemcpyAsync(w.ptr, b, vec, cudaMemcpyDeviceToDevice, s));
     k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 0, 0);
     count_launch();
@@ -728,7 +775,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
         k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
         count_launch();
-        if (M) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
+        if (M && !right) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
         else RTM_CUDA(cudaMemcpyAsync(w.ptr, t.ptr, vec, cudaMemcpyDeviceToDevice, s));
         res.matvecs += 1;
     } else {
@@ -743,7 +790,11 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         count_launch();
         for (int j = 0; j < m; ++j) {
             T2* vj = Vp + (int64_t)j * nrhs * n;
-            if (M) {
+            if (right) {
+                T2* zj = Z.as<T2>() + (int64_t)j * nrhs * n;
+                RTM_TRY(M->apply(vj, zj, nrhs, s, skip_step));
+                RTM_TRY(A->apply(zj, w.ptr, nrhs, s, skip_step));
+            } else if (M) {
                 RTM_TRY(A->apply(vj, t.ptr, nrhs, s, skip_step));
                 RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_step));
             } else {
@@ -764,10 +815,10 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
                 if (!any) break;
             }
         }
-        k_gm_solve<<<(nrhs + 31) / 32, 32, 0, s>>>(st, ar, nrhs);
-        k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, Vp, n, nrhs, st, ar);
+        launch_gm_solve(st, ar, nrhs, s);
+        k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, right ? Z.as<T2>() : Vp, n, nrhs, st, ar);
         k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
-        count_launch(3);
+        count_launch(2);
         RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
         RTM_CUDA(cudaStreamSynchronize(s));
         bool all = true;
@@ -777,7 +828,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
         k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
         count_launch();
-        if (M) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
+        if (M && !right) RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_done));
         else RTM_CUDA(cudaMemcpyAsync(w.ptr, t.ptr, vec, cudaMemcpyDeviceToDevice, s));
         k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 0);
         count_launch();
@@ -850,57 +901,9 @@ __global__ void k_ir_check(const double2* res, int* done, int* converged, double
     done[rhs] = converged[rhs] || !isfinite(rel);
 }
 
-// One FGMRES(m) cycle in FP32 from x = 0 for the right-hand sides r32 (right preconditioning, the
-// preconditioned directions z_j = M v_j are kept, x = Z y). Returns the inner iterations done.
-static int fgmres_cycle(LinearOp* A, LinearOp* M, const float2* r32, float2* x32, int64_t n, int nrhs, int m,
-                        double tol, DeviceBuffer& V, DeviceBuffer& Z, DeviceBuffer& w, DeviceBuffer& stb,
-                        GmArrays& ar, std::vector<GmState>& host, cudaStream_t s) {
-    const int nb = reduce_blocks(n);
-    const dim3 grid(nb, nrhs);
-    std::vector<GmState> init(nrhs);
-    for (auto& st : init) {
-        memset(&st, 0, sizeof st);
-        st.tol = tol;
-        st.max_iterations = m;
-        st.m = m;
-        st.skip_step = 1;
-    }
-    RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(GmState) * nrhs, cudaMemcpyHostToDevice, s));
-    GmState* st = stb.as<GmState>();
-    const int stride = (int)(sizeof(GmState) / sizeof(int));
-    SkipFlags skip_step{&st[0].skip_step, stride};
-    const size_t vec = (size_t)n * nrhs * sizeof(float2);
-    RTM_CUDA(cudaMemcpyAsync(w.ptr, r32, vec, cudaMemcpyDeviceToDevice, s));
-    RTM_CUDA(cudaMemsetAsync(x32, 0, vec, s));
-    k_gm_norm<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), n, st, ar, 0, 0);
-    k_gm_norm<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), n, st, ar, 1, 1);
-    k_gm_v0<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), V.as<float2>(), n, nrhs, st);
-    count_launch(3);
-    float2* Vp = V.as<float2>();
-    float2* Zp = M ? Z.as<float2>() : Vp;
-    for (int j = 0; j < m; ++j) {
-        float2* vj = Vp + (int64_t)j * nrhs * n;
-        float2* zj = Zp + (int64_t)j * nrhs * n;
-        if (M) RTM_TRY(M->apply(vj, zj, nrhs, s, skip_step));
-        RTM_TRY(A->apply(zj, w.ptr, nrhs, s, skip_step));
-        k_gm_dot<float2><<<grid, kRT, 0, s>>>(Vp, w.as<float2>(), n, nrhs, st, ar, 0);
-        k_gm_update<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st, ar, 0);
-        k_gm_dot<float2><<<grid, kRT, 0, s>>>(Vp, w.as<float2>(), n, nrhs, st, ar, 1);
-        k_gm_update<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st, ar, 1);
-        k_gm_next<float2><<<grid, kRT, 0, s>>>(w.as<float2>(), Vp, n, nrhs, st);
-        count_launch(5);
-        RTM_CUDA(cudaGetLastError());
-    }
-    k_gm_solve<<<(nrhs + 31) / 32, 32, 0, s>>>(st, ar, nrhs);
-    k_gm_xupdate<float2><<<grid, kRT, 0, s>>>(x32, Zp, n, nrhs, st, ar);
-    k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
-    count_launch(3);
-    RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
-    RTM_CUDA(cudaStreamSynchronize(s));
-    int most = 0;
-    for (auto& h : host) most = std::max(most, h.iteration);
-    return most;
-}
+template <typename T>
+static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv, const void* x0v, void* xv, int64_t n,
+                 int nrhs, SolveResult& res, cudaStream_t s);
 
 int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& cfg, const void* bv, const void* x0v,
                 void* xv, int64_t n, int nrhs, SolveResult& res, cudaStream_t s) {
@@ -931,29 +934,7 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     RTM_TRY(A64->reserve(nrhs));
     RTM_TRY(A32->reserve(nrhs));
     if (M32) RTM_TRY(M32->reserve(nrhs));
-    // FGMRES buffers (inner state, FP32 basis and preconditioned directions).
-    DeviceBuffer V, Z, w, stb, H, g, cs, sn, h, c, y, ipart, ihist;
     const bool inner_cg = cfg.method == RTM_METHOD_CG;
-    GmArrays ar{};
-    std::vector<GmState> ghost(nrhs);
-    if (!inner_cg) {
-        RTM_TRY(V.alloc(vec32 * (m + 1)));
-        if (M32) RTM_TRY(Z.alloc(vec32 * m));
-        RTM_TRY(w.alloc(vec32));
-        RTM_TRY(stb.alloc(sizeof(GmState) * nrhs));
-        RTM_TRY(H.alloc(sizeof(double2) * (m + 1) * m * nrhs));
-        RTM_TRY(g.alloc(sizeof(double2) * (m + 1) * nrhs));
-        RTM_TRY(cs.alloc(sizeof(double2) * m * nrhs));
-        RTM_TRY(sn.alloc(sizeof(double2) * m * nrhs));
-        RTM_TRY(h.alloc(sizeof(double2) * (m + 1) * nrhs));
-        RTM_TRY(c.alloc(sizeof(double2) * (m + 1) * nrhs));
-        RTM_TRY(y.alloc(sizeof(double2) * m * nrhs));
-        RTM_TRY(ipart.alloc(sizeof(double2) * (size_t)nb * (m + 1) * nrhs));
-        RTM_TRY(ihist.alloc(sizeof(double) * (m + 1) * nrhs));
-        RTM_CUDA(cudaMemsetAsync(H.ptr, 0, H.bytes, s));
-        ar = GmArrays{H.as<double2>(), g.as<double2>(), cs.as<double2>(), sn.as<double2>(), h.as<double2>(),
-                      c.as<double2>(), y.as<double2>(), ipart.as<double2>(), ihist.as<double>(), m + 1, m};
-    }
     if (x0) RTM_CUDA(cudaMemcpyAsync(x, x0, vec64, cudaMemcpyDeviceToDevice, s));
     else RTM_CUDA(cudaMemsetAsync(x, 0, vec64, s));
     int inner_total = 0, steps = 0;
@@ -976,25 +957,21 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         if (all || step >= cfg.max_refinements || inner_total >= cfg.max_iterations) break;
         k_ir_to32<<<grid, kRT, 0, s>>>(r64.as<double2>(), r32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
-        if (inner_cg) {
-            SolveConfig ic;
-            ic.method = RTM_METHOD_CG;
-            ic.tolerance = cfg.inner_tolerance;
-            ic.max_iterations = std::max(1, cfg.restart);
-            ic.check_every = cfg.check_every;
-            SolveResult ir;
-            RTM_TRY(cocg<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
-            int most = 0;
-            for (auto& st : ir.stats) most = std::max(most, st.iteration_count);
-            inner_total += most;
-            res.matvecs += ir.matvecs + most + 1;
-        } else {
-            const int it = fgmres_cycle(A32, M32, r32.as<float2>(), d32.as<float2>(), n, nrhs, m, cfg.inner_tolerance,
-                                        V, Z, w, stb, ar, ghost, s);
-            if (it < 0) return it;
-            inner_total += it;
-            res.matvecs += it;
-        }
+        // The inner FP32 solve of A32 d = r / ||r||: COCG, or restarted flexible GMRES(m).
+        SolveConfig ic;
+        ic.method = inner_cg ? RTM_METHOD_CG : RTM_METHOD_GMRES;
+        ic.tolerance = cfg.inner_tolerance;
+        ic.max_iterations = std::max(1, cfg.max_iterations - inner_total);
+        ic.restart = m;
+        ic.check_every = cfg.check_every;
+        ic.right_preconditioned = 1;
+        SolveResult ir;
+        if (inner_cg) RTM_TRY(cocg<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
+        else RTM_TRY(gmres<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
+        int most = 0;
+        for (auto& st : ir.stats) most = std::max(most, st.iteration_count);
+        inner_total += most;
+        res.matvecs += ir.matvecs + most + 1;
         k_ir_update<<<grid, kRT, 0, s>>>(x, d32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
     }

@@ -15,6 +15,7 @@ struct SolveConfig {
     int check_every = 0;
     double inner_tolerance = 1e-4;
     int max_refinements = 20;
+    int right_preconditioned = 0;  // GMRES: 0 left (the reference's form), 1 right (flexible)
 };
 
 struct SolveResult {
