@@ -125,7 +125,7 @@ template <int R, bool INV, typename T2> __device__ __forceinline__ void dft_odd(
     T2 w[R];
 #pragma unroll
     for (int m = 0; m < R; ++m) {
-        T2 t = __ldg(&tw[m * st]);
+        T2 t = tw[m * st];
         w[m] = INV ? cconj(t) : t;
     }
     T2 out[R];
@@ -172,7 +172,7 @@ __host__ __device__ inline int fft_threads(int lines, const FftPlan& p) {
 // One in-place Stockham stage: every thread loads its butterflies into registers, the CTA
 // synchronises, then every thread stores them. Needs items = lines n / R <= IPT blockDim.x.
 template <int R, int IPT, bool INV, typename T2>
-__device__ __noinline__ void pass_ip(T2* buf, int n, int Ns, int lines, int ls, int es, const T2* __restrict__ tw) {
+__device__ __forceinline__ void pass_ip_body(T2* buf, int n, int Ns, int lines, int ls, int es, const T2* tw) {
     const int nb = n / R;
     const int stride = n / (Ns * R);
     const int items = lines * nb;
@@ -188,7 +188,7 @@ __device__ __noinline__ void pass_ip(T2* buf, int n, int Ns, int lines, int ls, 
             if (Ns > 1) {
 #pragma unroll
                 for (int t = 1; t < R; ++t) {
-                    const T2 w = __ldg(&tw[t * k * stride]);
+                    const T2 w = tw[t * k * stride];
                     v[q][t] = INV ? cmulc(v[q][t], w) : cmul(v[q][t], w);
                 }
             }
@@ -210,10 +210,15 @@ __device__ __noinline__ void pass_ip(T2* buf, int n, int Ns, int lines, int ls, 
     __syncthreads();
 }
 
+template <int R, int IPT, bool INV, typename T2>
+__device__ __noinline__ void pass_ip(T2* buf, int n, int Ns, int lines, int ls, int es, const T2* tw) {
+    pass_ip_body<R, IPT, INV>(buf, n, Ns, lines, ls, es, tw);
+}
+
 // Any radix up to kMaxGenericRadix (rare: sizes with a prime factor above 7) by a direct DFT; one
 // butterfly per thread suffices since R > 16.
 template <bool INV, typename T2>
-__device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int lines, int ls, int es, const T2* __restrict__ tw) {
+__device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int lines, int ls, int es, const T2* tw) {
     const int nb = n / R;
     const int stride = n / (Ns * R);
     const int st = n / R;
@@ -229,7 +234,7 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
         for (int t = 0; t < R; ++t) {
             T2 x = s[(j + t * nb) * es];
             if (Ns > 1 && t > 0) {
-                const T2 w = __ldg(&tw[t * k * stride]);
+                const T2 w = tw[t * k * stride];
                 x = INV ? cmulc(x, w) : cmul(x, w);
             }
             v[t] = x;
@@ -242,7 +247,7 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
         for (int q = 0; q < R; ++q) {
             T2 acc = v[0];
             for (int t = 1; t < R; ++t) {
-                const T2 w = __ldg(&tw[((t * q) % R) * st]);
+                const T2 w = tw[((t * q) % R) * st];
                 acc = cadd(acc, INV ? cmulc(v[t], w) : cmul(v[t], w));
             }
             d[(base + q * Ns) * es] = acc;
@@ -252,25 +257,43 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
 }
 
 // Transforms, in place, the `lines` lines of length p.n in buf (element e of line l at
-// buf[l * ls + e * es]). Needs blockDim.x >= fft_threads(lines, p.n); call it after a
-// __syncthreads() that makes buf visible; it returns after one.
-template <bool INV, typename T2>
-__device__ void fft_inplace(T2* buf, int lines, int ls, int es, const FftPlan& p, const T2* __restrict__ tw) {
+// buf[l * ls + e * es]); tw (global or shared) holds the p.n roots. Needs blockDim.x >=
+// fft_threads(lines, p); call it after a __syncthreads() that makes buf visible; it returns after
+// one. POW2 instantiates radices 16, 8, 4 and 2 inline (lengths that are powers of two); otherwise
+// every radix runs as a separate function.
+template <bool INV, bool POW2, typename T2>
+__device__ __forceinline__ void fft_inplace(T2* buf, int lines, int ls, int es, const FftPlan& p, const T2* tw) {
     int Ns = 1;
     for (int s = 0; s < p.nstages; ++s) {
         const int r = p.radix[s];
-        switch (r) {
-            case 2: pass_ip<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 3: pass_ip<3, 6, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 4: pass_ip<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 5: pass_ip<5, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 7: pass_ip<7, 3, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 8: pass_ip<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            case 16: pass_ip<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-            default: pass_ip_generic<INV>(buf, p.n, r, Ns, lines, ls, es, tw); break;
+        if constexpr (POW2) {
+            switch (r) {
+                case 2: pass_ip_body<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 4: pass_ip_body<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 8: pass_ip_body<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                default: pass_ip_body<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+            }
+        } else {
+            switch (r) {
+                case 2: pass_ip<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 3: pass_ip<3, 6, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 4: pass_ip<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 5: pass_ip<5, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 7: pass_ip<7, 3, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 8: pass_ip<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 16: pass_ip<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                default: pass_ip_generic<INV>(buf, p.n, r, Ns, lines, ls, es, tw); break;
+            }
         }
         Ns *= r;
     }
+}
+
+// True when every radix of the plan is a power of two (the POW2 instantiation applies).
+__host__ __device__ inline bool fft_pow2(const FftPlan& p) {
+    for (int s = 0; s < p.nstages; ++s)
+        if (p.radix[s] != 2 && p.radix[s] != 4 && p.radix[s] != 8 && p.radix[s] != 16) return false;
+    return true;
 }
 
 }  // namespace rtm

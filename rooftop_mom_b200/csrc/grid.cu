@@ -59,218 +59,216 @@ template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rh
     return a.skip != nullptr && a.skip[(int64_t)rhs * a.skip_stride] != 0;
 }
 
+// Copies the n roots of unity into shared memory (ordered before use by the caller's barrier).
+template <typename T2> __device__ __forceinline__ void stage_roots(T2* dst, const T2* __restrict__ src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
 // --------------------------------------------------------------------------------------------
-// y-forward: W[py][c][j][i] = FFT_y( x_c(i, j) * mody(j)^py ) for a tile of TI x columns of one
-// component c and one y subband py (grid: tiles x (component, subband) x right-hand sides).
-template <typename T>
+// y-forward: for a tile of TI x columns of component c, both y subbands at once:
+// W[py][c][j][i] = FFT_y( x_c(i, j) mody(j)^py ). Shared tile A[j][L], L = npy TI lines,
+// line pyi TI + l (grid: tiles x components x right-hand sides).
+template <typename T, bool POW2>
 __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int TI = a.ti, Q = a.Q;
+    const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    const int c = blockIdx.y % a.ncomp, pyi = blockIdx.y / a.ncomp, py = a.py0 + pyi;
-    const int rhs = blockIdx.z;
+    T2* tws = A + (size_t)L * Q;
+    const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
     if (i0 >= rows || skipped(a, rhs)) return;
+    stage_roots(tws, a.twQ, Q);
     const T2* xr = x + (int64_t)rhs * a.n + a.off[c];
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
         T2 v = czero<T2>();
-        if (i < rows && j < cols) {
-            v = xr[i + (int64_t)j * rows];
-            if (py) v = cmul(v, __ldg(&a.modQ[j]));
+        if (i < rows && j < cols) v = xr[i + (int64_t)j * rows];
+        T2* row = A + (size_t)j * L + l;
+        if (a.npy == 2) {
+            row[0] = v;
+            row[TI] = cmul(v, __ldg(&a.modQ[j]));
+        } else {
+            row[0] = a.py0 ? cmul(v, __ldg(&a.modQ[j])) : v;
         }
-        A[it] = v;
     }
     __syncthreads();
-    fft_inplace<false>(A, TI, 1, TI, a.planQ, a.twQ);
-    T2* dst = a.work + (int64_t)rhs * a.work_rhs + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
-    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-        const int l = it % TI, j = it / TI, i = i0 + l;
-        if (i < rows) dst[(int64_t)j * a.P + i] = A[it];
+    fft_inplace<false, POW2>(A, L, 1, L, a.planQ, tws);
+    T2* dst = a.work + (int64_t)rhs * a.work_rhs;
+    for (int it = threadIdx.x; it < L * Q; it += blockDim.x) {
+        const int l = it % L, j = it / L;
+        const int pyi = l / TI, i = i0 + (l - pyi * TI);
+        if (i < rows) dst[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] = A[it];
     }
 }
 
 // --------------------------------------------------------------------------------------------
-// x-mix: for CB y frequencies j of the y subband py and both components: sum over px of
-// demod_x^px IFFT_x( B(px, py) FFT_x( W mod_x^px ) ), scaled by 1/(PQ), in place in W. The
-// 2 CB lines sit in shared memory with an odd line stride (a.ls) so that consecutive lines fall on
-// different banks.
-template <typename T>
+// x-mix: CB y frequencies j of the y subband py; for both components and both x subbands at once
+// (line (jj nsx + px) nc + c): sum over px of demod_x^px IFFT_x( B(px, py) FFT_x( W mod_x^px ) ),
+// scaled by 1/(PQ), in place in W. Lines have an odd stride (a.ls) to spread the banks.
+template <typename T, bool POW2>
 __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_x_mix(const GridArgs<T> a) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int P = a.P, Q = a.Q, nc = a.ncomp, CB = a.cb, ls = a.ls;
-    const int lines = nc * CB;
+    const int P = a.P, Q = a.Q, nc = a.ncomp, CB = a.cb, ls = a.ls, nsx = a.nsx;
+    const int lines = CB * nsx * nc;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* acc = A + lines * ls;
+    T2* tws = A + (size_t)lines * ls;
     const int j0 = blockIdx.x * CB;
     const int pyi = blockIdx.y;
     const int py = a.py0 + pyi;
     const int rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
+    stage_roots(tws, a.twP, P);
     T2* wr = a.work + (int64_t)rhs * a.work_rhs + (int64_t)pyi * nc * Q * P;
-    const T2* vy = py ? a.vy1 : a.vy0;
-    // line l = jj * nc + c: column j0 + jj of component c
-    for (int px = 0; px < a.nsx; ++px) {
-        for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
-            const int l = it / P, i = it - l * P;
-            const int c = l % nc, j = j0 + l / nc;
-            T2 v = czero<T2>();
-            if (i < a.rows[c] && j < Q) {
-                v = wr[((int64_t)c * Q + j) * P + i];
-                if (px) v = cmul(v, __ldg(&a.modP[i]));
-            }
-            A[l * ls + i] = v;
-        }
-        __syncthreads();
-        fft_inplace<false>(A, lines, ls, 1, a.planP, a.twP);
-        const int sub = px + a.nsx * py;
-        const T2* ux = px ? a.ux1 : a.ux0;
-        for (int it = threadIdx.x; it < CB * P; it += blockDim.x) {
-            const int jj = it / P, i = it - jj * P, j = j0 + jj;
-            if (j >= Q) continue;
-            T2* lx = A + (jj * nc) * ls;
-            T2* ly = lx + ls;
-            const T2 sx = lx[i], sy = ly[i];
-            T2 ox, oy;
-            if (a.mode == kGen3) {
-                const int64_t base = ((int64_t)(sub * 3) * Q + j) * P + i;
-                const T2 E = __ldg(&a.spec[base]);
-                const T2 Mx = __ldg(&a.spec[base + (int64_t)Q * P]);
-                const T2 My = __ldg(&a.spec[base + 2 * (int64_t)Q * P]);
-                const T2 u = __ldg(&ux[i]);
-                const T2 v = __ldg(&vy[j]);
-                const T cu = (u.x * u.x + u.y * u.y) * a.inv_a2;
-                const T cv = (v.x * v.x + v.y * v.y) * a.inv_b2;
-                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E.
-                T2 qc = cmulc(u, v);
-                qc.x = -qc.x * a.inv_ab;
-                qc.y = -qc.y * a.inv_ab;
-                const T2 Ex = cmul(E, sx), Ey = cmul(E, sy);
-                ox = csub(cmul(Mx, sx), cscale(Ex, cu));
-                ox = cadd(ox, cmul(qc, Ey));
-                oy = csub(cmul(My, sy), cscale(Ey, cv));
-                oy = cadd(oy, cmul(cconj(qc), Ex));
-            } else {
-                const int64_t base = (int64_t)j * P + i, blk = (int64_t)Q * P;
-                const T2 XX = __ldg(&a.spec[base]), XY = __ldg(&a.spec[base + blk]);
-                const T2 YX = __ldg(&a.spec[base + 2 * blk]), YY = __ldg(&a.spec[base + 3 * blk]);
-                ox = cadd(cmul(XX, sx), cmul(XY, sy));
-                oy = cadd(cmul(YX, sx), cmul(YY, sy));
-            }
-            lx[i] = ox;
-            ly[i] = oy;
-        }
-        __syncthreads();
-        fft_inplace<true>(A, lines, ls, 1, a.planP, a.twP);
-        for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
-            const int l = it / P, i = it - l * P;
-            T2 v = A[l * ls + i];
-            if (px) v = cadd(acc[l * ls + i], cmulc(v, __ldg(&a.modP[i])));
-            acc[l * ls + i] = v;
-        }
-        __syncthreads();
+    for (int it = threadIdx.x; it < CB * nc * P; it += blockDim.x) {
+        const int jc = it / P, i = it - jc * P;
+        const int jj = jc / nc, c = jc - jj * nc, j = j0 + jj;
+        T2 v = czero<T2>();
+        if (i < a.rows[c] && j < Q) v = wr[((int64_t)c * Q + j) * P + i];
+        A[(size_t)((jj * nsx) * nc + c) * ls + i] = v;
+        if (nsx == 2) A[(size_t)((jj * nsx + 1) * nc + c) * ls + i] = cmul(v, __ldg(&a.modP[i]));
     }
-    for (int it = threadIdx.x; it < lines * P; it += blockDim.x) {
-        const int l = it / P, i = it - l * P;
-        const int c = l % nc, j = j0 + l / nc;
-        if (i < a.rows[c] && j < Q) wr[((int64_t)c * Q + j) * P + i] = cscale(acc[l * ls + i], a.scale);
+    __syncthreads();
+    fft_inplace<false, POW2>(A, lines, ls, 1, a.planP, tws);
+    const T2* vy = py ? a.vy1 : a.vy0;
+    for (int it = threadIdx.x; it < CB * nsx * P; it += blockDim.x) {
+        const int jp = it / P, i = it - jp * P;
+        const int jj = jp / nsx, px = jp - jj * nsx, j = j0 + jj;
+        if (j >= Q) continue;
+        T2* lx = A + (size_t)(jp * nc) * ls;
+        T2* ly = lx + ls;
+        const T2 sx = lx[i], sy = ly[i];
+        const int sub = px + nsx * py;
+        T2 ox, oy;
+        if (a.mode == kGen3) {
+            const int64_t base = ((int64_t)(sub * 3) * Q + j) * P + i;
+            const T2 E = __ldg(&a.spec[base]);
+            const T2 Mx = __ldg(&a.spec[base + (int64_t)Q * P]);
+            const T2 My = __ldg(&a.spec[base + 2 * (int64_t)Q * P]);
+            const T2 u = __ldg(&(px ? a.ux1 : a.ux0)[i]);
+            const T2 v = __ldg(&vy[j]);
+            const T cu = (u.x * u.x + u.y * u.y) * a.inv_a2;
+            const T cv = (v.x * v.x + v.y * v.y) * a.inv_b2;
+            // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E.
+            T2 qc = cmulc(u, v);
+            qc.x = -qc.x * a.inv_ab;
+            qc.y = -qc.y * a.inv_ab;
+            const T2 Ex = cmul(E, sx), Ey = cmul(E, sy);
+            ox = csub(cmul(Mx, sx), cscale(Ex, cu));
+            ox = cadd(ox, cmul(qc, Ey));
+            oy = csub(cmul(My, sy), cscale(Ey, cv));
+            oy = cadd(oy, cmul(cconj(qc), Ex));
+        } else {
+            const int64_t base = (int64_t)j * P + i, blk = (int64_t)Q * P;
+            const T2 XX = __ldg(&a.spec[base]), XY = __ldg(&a.spec[base + blk]);
+            const T2 YX = __ldg(&a.spec[base + 2 * blk]), YY = __ldg(&a.spec[base + 3 * blk]);
+            ox = cadd(cmul(XX, sx), cmul(XY, sy));
+            oy = cadd(cmul(YX, sx), cmul(YY, sy));
+        }
+        lx[i] = ox;
+        ly[i] = oy;
+    }
+    __syncthreads();
+    fft_inplace<true, POW2>(A, lines, ls, 1, a.planP, tws);
+    for (int it = threadIdx.x; it < CB * nc * P; it += blockDim.x) {
+        const int jc = it / P, i = it - jc * P;
+        const int jj = jc / nc, c = jc - jj * nc, j = j0 + jj;
+        if (i >= a.rows[c] || j >= Q) continue;
+        T2 v = A[(size_t)((jj * nsx) * nc + c) * ls + i];
+        if (nsx == 2) v = cadd(v, cmulc(A[(size_t)((jj * nsx + 1) * nc + c) * ls + i], __ldg(&a.modP[i])));
+        wr[((int64_t)c * Q + j) * P + i] = cscale(v, a.scale);
     }
 }
 
 // --------------------------------------------------------------------------------------------
 // y-inverse: y_c(i, j) = sum_py demod_y^py IFFT_y(W[py][c][:, i]) for a tile of TI columns of one
-// component, cropped to the rooftop grid (grid: tiles x components x right-hand sides).
-template <typename T>
+// component, both y subbands at once (tile A[j][L] as in the y-forward), cropped to the rooftop grid.
+template <typename T, bool POW2>
 __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int TI = a.ti, Q = a.Q;
+    const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* acc = A + TI * Q;
+    T2* tws = A + (size_t)L * Q;
     const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
     if (i0 >= rows || skipped(a, rhs)) return;
+    stage_roots(tws, a.twQ, Q);
     const T2* wr = a.work + (int64_t)rhs * a.work_rhs;
-    for (int pyi = 0; pyi < a.npy; ++pyi) {
-        const int py = a.py0 + pyi;
-        const T2* src = wr + ((int64_t)(pyi * a.ncomp + c) * Q) * a.P;
-        for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-            const int l = it % TI, j = it / TI, i = i0 + l;
-            A[it] = (i < rows) ? src[(int64_t)j * a.P + i] : czero<T2>();
-        }
-        __syncthreads();
-        fft_inplace<true>(A, TI, 1, TI, a.planQ, a.twQ);
-        for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-            const int j = it / TI;
-            T2 v = A[it];
-            if (py) v = cmulc(v, __ldg(&a.modQ[j]));
-            acc[it] = pyi ? cadd(acc[it], v) : v;
-        }
-        __syncthreads();
+    for (int it = threadIdx.x; it < L * Q; it += blockDim.x) {
+        const int l = it % L, j = it / L;
+        const int pyi = l / TI, i = i0 + (l - pyi * TI);
+        A[it] = (i < rows) ? wr[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] : czero<T2>();
     }
+    __syncthreads();
+    fft_inplace<true, POW2>(A, L, 1, L, a.planQ, tws);
     T2* yr = y + (int64_t)rhs * a.n + a.off[c];
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
-        if (i < rows && j < cols) {
-            const int64_t idx = i + (int64_t)j * rows;
-            yr[idx] = a.accumulate ? cadd(yr[idx], acc[it]) : acc[it];
-        }
+        if (i >= rows || j >= cols) continue;
+        const T2* row = A + (size_t)j * L + l;
+        T2 v;
+        if (a.npy == 2) v = cadd(row[0], cmulc(row[TI], __ldg(&a.modQ[j])));
+        else v = a.py0 ? cmulc(row[0], __ldg(&a.modQ[j])) : row[0];
+        const int64_t idx = i + (int64_t)j * rows;
+        yr[idx] = a.accumulate ? cadd(yr[idx], v) : v;
     }
 }
 
 // --------------------------------------------------------------------------------------------
-// Strip: y = sum_s demod^s IFFT( B_s * FFT( x * mod^s ) ) / L on one line per right-hand side.
-template <typename T>
+// Strip: y = sum_s demod^s IFFT( B_s FFT( x mod^s ) ) / L, the subbands as lines of one transform.
+template <typename T, bool POW2>
 __global__ void __launch_bounds__(kMaxThreads, 1) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
-                                               typename Cx<T>::T2* __restrict__ y) {
+                                                         typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L = a.P;
+    const int L = a.P, ls = a.ls, ns = a.nsx;
     const int count = (int)a.n;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* acc = A + L;
+    T2* tws = A + (size_t)ns * ls;
     const int rhs = blockIdx.x;
     if (skipped(a, rhs)) return;
+    stage_roots(tws, a.twP, L);
     const T2* xr = x + (int64_t)rhs * a.n;
     T2* yr = y + (int64_t)rhs * a.n;
-    for (int s = 0; s < a.nsx; ++s) {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            T2 v = czero<T2>();
-            if (i < count) {
-                v = xr[i];
-                if (s) v = cmul(v, __ldg(&a.modP[i]));
-            }
-            A[i] = v;
-        }
-        __syncthreads();
-        fft_inplace<false>(A, 1, L, 1, a.planP, a.twP);
-        for (int i = threadIdx.x; i < L; i += blockDim.x) A[i] = cmul(A[i], __ldg(&a.spec[(int64_t)s * L + i]));
-        __syncthreads();
-        fft_inplace<true>(A, 1, L, 1, a.planP, a.twP);
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            T2 v = A[i];
-            if (s) v = cadd(acc[i], cmulc(v, __ldg(&a.modP[i])));
-            acc[i] = v;
-        }
-        __syncthreads();
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        const T2 v = i < count ? xr[i] : czero<T2>();
+        A[i] = v;
+        if (ns == 2) A[ls + i] = cmul(v, __ldg(&a.modP[i]));
     }
-    for (int i = threadIdx.x; i < count; i += blockDim.x) yr[i] = cscale(acc[i], a.scale);
+    __syncthreads();
+    fft_inplace<false, POW2>(A, ns, ls, 1, a.planP, tws);
+    for (int it = threadIdx.x; it < ns * L; it += blockDim.x) {
+        const int s = it / L, i = it - s * L;
+        A[s * ls + i] = cmul(A[s * ls + i], __ldg(&a.spec[(int64_t)s * L + i]));
+    }
+    __syncthreads();
+    fft_inplace<true, POW2>(A, ns, ls, 1, a.planP, tws);
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        T2 v = A[i];
+        if (ns == 2) v = cadd(v, cmulc(A[ls + i], __ldg(&a.modP[i])));
+        yr[i] = cscale(v, a.scale);
+    }
 }
 
 // --------------------------------------------------------------------------------------------
+template <typename T, bool POW2> static void set_attrs_one() {
+    cudaFuncSetAttribute(k_grid_y_fwd<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_grid_x_mix<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_grid_y_inv<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_strip<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
 template <typename T> static void set_smem_attrs() {
     static bool done[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (done[dev & 63]) return;
-    cudaFuncSetAttribute(k_grid_y_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_grid_x_mix<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_grid_y_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    set_attrs_one<T, true>();
+    set_attrs_one<T, false>();
     done[dev & 63] = true;
 }
 
@@ -320,11 +318,13 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     const size_t elem = sizeof(T2);
     if (g.mode == kStrip) {
         a.scale = (T)(1.0 / g.P);
-        const size_t smem = 2 * (size_t)g.P * elem;
-        const int thr = fft_threads(1, g.tP->plan);
+        a.ls = g.P | 1;
+        const size_t smem = ((size_t)g.nsx * a.ls + g.P) * elem;
+        const int thr = fft_threads(g.nsx, g.tP->plan);
         if (smem > (size_t)kSmemBudget || thr > kMaxThreads)
             return fail(RTM_ERR_UNSUPPORTED, "strip too long for this build");
-        k_strip<T><<<nrhs, thr, smem, s>>>(a, x, y);
+        if (fft_pow2(g.tP->plan)) k_strip<T, true><<<nrhs, thr, smem, s>>>(a, x, y);
+        else k_strip<T, false><<<nrhs, thr, smem, s>>>(a, x, y);
         count_launch();
         RTM_CUDA(cudaGetLastError());
         return RTM_OK;
@@ -334,36 +334,40 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
     const int passes = g.lean ? g.nsy : 1;
     const int npy = g.lean ? 1 : g.nsy;
-    // y passes: TI x columns per CTA (rows of 64 bytes), fewer if two tiles would not fit.
+    // y passes: TI x columns per CTA (rows of 64 bytes) for every y subband at once; fewer columns
+    // while the tile (plus the roots) would not fit or would need more than kMaxThreads threads.
     int ti = sizeof(T) == 8 ? 4 : 8;
-    while (ti > 1 && (2 * (size_t)ti * g.Q * elem > (size_t)kSmemBudget || fft_threads(ti, g.tQ->plan) > kMaxThreads))
-        ti /= 2;
-    const int thr_y = fft_threads(ti, g.tQ->plan);
-    // x-mix: CB y frequencies per CTA (2 CB lines), as many as keep about 256 threads busy while
-    // the grid still has two waves of CTAs.
-    int cb = std::max(1, std::min(16, 2048 / g.P));
-    while (cb > 1 && (int64_t)((g.Q + cb - 1) / cb) * npy * nrhs < 2 * 148) cb /= 2;
+    auto y_smem = [&](int t) { return ((size_t)npy * t * g.Q + g.Q) * elem; };
+    while (ti > 1 && (y_smem(ti) > (size_t)kSmemBudget || fft_threads(npy * ti, g.tQ->plan) > kMaxThreads)) ti /= 2;
+    const int thr_y = fft_threads(npy * ti, g.tQ->plan);
+    // x-mix: CB y frequencies per CTA, every x subband and component at once (CB nsx 2 lines).
     const int ls = g.P | 1;
-    while (cb > 1 && (2 * (size_t)(2 * cb) * ls * elem > (size_t)kSmemBudget ||
-                      fft_threads(2 * cb, g.tP->plan) > kMaxThreads))
+    auto x_smem = [&](int c) { return ((size_t)c * g.nsx * 2 * ls + g.P) * elem; };
+    int cb = 8;
+    while (cb > 1 && (x_smem(cb) > (size_t)kSmemBudget || fft_threads(cb * g.nsx * 2, g.tP->plan) > kMaxThreads))
         cb /= 2;
-    const size_t smem_mix = 2 * (size_t)(2 * cb) * ls * elem;
-    const int thr_x = fft_threads(2 * cb, g.tP->plan);
-    if (2 * (size_t)ti * g.Q * elem > (size_t)kSmemBudget || smem_mix > (size_t)kSmemBudget ||
-        thr_y > kMaxThreads || thr_x > kMaxThreads)
+    while (cb > 1 && (int64_t)((g.Q + cb - 1) / cb) * npy * nrhs < 148) cb /= 2;
+    const int thr_x = fft_threads(cb * g.nsx * 2, g.tP->plan);
+    if (y_smem(ti) > (size_t)kSmemBudget || x_smem(cb) > (size_t)kSmemBudget || thr_y > kMaxThreads ||
+        thr_x > kMaxThreads)
         return fail(RTM_ERR_UNSUPPORTED, "FFT grid too large for this build");
     a.ti = ti;
     a.cb = cb;
     a.ls = ls;
+    const bool p2x = fft_pow2(g.tP->plan), p2y = fft_pow2(g.tQ->plan);
     const int rows_max = std::max(g.rows[0], g.rows[1]);
     const unsigned tiles = (unsigned)((rows_max + ti - 1) / ti);
     for (int pass = 0; pass < passes; ++pass) {
         a.py0 = g.lean ? pass : 0;
         a.npy = npy;
         a.accumulate = g.lean && pass > 0;
-        k_grid_y_fwd<T><<<dim3(tiles, 2 * npy, nrhs), thr_y, (size_t)ti * g.Q * elem, s>>>(a, x);
-        k_grid_x_mix<T><<<dim3((g.Q + cb - 1) / cb, npy, nrhs), thr_x, smem_mix, s>>>(a);
-        k_grid_y_inv<T><<<dim3(tiles, 2, nrhs), thr_y, 2 * (size_t)ti * g.Q * elem, s>>>(a, y);
+        const dim3 gy(tiles, 2, nrhs), gx((g.Q + cb - 1) / cb, npy, nrhs);
+        if (p2y) k_grid_y_fwd<T, true><<<gy, thr_y, y_smem(ti), s>>>(a, x);
+        else k_grid_y_fwd<T, false><<<gy, thr_y, y_smem(ti), s>>>(a, x);
+        if (p2x) k_grid_x_mix<T, true><<<gx, thr_x, x_smem(cb), s>>>(a);
+        else k_grid_x_mix<T, false><<<gx, thr_x, x_smem(cb), s>>>(a);
+        if (p2y) k_grid_y_inv<T, true><<<gy, thr_y, y_smem(ti), s>>>(a, y);
+        else k_grid_y_inv<T, false><<<gy, thr_y, y_smem(ti), s>>>(a, y);
         count_launch(3);
         RTM_CUDA(cudaGetLastError());
     }
@@ -371,6 +375,8 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
 }
 
 int GridApplicator::reserve(int nrhs) {
+    // kernel attributes are set here, outside of any stream capture
+    if (precision == RTM_FP64) set_smem_attrs<double>(); else set_smem_attrs<float>();
     if (nrhs <= max_rhs && (mode == kStrip || work.bytes >= work_bytes_per_rhs() * (size_t)nrhs)) return RTM_OK;
     if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
     max_rhs = std::max(max_rhs, nrhs);
@@ -481,7 +487,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_y(const GenArgs a) {
         A[it] = (i < a.P) ? gen_value(a, item, i, j) : make_double2(0, 0);
     }
     __syncthreads();
-    fft_inplace<false>(A, TI, 1, TI, a.planQ, a.twQ);
+    fft_inplace<false, false>(A, TI, 1, TI, a.planQ, a.twQ);
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
         if (i < a.P) item.dst[(int64_t)j * a.P + i] = A[it];
@@ -497,7 +503,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
     double2* col = item.dst + (int64_t)j * P;
     for (int i = threadIdx.x; i < P; i += blockDim.x) A[i] = col[i];
     __syncthreads();
-    fft_inplace<false>(A, 1, P, 1, a.planP, a.twP);
+    fft_inplace<false, false>(A, 1, P, 1, a.planP, a.twP);
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
         double2 v = A[i];
         if (a.realify) v.y = 0.0;

@@ -25,6 +25,7 @@
 namespace rtm {
 
 constexpr int kRT = 256;  // threads of the vector kernels
+static int reduce_blocks(int64_t n);
 
 __device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 to_d2(double2 v) { return v; }
@@ -325,84 +326,9 @@ __global__ void __launch_bounds__(kRT) k_gm_v0(const T2* __restrict__ w, T2* __r
     }
 }
 
-// c_k = V_k^H w for k <= step (pass 0: h = c; pass 1: h += c).
-template <typename T2>
-__global__ void __launch_bounds__(kRT) k_gm_dot(const T2* __restrict__ V, const T2* __restrict__ w, int64_t n, int nrhs,
-                                                GmState* st, GmArrays ar, int pass) {
-    const int rhs = blockIdx.y;
-    GmState& S = st[rhs];
-    if (!S.active) return;
-    const int cols = S.step + 1;
-    const T2* wr = w + rhs * n;
-    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
-    for (int k0 = 0; k0 < cols; k0 += 8) {
-        double2 acc[8];
-#pragma unroll
-        for (int kk = 0; kk < 8; ++kk) acc[kk] = make_double2(0, 0);
-        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-            const double2 wv = to_d2(wr[i]);
-#pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
-                if (k0 + kk < cols) {
-                    const double2 v = to_d2(V[((int64_t)(k0 + kk) * nrhs + rhs) * n + i]);
-                    acc[kk] = dadd(acc[kk], dmulc(v, wv));
-                }
-            }
-        }
-        double2 out[8];
-        block_sum<8>(acc, out);
-        if (threadIdx.x < 8 && k0 + threadIdx.x < cols)
-            part[(int64_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = out[threadIdx.x];
-    }
-    if (!arrive(&S.counter)) return;
-    // One warp per column: lanes sum strided partials, then a shuffle tree (fixed order).
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int k = warp; k < cols; k += nw) {
-        double2 v = make_double2(0, 0);
-        const double2* pk = part + (int64_t)k * gridDim.x;
-        for (int b = lane; b < (int)gridDim.x; b += 32) v = dadd(v, pk[b]);
-        for (int o = 16; o > 0; o >>= 1) {
-            v.x += __shfl_down_sync(0xffffffffu, v.x, o);
-            v.y += __shfl_down_sync(0xffffffffu, v.y, o);
-        }
-        if (lane == 0) {
-            double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
-            ar.c[(int64_t)rhs * (ar.m + 1) + k] = v;
-            h[k] = pass == 0 ? v : dadd(h[k], v);
-        }
-    }
-}
-
-// w -= V c; with finish, also ||w|| and the rest of the Arnoldi step: the Hessenberg column, its
-// rotations, the new rotation, the rotated right-hand side, the history and the stopping tests.
-template <typename T2>
-__global__ void __launch_bounds__(kRT) k_gm_update(T2* __restrict__ w, const T2* __restrict__ V, int64_t n, int nrhs,
-                                                   GmState* st, GmArrays ar, int finish) {
-    const int rhs = blockIdx.y;
-    GmState& S = st[rhs];
-    if (!S.active) return;
-    const int cols = S.step + 1;
-    const double2* c = ar.c + (int64_t)rhs * (ar.m + 1);
-    T2* wr = w + rhs * n;
-    double2 acc[1] = {make_double2(0, 0)};
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double2 v = to_d2(wr[i]);
-        for (int k = 0; k < cols; ++k) {
-            const double2 p = dmul(to_d2(V[((int64_t)k * nrhs + rhs) * n + i]), c[k]);
-            v.x -= p.x;
-            v.y -= p.y;
-        }
-        const T2 vs = from_d2<T2>(v);
-        wr[i] = vs;
-        const double2 vd = to_d2(vs);
-        acc[0].x += vd.x * vd.x + vd.y * vd.y;
-    }
-    if (!finish) return;
-    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
-    block_sum<1>(acc, part + blockIdx.x);
-    if (!arrive(&S.counter)) return;
-    const double s = cta_total(part, gridDim.x).x;
-    if (threadIdx.x != 0) return;
+// The rest of an Arnoldi step once ||w|| is known: the Hessenberg column, its previous rotations,
+// the new rotation, the rotated right-hand side, the history and the stopping tests (one thread).
+__device__ void arnoldi_finish(GmState& S, GmArrays& ar, int rhs, double s) {
     const double sub = sqrt(s);
     const int m = ar.m, j = S.step;
     double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
@@ -447,6 +373,136 @@ __global__ void __launch_bounds__(kRT) k_gm_update(T2* __restrict__ w, const T2*
     S.active = more;
     S.skip_step = !more;
     S.done = S.converged || S.iteration >= S.max_iterations;
+}
+
+// One pass of the classical Gram-Schmidt run twice (orthogonalize_.m:15-23) over tiles of TR rows:
+//   mode 0: c = V^H w                       (h = c)
+//   mode 1: w -= V h, then c = V^H w        (h += c)
+//   mode 2: w -= V c, then ||w|| and the end of the Arnoldi step.
+// The CTA stages the tile of the basis (columns 0..step, rows of the tile) and of w in shared memory
+// with all its loads in flight, so every pass reads the basis once. Column partials accumulate in
+// shared memory over the CTA's tiles; the last CTA sums the per-CTA partials in a fixed order.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* __restrict__ w, int64_t n, int nrhs,
+                                                 GmState* st, GmArrays ar, int mode, int TR) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int rhs = blockIdx.y;
+    GmState& S = st[rhs];
+    if (!S.active) return;
+    const int cols = S.step + 1;
+    const int ld = TR + 1;
+    double2* colacc = reinterpret_cast<double2*>(smem_raw);  // [m + 1]
+    double2* coef = colacc + (ar.m + 1);                       // [m + 1]
+    double2* scratch = coef + (ar.m + 1);                      // [max(kRT, m + 1)]
+    T2* ws = reinterpret_cast<T2*>(scratch + (kRT > ar.m + 1 ? kRT : ar.m + 1));  // [TR]
+    T2* Vs = ws + TR;                                          // [cols][ld]
+    const double2* cf = mode == 1 ? ar.h + (int64_t)rhs * (ar.m + 1) : ar.c + (int64_t)rhs * (ar.m + 1);
+    for (int k = threadIdx.x; k < cols; k += blockDim.x) {
+        colacc[k] = make_double2(0, 0);
+        if (mode) coef[k] = cf[k];
+    }
+    const int G = kRT / cols > 0 ? kRT / cols : 1;  // row groups of the column sums
+    T2* wr = w + rhs * n;
+    double nrm = 0;
+    const int64_t tiles = (n + TR - 1) / TR;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t r0 = tile * TR;
+        __syncthreads();  // the previous tile's readers are done (and coef is visible)
+        for (int t = threadIdx.x; t < cols * TR; t += blockDim.x) {
+            const int k = t / TR, r = t - k * TR;
+            const int64_t row = r0 + r;
+            Vs[k * ld + r] = row < n ? V[((int64_t)k * nrhs + rhs) * n + row] : from_d2<T2>(make_double2(0, 0));
+        }
+        for (int r = threadIdx.x; r < TR; r += blockDim.x) {
+            const int64_t row = r0 + r;
+            ws[r] = row < n ? wr[row] : from_d2<T2>(make_double2(0, 0));
+        }
+        __syncthreads();
+        if (mode) {
+            for (int r = threadIdx.x; r < TR; r += blockDim.x) {
+                double2 v = to_d2(ws[r]);
+                for (int k = 0; k < cols; ++k) {
+                    const double2 p = dmul(to_d2(Vs[k * ld + r]), coef[k]);
+                    v.x -= p.x;
+                    v.y -= p.y;
+                }
+                const T2 vs = from_d2<T2>(v);
+                ws[r] = vs;
+                const int64_t row = r0 + r;
+                if (row < n) {
+                    wr[row] = vs;
+                    const double2 vd = to_d2(vs);
+                    nrm += vd.x * vd.x + vd.y * vd.y;
+                }
+            }
+            __syncthreads();
+        }
+        if (mode < 2) {
+            for (int t = threadIdx.x; t < cols * G; t += blockDim.x) {
+                const int k = t % cols, g = t / cols;
+                double2 acc = make_double2(0, 0);
+                for (int r = g; r < TR; r += G) acc = dadd(acc, dmulc(to_d2(Vs[k * ld + r]), to_d2(ws[r])));
+                scratch[t] = acc;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < cols; k += blockDim.x) {
+                double2 acc = colacc[k];
+                for (int g = 0; g < G; ++g) acc = dadd(acc, scratch[k + g * cols]);
+                colacc[k] = acc;
+            }
+        }
+    }
+    __syncthreads();
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
+    if (mode < 2) {
+        for (int k = threadIdx.x; k < cols; k += blockDim.x) part[(int64_t)k * gridDim.x + blockIdx.x] = colacc[k];
+    } else {
+        double2 v[1] = {make_double2(nrm, 0)};
+        block_sum<1>(v, part + blockIdx.x);
+    }
+    if (!arrive(&S.counter)) return;
+    if (mode == 2) {
+        const double tot = cta_total(part, gridDim.x).x;
+        if (threadIdx.x == 0) arnoldi_finish(S, ar, rhs, tot);
+        return;
+    }
+    // One warp per column: lanes sum strided partials, then a shuffle tree (fixed order).
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = warp; k < cols; k += nw) {
+        double2 v = make_double2(0, 0);
+        const double2* pk = part + (int64_t)k * gridDim.x;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v = dadd(v, pk[b]);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+        }
+        if (lane == 0) {
+            double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
+            ar.c[(int64_t)rhs * (ar.m + 1) + k] = v;
+            h[k] = mode == 0 ? v : dadd(h[k], v);
+        }
+    }
+}
+
+// Rows per tile and shared bytes of k_gm_orth for a basis of up to m + 1 columns.
+template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
+    const size_t fixed = (size_t)(2 * (m + 1) + std::max(kRT, m + 1)) * sizeof(double2);
+    int tr = 256;
+    while (tr > 32 && fixed + (size_t)tr * sizeof(T2) + (size_t)(m + 1) * (tr + 1) * sizeof(T2) > 96 * 1024) tr -= 32;
+    *TR = tr;
+    *smem = fixed + (size_t)tr * sizeof(T2) + (size_t)(m + 1) * (tr + 1) * sizeof(T2);
+}
+
+// (the dynamic shared-memory attributes are set before any capture, in gmres())
+template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, int nrhs, GmState* st, const GmArrays& ar,
+                                               int mode, cudaStream_t s) {
+    int TR;
+    size_t smem;
+    orth_config<T2>(ar.m, &TR, &smem);
+    const int64_t tiles = (n + TR - 1) / TR;
+    const int blocks = (int)std::min<int64_t>(tiles, reduce_blocks(n));
+    k_gm_orth<T2><<<dim3(blocks, nrhs), kRT, smem, s>>>(V, w, n, nrhs, st, ar, mode, TR);
+    count_launch();
 }
 
 // V[:, step] = w / H(step, step - 1) while the cycle goes on.
@@ -510,11 +566,6 @@ __global__ void k_gm_solve(GmState* st, GmArrays ar, int staged) {
 }
 
 static void launch_gm_solve(GmState* st, const GmArrays& ar, int nrhs, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
-    }
     const size_t bytes = ((size_t)ar.m * ar.m + ar.m) * sizeof(double2);
     const bool staged = bytes <= 200 * 1024;
     k_gm_solve<<<nrhs, 128, staged ? bytes : 0, s>>>(st, ar, staged ? 1 : 0);
@@ -614,6 +665,42 @@ static int reduce_blocks(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, 592));
 }
 
+// A CUDA graph of a fixed launch sequence: captured once from the stream, replayed per chunk.
+struct GraphRunner {
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+    GraphRunner() = default;
+    GraphRunner(const GraphRunner&) = delete;
+    GraphRunner& operator=(const GraphRunner&) = delete;
+    ~GraphRunner() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+    template <class F> int capture(cudaStream_t s, F&& body) {
+        const int64_t before = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+        RTM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int st = body();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        // the captured launches have not run yet; they are counted at every replay
+        kernels = __atomic_load_n(&g_launches, __ATOMIC_RELAXED) - before;
+        __atomic_fetch_sub(&g_launches, kernels, __ATOMIC_RELAXED);
+        if (st != RTM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+        return RTM_OK;
+    }
+    int launch(cudaStream_t s) {
+        RTM_CUDA(cudaGraphLaunch(exec, s));
+        count_launch((int)kernels);
+        return RTM_OK;
+    }
+};
+
 // ============================================================================================
 template <typename T>
 static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv, const void* x0v, void* xv, int64_t n,
@@ -666,14 +753,9 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
     std::vector<CgState> host(nrhs);
     int launched = 0;
     res.matvecs = x0 ? 1 : 0;
-    while (true) {
-        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, s));
-        RTM_CUDA(cudaStreamSynchronize(s));
-        bool all = true;
-        for (auto& h : host) all = all && h.done;
-        if (all || launched >= cfg.max_iterations) break;
-        const int chunk = std::min(every, cfg.max_iterations - launched);
-        for (int it = 0; it < chunk; ++it) {
+    // `every` iterations as one graph; iterations past the stopping test are no-ops on the device.
+    auto chunk_body = [&]() -> int {
+        for (int it = 0; it < every; ++it) {
             if (M) RTM_TRY(M->apply(r.ptr, z.ptr, nrhs, s, skip));
             k_cg_rz<T2><<<grid, kRT, 0, s>>>(r.as<T2>(), zp, n, st, part.as<double2>());
             k_cg_dir<T2><<<grid, kRT, 0, s>>>(zp, d.as<T2>(), n, st);
@@ -684,7 +766,18 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
             count_launch(4);
         }
         RTM_CUDA(cudaGetLastError());
-        launched += chunk;
+        return RTM_OK;
+    };
+    GraphRunner graph;
+    while (true) {
+        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        bool all = true;
+        for (auto& h : host) all = all && h.done;
+        if (all || launched >= cfg.max_iterations) break;
+        if (!graph.exec) RTM_TRY(graph.capture(s, chunk_body));
+        RTM_TRY(graph.launch(s));
+        launched += every;
     }
     // IterativeMethod.m:52: the true residual costs one more product.
     RTM_TRY(A->apply(x, q.ptr, nrhs, s, SkipFlags{}));
@@ -783,9 +876,15 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     }
     k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 1);
     count_launch();
+    // function attributes are set before the capture
+    cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     std::vector<GmState> host(nrhs);
     T2* Vp = V.as<T2>();
-    while (true) {
+    // One restart cycle as a graph: the m Arnoldi steps, the least-squares solve, the update of x and
+    // the true residual the next cycle starts from (iterate_.m:30-82). Steps after the stopping test
+    // and the restart of a finished system are no-ops on the device.
+    auto cycle_body = [&]() -> int {
         k_gm_v0<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
         count_launch();
         for (int j = 0; j < m; ++j) {
@@ -800,31 +899,16 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
             } else {
                 RTM_TRY(A->apply(vj, w.ptr, nrhs, s, skip_step));
             }
-            k_gm_dot<T2><<<grid, kRT, 0, s>>>(Vp, w.as<T2>(), n, nrhs, st, ar, 0);
-            k_gm_update<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st, ar, 0);
-            k_gm_dot<T2><<<grid, kRT, 0, s>>>(Vp, w.as<T2>(), n, nrhs, st, ar, 1);
-            k_gm_update<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st, ar, 1);
+            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 0, s);
+            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, s);
+            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 2, s);
             k_gm_next<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
-            count_launch(5);
-            RTM_CUDA(cudaGetLastError());
-            if (cfg.check_every > 0 && (j + 1) % cfg.check_every == 0 && j + 1 < m) {
-                RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
-                RTM_CUDA(cudaStreamSynchronize(s));
-                bool any = false;
-                for (auto& hh : host) any = any || hh.active;
-                if (!any) break;
-            }
+            count_launch(1);
         }
         launch_gm_solve(st, ar, nrhs, s);
         k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, right ? Z.as<T2>() : Vp, n, nrhs, st, ar);
         k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
         count_launch(2);
-        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
-        RTM_CUDA(cudaStreamSynchronize(s));
-        bool all = true;
-        for (auto& hh : host) all = all && hh.done;
-        if (all) break;
-        // The next cycle starts from the true residual (iterate_.m:77-81).
         RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
         k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
         count_launch();
@@ -832,6 +916,20 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         else RTM_CUDA(cudaMemcpyAsync(w.ptr, t.ptr, vec, cudaMemcpyDeviceToDevice, s));
         k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 0);
         count_launch();
+        RTM_CUDA(cudaGetLastError());
+        return RTM_OK;
+    };
+    GraphRunner graph;
+    int cycles = 0;
+    while (true) {
+        RTM_CUDA(cudaMemcpyAsync(host.data(), stb.ptr, sizeof(GmState) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        bool all = true;
+        for (auto& hh : host) all = all && hh.done;
+        if (all || cycles > cfg.max_iterations) break;
+        if (!graph.exec) RTM_TRY(graph.capture(s, cycle_body));
+        RTM_TRY(graph.launch(s));
+        ++cycles;
         res.matvecs += 1;
     }
     RTM_TRY(A->apply(x, t.ptr, nrhs, s, SkipFlags{}));

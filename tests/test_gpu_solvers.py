@@ -84,7 +84,8 @@ def test_iteration_limit_is_not_an_error():
 
 @pytest.mark.parametrize("method", ["cg", "gmres"])
 def test_plate_solve_matches_the_oracle(method):
-    """SolverTest.m:9-21 style: a plane wave on a small plate, residual vs the dense matrix."""
+    """SolverTest.m:9-21: a plane wave on a small plate, the residual against the dense matrix; and
+    the GPU iteration against the oracle's on the same generators."""
     import rooftop_mom_b200 as R
     from oracle import assembly as A, excitation as EX, geometry as G, solvers as OS, spectra as S
 
@@ -93,21 +94,26 @@ def test_plate_solve_matches_the_oracle(method):
     prob = R.Problem(R.Mesh(cx, cy, h, h), 2 * np.pi)
     op = R.Operator(prob)
     exc = R.Excitation.planeWave(prob)
-    res = R.Solver(method=method, tolerance=1e-12, restart=30).solve(op, exc)
     xx, yy, e = prob.generators().arrays()
     rt = G.Rooftops(cx, cy, h, h, 8)
     gen = A.Generators(xx, yy, e, rt.content)
-    dense = EX.dense_matrix(gen, rt)
     b = exc.vector()
-    assert np.linalg.norm(dense @ res.solution() - b) / np.linalg.norm(b) < 1e-10
     sub = S.subband_spectra(gen, h, h)
-    ref = OS.solve(method, lambda v: S.split_apply(rt, sub, rt.content, v), b, tol=1e-12, restart=30)
-    # Driven to 1e-12 on an EFIE plate, the two runs' rounding (different FFTs) shifts the last
-    # iterations by a few; the early history agrees closely and both solutions are converged.
+    apply = lambda v: S.split_apply(rt, sub, rt.content, v)
+    # Iteration parity at 1e-6: the histories agree closely and the counts match within a few.
+    # (Deeper, restarted GMRES stagnates and amplifies rounding: the oracle itself needs 154
+    # iterations to 1e-9 with the dense product and 168 with the split-FFT one.)
+    res = R.Solver(method=method, tolerance=1e-6, restart=30).solve(op, exc)
+    ref = OS.solve(method, apply, b, tol=1e-6, restart=30)
     assert res.converged() and ref.converged
     early = min(30, len(ref.residual_norms))
     np.testing.assert_allclose(res.residualNorms()[:early], ref.residual_norms[:early], rtol=1e-6)
-    assert abs(res.iterationCount() - ref.iteration_count) <= max(3, ref.iteration_count // 20)
+    assert abs(res.iterationCount() - ref.iteration_count) <= max(2, ref.iteration_count // 50)
+    # Solution parity driven to 1e-12 (near the FP64 floor the restarted counts drift apart).
+    res = R.Solver(method=method, tolerance=1e-12, restart=30, maxIterationCount=3000).solve(op, exc)
+    ref = OS.solve(method, apply, b, tol=1e-12, restart=30, maxit=3000)
+    dense = EX.dense_matrix(gen, rt)
+    assert np.linalg.norm(dense @ res.solution() - b) / np.linalg.norm(b) < 1e-10
     assert rel(res.solution(), ref.solution) < 1e-10
 
 
