@@ -1,7 +1,7 @@
 // Shared-memory mixed-radix FFT engine for sm_100a (device code only).
 //
 // A CTA transforms, in place, `lines` lines of length n that sit in shared memory; element e of
-// line l is at buf[l * ls + e * es]. The transform is a Stockham autosort FFT (natural order in and
+// line l is at buf[l * ls + sk(e) * es]. The transform is a Stockham autosort FFT (natural order in and
 // out): at a stage of radix R after sub-transforms of length Ns, butterfly j reads the R elements
 // j + t n/R, twiddles them by w^(t k n/(Ns R)) with k = j mod Ns, applies a radix-R DFT and writes
 // them to (j - k) R + k + q Ns. Butterflies are numbered line-fastest, so a warp touches the same
@@ -152,6 +152,10 @@ template <int R, bool INV, typename T2> __device__ __forceinline__ void dft(T2* 
     else dft_odd<R, INV>(v, tw, n);
 }
 
+// Shared-memory position of element e of a line: one slot of padding after every 16 elements, so
+// that the stride-16 writes of a first radix-16 stage fall on different banks.
+__host__ __device__ __forceinline__ int sk(int e) { return e + (e >> 4); }
+
 // Butterflies per thread of a stage of radix R (at most about 16 complex values in registers).
 __host__ __device__ constexpr int fft_ipt(int r) {
     return r == 2 ? 8 : r == 3 ? 6 : r == 4 ? 4 : r == 5 ? 4 : r == 7 ? 3 : r == 8 ? 2 : 1;
@@ -184,7 +188,7 @@ __device__ __forceinline__ void pass_ip_body(T2* buf, int n, int Ns, int lines, 
             const int line = it % lines, j = it / lines, k = j % Ns;
             const T2* s = buf + line * ls;
 #pragma unroll
-            for (int t = 0; t < R; ++t) v[q][t] = s[(j + t * nb) * es];
+            for (int t = 0; t < R; ++t) v[q][t] = s[sk(j + t * nb) * es];
             if (Ns > 1) {
 #pragma unroll
                 for (int t = 1; t < R; ++t) {
@@ -204,7 +208,7 @@ __device__ __forceinline__ void pass_ip_body(T2* buf, int n, int Ns, int lines, 
             const int base = (j - k) * R + k;
             T2* d = buf + line * ls;
 #pragma unroll
-            for (int t = 0; t < R; ++t) d[(base + t * Ns) * es] = v[q][t];
+            for (int t = 0; t < R; ++t) d[sk(base + t * Ns) * es] = v[q][t];
         }
     }
     __syncthreads();
@@ -232,7 +236,7 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
         k = j % Ns;
         const T2* s = buf + line * ls;
         for (int t = 0; t < R; ++t) {
-            T2 x = s[(j + t * nb) * es];
+            T2 x = s[sk(j + t * nb) * es];
             if (Ns > 1 && t > 0) {
                 const T2 w = tw[t * k * stride];
                 x = INV ? cmulc(x, w) : cmul(x, w);
@@ -250,14 +254,14 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
                 const T2 w = tw[((t * q) % R) * st];
                 acc = cadd(acc, INV ? cmulc(v[t], w) : cmul(v[t], w));
             }
-            d[(base + q * Ns) * es] = acc;
+            d[sk(base + q * Ns) * es] = acc;
         }
     }
     __syncthreads();
 }
 
 // Transforms, in place, the `lines` lines of length p.n in buf (element e of line l at
-// buf[l * ls + e * es]); tw (global or shared) holds the p.n roots. Needs blockDim.x >=
+// buf[l * ls + sk(e) * es]); tw (global or shared) holds the p.n roots. Needs blockDim.x >=
 // fft_threads(lines, p); call it after a __syncthreads() that makes buf visible; it returns after
 // one. POW2 instantiates radices 16, 8, 4 and 2 inline (lengths that are powers of two); otherwise
 // every radix runs as a separate function.

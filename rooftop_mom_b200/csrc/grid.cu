@@ -64,33 +64,46 @@ template <typename T2> __device__ __forceinline__ void stage_roots(T2* dst, cons
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
+constexpr int kBatch = 8;  // independent global loads a thread issues before it uses them
+
 // --------------------------------------------------------------------------------------------
 // y-forward: for a tile of TI x columns of component c, both y subbands at once:
-// W[py][c][j][i] = FFT_y( x_c(i, j) mody(j)^py ). Shared tile A[j][L], L = npy TI lines,
+// W[py][c][j][i] = FFT_y( x_c(i, j) mody(j)^py ). Shared tile A[sk(j)][L], L = npy TI lines,
 // line pyi TI + l (grid: tiles x components x right-hand sides).
 template <typename T, bool POW2>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+__global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_grid_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* tws = A + (size_t)L * Q;
+    T2* tws = A + (size_t)L * (sk(Q - 1) + 1);
     const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
     if (i0 >= rows || skipped(a, rhs)) return;
     stage_roots(tws, a.twQ, Q);
     const T2* xr = x + (int64_t)rhs * a.n + a.off[c];
-    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
-        const int l = it % TI, j = it / TI, i = i0 + l;
-        T2 v = czero<T2>();
-        if (i < rows && j < cols) v = xr[i + (int64_t)j * rows];
-        T2* row = A + (size_t)j * L + l;
-        if (a.npy == 2) {
-            row[0] = v;
-            row[TI] = cmul(v, __ldg(&a.modQ[j]));
-        } else {
-            row[0] = a.py0 ? cmul(v, __ldg(&a.modQ[j])) : v;
+    const int total = TI * Q;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+        T2 v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            const int l = it % TI, j = it / TI, i = i0 + l;
+            v[u] = (it < total && i < rows && j < cols) ? xr[i + (int64_t)j * rows] : czero<T2>();
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            if (it >= total) break;
+            const int l = it % TI, j = it / TI;
+            T2* row = A + (size_t)sk(j) * L + l;
+            if (a.npy == 2) {
+                row[0] = v[u];
+                row[TI] = cmul(v[u], __ldg(&a.modQ[j]));
+            } else {
+                row[0] = a.py0 ? cmul(v[u], __ldg(&a.modQ[j])) : v[u];
+            }
         }
     }
     __syncthreads();
@@ -99,16 +112,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_fwd(const GridArgs<T>
     for (int it = threadIdx.x; it < L * Q; it += blockDim.x) {
         const int l = it % L, j = it / L;
         const int pyi = l / TI, i = i0 + (l - pyi * TI);
-        if (i < rows) dst[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] = A[it];
+        if (i < rows) dst[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] = A[(size_t)sk(j) * L + l];
     }
 }
 
 // --------------------------------------------------------------------------------------------
 // x-mix: CB y frequencies j of the y subband py; for both components and both x subbands at once
 // (line (jj nsx + px) nc + c): sum over px of demod_x^px IFFT_x( B(px, py) FFT_x( W mod_x^px ) ),
-// scaled by 1/(PQ), in place in W. Lines have an odd stride (a.ls) to spread the banks.
+// scaled by 1/(PQ), in place in W. Line stride a.ls spreads the lines of a warp over the banks.
 template <typename T, bool POW2>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_x_mix(const GridArgs<T> a) {
+__global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_grid_x_mix(const GridArgs<T> a) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = a.P, Q = a.Q, nc = a.ncomp, CB = a.cb, ls = a.ls, nsx = a.nsx;
@@ -122,53 +135,86 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_x_mix(const GridArgs<T>
     if (skipped(a, rhs)) return;
     stage_roots(tws, a.twP, P);
     T2* wr = a.work + (int64_t)rhs * a.work_rhs + (int64_t)pyi * nc * Q * P;
-    for (int it = threadIdx.x; it < CB * nc * P; it += blockDim.x) {
-        const int jc = it / P, i = it - jc * P;
-        const int jj = jc / nc, c = jc - jj * nc, j = j0 + jj;
-        T2 v = czero<T2>();
-        if (i < a.rows[c] && j < Q) v = wr[((int64_t)c * Q + j) * P + i];
-        A[(size_t)((jj * nsx) * nc + c) * ls + i] = v;
-        if (nsx == 2) A[(size_t)((jj * nsx + 1) * nc + c) * ls + i] = cmul(v, __ldg(&a.modP[i]));
+    const int total = CB * nc * P;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+        T2 v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            const int jc = it / P, i = it - jc * P;
+            const int jj = jc / nc, c = jc - jj * nc, j = j0 + jj;
+            v[u] = (it < total && i < a.rows[c] && j < Q) ? wr[((int64_t)c * Q + j) * P + i] : czero<T2>();
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            if (it >= total) break;
+            const int jc = it / P, i = it - jc * P;
+            const int jj = jc / nc, c = jc - jj * nc;
+            A[(size_t)((jj * nsx) * nc + c) * ls + sk(i)] = v[u];
+            if (nsx == 2) A[(size_t)((jj * nsx + 1) * nc + c) * ls + sk(i)] = cmul(v[u], __ldg(&a.modP[i]));
+        }
     }
     __syncthreads();
     fft_inplace<false, POW2>(A, lines, ls, 1, a.planP, tws);
     const T2* vy = py ? a.vy1 : a.vy0;
-    for (int it = threadIdx.x; it < CB * nsx * P; it += blockDim.x) {
-        const int jp = it / P, i = it - jp * P;
-        const int jj = jp / nsx, px = jp - jj * nsx, j = j0 + jj;
-        if (j >= Q) continue;
-        T2* lx = A + (size_t)(jp * nc) * ls;
-        T2* ly = lx + ls;
-        const T2 sx = lx[i], sy = ly[i];
-        const int sub = px + nsx * py;
-        T2 ox, oy;
-        if (a.mode == kGen3) {
-            const int64_t base = ((int64_t)(sub * 3) * Q + j) * P + i;
-            const T2 E = __ldg(&a.spec[base]);
-            const T2 Mx = __ldg(&a.spec[base + (int64_t)Q * P]);
-            const T2 My = __ldg(&a.spec[base + 2 * (int64_t)Q * P]);
-            const T2 u = __ldg(&(px ? a.ux1 : a.ux0)[i]);
-            const T2 v = __ldg(&vy[j]);
-            const T cu = (u.x * u.x + u.y * u.y) * a.inv_a2;
-            const T cv = (v.x * v.x + v.y * v.y) * a.inv_b2;
-            // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E.
-            T2 qc = cmulc(u, v);
-            qc.x = -qc.x * a.inv_ab;
-            qc.y = -qc.y * a.inv_ab;
-            const T2 Ex = cmul(E, sx), Ey = cmul(E, sy);
-            ox = csub(cmul(Mx, sx), cscale(Ex, cu));
-            ox = cadd(ox, cmul(qc, Ey));
-            oy = csub(cmul(My, sy), cscale(Ey, cv));
-            oy = cadd(oy, cmul(cconj(qc), Ex));
-        } else {
-            const int64_t base = (int64_t)j * P + i, blk = (int64_t)Q * P;
-            const T2 XX = __ldg(&a.spec[base]), XY = __ldg(&a.spec[base + blk]);
-            const T2 YX = __ldg(&a.spec[base + 2 * blk]), YY = __ldg(&a.spec[base + 3 * blk]);
-            ox = cadd(cmul(XX, sx), cmul(XY, sy));
-            oy = cadd(cmul(YX, sx), cmul(YY, sy));
+    constexpr int kMix = 4;
+    const int mtotal = CB * nsx * P;
+    for (int base = threadIdx.x; base < mtotal; base += kMix * blockDim.x) {
+        T2 e3[kMix][3];
+#pragma unroll
+        for (int u = 0; u < kMix; ++u) {
+            const int it = base + u * blockDim.x;
+            const int jp = it / P, i = it - jp * P;
+            const int jj = jp / nsx, px = jp - jj * nsx, j = j0 + jj;
+            const int sub = px + nsx * py;
+            if (it < mtotal && j < Q) {
+                if (a.mode == kGen3) {
+                    const int64_t sb = ((int64_t)(sub * 3) * Q + j) * P + i;
+                    e3[u][0] = __ldg(&a.spec[sb]);
+                    e3[u][1] = __ldg(&a.spec[sb + (int64_t)Q * P]);
+                    e3[u][2] = __ldg(&a.spec[sb + 2 * (int64_t)Q * P]);
+                } else {
+                    e3[u][0] = e3[u][1] = e3[u][2] = czero<T2>();
+                }
+            }
         }
-        lx[i] = ox;
-        ly[i] = oy;
+#pragma unroll
+        for (int u = 0; u < kMix; ++u) {
+            const int it = base + u * blockDim.x;
+            if (it >= mtotal) break;
+            const int jp = it / P, i = it - jp * P;
+            const int jj = jp / nsx, px = jp - jj * nsx, j = j0 + jj;
+            if (j >= Q) continue;
+            T2* lx = A + (size_t)(jp * nc) * ls + sk(i);
+            T2* ly = lx + ls;
+            const T2 sx = *lx, sy = *ly;
+            T2 ox, oy;
+            if (a.mode == kGen3) {
+                const T2 E = e3[u][0], Mx = e3[u][1], My = e3[u][2];
+                const T2 uu = __ldg(&(px ? a.ux1 : a.ux0)[i]);
+                const T2 vv = __ldg(&vy[j]);
+                const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E.
+                T2 qc = cmulc(uu, vv);
+                qc.x = -qc.x * a.inv_ab;
+                qc.y = -qc.y * a.inv_ab;
+                const T2 Ex = cmul(E, sx), Ey = cmul(E, sy);
+                ox = csub(cmul(Mx, sx), cscale(Ex, cu));
+                ox = cadd(ox, cmul(qc, Ey));
+                oy = csub(cmul(My, sy), cscale(Ey, cv));
+                oy = cadd(oy, cmul(cconj(qc), Ex));
+            } else {
+                const int64_t sb = (int64_t)j * P + i, blk = (int64_t)Q * P;
+                const T2 XX = __ldg(&a.spec[sb]), XY = __ldg(&a.spec[sb + blk]);
+                const T2 YX = __ldg(&a.spec[sb + 2 * blk]), YY = __ldg(&a.spec[sb + 3 * blk]);
+                ox = cadd(cmul(XX, sx), cmul(XY, sy));
+                oy = cadd(cmul(YX, sx), cmul(YY, sy));
+            }
+            *lx = ox;
+            *ly = oy;
+        }
     }
     __syncthreads();
     fft_inplace<true, POW2>(A, lines, ls, 1, a.planP, tws);
@@ -176,32 +222,45 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_x_mix(const GridArgs<T>
         const int jc = it / P, i = it - jc * P;
         const int jj = jc / nc, c = jc - jj * nc, j = j0 + jj;
         if (i >= a.rows[c] || j >= Q) continue;
-        T2 v = A[(size_t)((jj * nsx) * nc + c) * ls + i];
-        if (nsx == 2) v = cadd(v, cmulc(A[(size_t)((jj * nsx + 1) * nc + c) * ls + i], __ldg(&a.modP[i])));
+        T2 v = A[(size_t)((jj * nsx) * nc + c) * ls + sk(i)];
+        if (nsx == 2) v = cadd(v, cmulc(A[(size_t)((jj * nsx + 1) * nc + c) * ls + sk(i)], __ldg(&a.modP[i])));
         wr[((int64_t)c * Q + j) * P + i] = cscale(v, a.scale);
     }
 }
 
 // --------------------------------------------------------------------------------------------
 // y-inverse: y_c(i, j) = sum_py demod_y^py IFFT_y(W[py][c][:, i]) for a tile of TI columns of one
-// component, both y subbands at once (tile A[j][L] as in the y-forward), cropped to the rooftop grid.
+// component, both y subbands at once (tile A[sk(j)][L] as in the y-forward), cropped.
 template <typename T, bool POW2>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+__global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_grid_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* tws = A + (size_t)L * Q;
+    T2* tws = A + (size_t)L * (sk(Q - 1) + 1);
     const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
     if (i0 >= rows || skipped(a, rhs)) return;
     stage_roots(tws, a.twQ, Q);
     const T2* wr = a.work + (int64_t)rhs * a.work_rhs;
-    for (int it = threadIdx.x; it < L * Q; it += blockDim.x) {
-        const int l = it % L, j = it / L;
-        const int pyi = l / TI, i = i0 + (l - pyi * TI);
-        A[it] = (i < rows) ? wr[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] : czero<T2>();
+    const int total = L * Q;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+        T2 v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            const int l = it % L, j = it / L;
+            const int pyi = l / TI, i = i0 + (l - pyi * TI);
+            v[u] = (it < total && i < rows) ? wr[((int64_t)(pyi * a.ncomp + c) * Q + j) * a.P + i] : czero<T2>();
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int it = base + u * blockDim.x;
+            if (it >= total) break;
+            const int l = it % L, j = it / L;
+            A[(size_t)sk(j) * L + l] = v[u];
+        }
     }
     __syncthreads();
     fft_inplace<true, POW2>(A, L, 1, L, a.planQ, tws);
@@ -209,7 +268,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_inv(const GridArgs<T>
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
         if (i >= rows || j >= cols) continue;
-        const T2* row = A + (size_t)j * L + l;
+        const T2* row = A + (size_t)sk(j) * L + l;
         T2 v;
         if (a.npy == 2) v = cadd(row[0], cmulc(row[TI], __ldg(&a.modQ[j])));
         else v = a.py0 ? cmulc(row[0], __ldg(&a.modQ[j])) : row[0];
@@ -221,7 +280,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_grid_y_inv(const GridArgs<T>
 // --------------------------------------------------------------------------------------------
 // Strip: y = sum_s demod^s IFFT( B_s FFT( x mod^s ) ) / L, the subbands as lines of one transform.
 template <typename T, bool POW2>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
+__global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_strip(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x,
                                                          typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -236,30 +295,30 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_strip(const GridArgs<T> a, c
     T2* yr = y + (int64_t)rhs * a.n;
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         const T2 v = i < count ? xr[i] : czero<T2>();
-        A[i] = v;
-        if (ns == 2) A[ls + i] = cmul(v, __ldg(&a.modP[i]));
+        A[sk(i)] = v;
+        if (ns == 2) A[ls + sk(i)] = cmul(v, __ldg(&a.modP[i]));
     }
     __syncthreads();
     fft_inplace<false, POW2>(A, ns, ls, 1, a.planP, tws);
     for (int it = threadIdx.x; it < ns * L; it += blockDim.x) {
         const int s = it / L, i = it - s * L;
-        A[s * ls + i] = cmul(A[s * ls + i], __ldg(&a.spec[(int64_t)s * L + i]));
+        A[s * ls + sk(i)] = cmul(A[s * ls + sk(i)], __ldg(&a.spec[(int64_t)s * L + i]));
     }
     __syncthreads();
     fft_inplace<true, POW2>(A, ns, ls, 1, a.planP, tws);
     for (int i = threadIdx.x; i < count; i += blockDim.x) {
-        T2 v = A[i];
-        if (ns == 2) v = cadd(v, cmulc(A[ls + i], __ldg(&a.modP[i])));
+        T2 v = A[sk(i)];
+        if (ns == 2) v = cadd(v, cmulc(A[ls + sk(i)], __ldg(&a.modP[i])));
         yr[i] = cscale(v, a.scale);
     }
 }
 
 // --------------------------------------------------------------------------------------------
 template <typename T, bool POW2> static void set_attrs_one() {
-    cudaFuncSetAttribute(k_grid_y_fwd<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_grid_x_mix<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_grid_y_inv<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_strip<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_grid_y_fwd<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_grid_x_mix<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_grid_y_inv<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_strip<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 template <typename T> static void set_smem_attrs() {
@@ -270,6 +329,18 @@ template <typename T> static void set_smem_attrs() {
     set_attrs_one<T, true>();
     set_attrs_one<T, false>();
     done[dev & 63] = true;
+}
+
+// Shared stride of the lines of a CTA that transforms `lines` lines of length n in place: room for
+// the skewed positions sk(e), and a remainder modulo the elements of 128 bytes chosen so that the
+// lines touched by one warp start on different banks.
+static int line_stride(int n, int lines, size_t elem) {
+    const int W = (int)(128 / elem);
+    const int per = 32 / std::max(1, std::min(lines, 32));
+    const int target = per % W;
+    int ls = sk(n - 1) + 1;
+    while (ls % W != target) ++ls;
+    return ls;
 }
 
 size_t GridApplicator::work_bytes_per_rhs() const {
@@ -318,7 +389,7 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     const size_t elem = sizeof(T2);
     if (g.mode == kStrip) {
         a.scale = (T)(1.0 / g.P);
-        a.ls = g.P | 1;
+        a.ls = line_stride(g.P, g.nsx, elem);
         const size_t smem = ((size_t)g.nsx * a.ls + g.P) * elem;
         const int thr = fft_threads(g.nsx, g.tP->plan);
         if (smem > (size_t)kSmemBudget || thr > kMaxThreads)
@@ -337,16 +408,16 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     // y passes: TI x columns per CTA (rows of 64 bytes) for every y subband at once; fewer columns
     // while the tile (plus the roots) would not fit or would need more than kMaxThreads threads.
     int ti = sizeof(T) == 8 ? 4 : 8;
-    auto y_smem = [&](int t) { return ((size_t)npy * t * g.Q + g.Q) * elem; };
+    auto y_smem = [&](int t) { return ((size_t)npy * t * (sk(g.Q - 1) + 1) + g.Q) * elem; };
     while (ti > 1 && (y_smem(ti) > (size_t)kSmemBudget || fft_threads(npy * ti, g.tQ->plan) > kMaxThreads)) ti /= 2;
     const int thr_y = fft_threads(npy * ti, g.tQ->plan);
     // x-mix: CB y frequencies per CTA, every x subband and component at once (CB nsx 2 lines).
-    const int ls = g.P | 1;
-    auto x_smem = [&](int c) { return ((size_t)c * g.nsx * 2 * ls + g.P) * elem; };
+    auto x_smem = [&](int c) { return ((size_t)c * g.nsx * 2 * line_stride(g.P, c * g.nsx * 2, elem) + g.P) * elem; };
     int cb = 8;
     while (cb > 1 && (x_smem(cb) > (size_t)kSmemBudget || fft_threads(cb * g.nsx * 2, g.tP->plan) > kMaxThreads))
         cb /= 2;
     while (cb > 1 && (int64_t)((g.Q + cb - 1) / cb) * npy * nrhs < 148) cb /= 2;
+    const int ls = line_stride(g.P, cb * g.nsx * 2, elem);
     const int thr_x = fft_threads(cb * g.nsx * 2, g.tP->plan);
     if (y_smem(ti) > (size_t)kSmemBudget || x_smem(cb) > (size_t)kSmemBudget || thr_y > kMaxThreads ||
         thr_x > kMaxThreads)
@@ -484,13 +555,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_y(const GenArgs a) {
     const int i0 = blockIdx.x * TI;
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
-        A[it] = (i < a.P) ? gen_value(a, item, i, j) : make_double2(0, 0);
+        A[sk(j) * TI + l] = (i < a.P) ? gen_value(a, item, i, j) : make_double2(0, 0);
     }
     __syncthreads();
     fft_inplace<false, false>(A, TI, 1, TI, a.planQ, a.twQ);
     for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
         const int l = it % TI, j = it / TI, i = i0 + l;
-        if (i < a.P) item.dst[(int64_t)j * a.P + i] = A[it];
+        if (i < a.P) item.dst[(int64_t)j * a.P + i] = A[sk(j) * TI + l];
     }
 }
 
@@ -501,11 +572,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
     const GenItem& item = a.items[blockIdx.y];
     const int j = blockIdx.x;
     double2* col = item.dst + (int64_t)j * P;
-    for (int i = threadIdx.x; i < P; i += blockDim.x) A[i] = col[i];
+    for (int i = threadIdx.x; i < P; i += blockDim.x) A[sk(i)] = col[i];
     __syncthreads();
     fft_inplace<false, false>(A, 1, P, 1, a.planP, a.twP);
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        double2 v = A[i];
+        double2 v = A[sk(i)];
         if (a.realify) v.y = 0.0;
         col[i] = v;
     }
@@ -514,23 +585,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
 static int run_gen(GenArgs& a, cudaStream_t s) {
     static bool attrs = false;
     if (!attrs) {
-        cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attrs = true;
     }
     if (a.nitems == 0) return RTM_OK;
     a.ti = 4;
-    while (a.ti > 1 && ((size_t)a.ti * a.Q * sizeof(double2) > (size_t)kSmemBudget ||
+    while (a.ti > 1 && ((size_t)a.ti * (sk(a.Q - 1) + 1) * sizeof(double2) > (size_t)kSmemBudget ||
                         fft_threads(a.ti, a.planQ) > kMaxThreads))
         a.ti /= 2;
     const int thr_y = fft_threads(a.ti, a.planQ), thr_x = fft_threads(1, a.planP);
-    if ((size_t)a.ti * a.Q * sizeof(double2) > (size_t)kSmemBudget ||
-        (size_t)a.P * sizeof(double2) > (size_t)kSmemBudget || thr_y > kMaxThreads || thr_x > kMaxThreads)
+    const size_t smem_y = (size_t)a.ti * (sk(a.Q - 1) + 1) * sizeof(double2);
+    const size_t smem_x = (size_t)(sk(a.P - 1) + 1) * sizeof(double2);
+    if (smem_y > (size_t)kSmemBudget || smem_x > (size_t)kSmemBudget || thr_y > kMaxThreads || thr_x > kMaxThreads)
         return fail(RTM_ERR_UNSUPPORTED, "spectra grid too large for this build");
     dim3 gy((a.P + a.ti - 1) / a.ti, a.nitems);
-    k_gen_y<<<gy, thr_y, (size_t)a.ti * a.Q * sizeof(double2), s>>>(a);
+    k_gen_y<<<gy, thr_y, smem_y, s>>>(a);
     dim3 gx(a.Q, a.nitems);
-    k_gen_x<<<gx, thr_x, (size_t)a.P * sizeof(double2), s>>>(a);
+    k_gen_x<<<gx, thr_x, smem_x, s>>>(a);
     count_launch(2);
     RTM_CUDA(cudaGetLastError());
     return RTM_OK;

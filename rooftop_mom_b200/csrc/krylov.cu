@@ -16,6 +16,8 @@
 // the reference's iteration, and the extra launched iterations are no-ops.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -677,7 +679,7 @@ struct GraphRunner {
     }
     template <class F> int capture(cudaStream_t s, F&& body) {
         const int64_t before = __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
-        RTM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        RTM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
         const int st = body();
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &g);
@@ -694,6 +696,20 @@ struct GraphRunner {
         if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
         return RTM_OK;
     }
+    // Captures once; if the capture fails the sequence runs as plain launches from then on (the
+    // same kernels, only without the graph).
+    template <class F> int run(cudaStream_t s, F&& body) {
+        if (!exec && !eager) {
+            if (capture(s, body) != RTM_OK) {
+                cudaGetLastError();
+                eager = true;
+                if (getenv("RTM_DEBUG")) fprintf(stderr, "librtm: graph capture failed, launching eagerly\n");
+            }
+        }
+        if (eager) return body();
+        return launch(s);
+    }
+    bool eager = false;
     int launch(cudaStream_t s) {
         RTM_CUDA(cudaGraphLaunch(exec, s));
         count_launch((int)kernels);
@@ -775,8 +791,7 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
         bool all = true;
         for (auto& h : host) all = all && h.done;
         if (all || launched >= cfg.max_iterations) break;
-        if (!graph.exec) RTM_TRY(graph.capture(s, chunk_body));
-        RTM_TRY(graph.launch(s));
+        RTM_TRY(graph.run(s, chunk_body));
         launched += every;
     }
     // IterativeMethod.m:52: the true residual costs one more product.
@@ -877,8 +892,8 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 1);
     count_launch();
     // function attributes are set before the capture
-    cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     std::vector<GmState> host(nrhs);
     T2* Vp = V.as<T2>();
     // One restart cycle as a graph: the m Arnoldi steps, the least-squares solve, the update of x and
@@ -927,8 +942,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         bool all = true;
         for (auto& hh : host) all = all && hh.done;
         if (all || cycles > cfg.max_iterations) break;
-        if (!graph.exec) RTM_TRY(graph.capture(s, cycle_body));
-        RTM_TRY(graph.launch(s));
+        RTM_TRY(graph.run(s, cycle_body));
         ++cycles;
         res.matvecs += 1;
     }
