@@ -377,13 +377,24 @@ __device__ void arnoldi_finish(GmState& S, GmArrays& ar, int rhs, double s) {
     S.done = S.converged || S.iteration >= S.max_iterations;
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80 and later): a thread issues all the copies
+// of a tile without waiting, then waits for its groups before the CTA barrier.
+template <int BYTES> __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 // One pass of the classical Gram-Schmidt run twice (orthogonalize_.m:15-23) over tiles of TR rows:
 //   mode 0: c = V^H w                       (h = c)
 //   mode 1: w -= V h, then c = V^H w        (h += c)
 //   mode 2: w -= V c, then ||w|| and the end of the Arnoldi step.
-// The CTA stages the tile of the basis (columns 0..step, rows of the tile) and of w in shared memory
-// with all its loads in flight, so every pass reads the basis once. Column partials accumulate in
-// shared memory over the CTA's tiles; the last CTA sums the per-CTA partials in a fixed order.
+// Every CTA streams its tiles of the basis (columns 0..step) and of w through two shared buffers
+// with asynchronous copies: the next tile is in flight while the current one is reduced, and each
+// pass reads the basis once. Column partials accumulate in shared memory over the CTA's tiles; the
+// last CTA sums the per-CTA partials in a fixed order.
 template <typename T2>
 __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* __restrict__ w, int64_t n, int nrhs,
                                                  GmState* st, GmArrays ar, int mode, int TR) {
@@ -393,12 +404,13 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
     if (!S.active) return;
     const int cols = S.step + 1;
     const int ld = TR + 1;
+    const int mc = ar.m + 1;
     double2* colacc = reinterpret_cast<double2*>(smem_raw);  // [m + 1]
-    double2* coef = colacc + (ar.m + 1);                       // [m + 1]
-    double2* scratch = coef + (ar.m + 1);                      // [max(kRT, m + 1)]
-    T2* ws = reinterpret_cast<T2*>(scratch + (kRT > ar.m + 1 ? kRT : ar.m + 1));  // [TR]
-    T2* Vs = ws + TR;                                          // [cols][ld]
-    const double2* cf = mode == 1 ? ar.h + (int64_t)rhs * (ar.m + 1) : ar.c + (int64_t)rhs * (ar.m + 1);
+    double2* coef = colacc + mc;                               // [m + 1]
+    double2* scratch = coef + mc;                              // [max(kRT, m + 1)]
+    T2* wsb = reinterpret_cast<T2*>(scratch + (kRT > mc ? kRT : mc));  // [2][TR]
+    T2* Vsb = wsb + 2 * TR;                                    // [2][m + 1][ld]
+    const double2* cf = mode == 1 ? ar.h + (int64_t)rhs * mc : ar.c + (int64_t)rhs * mc;
     for (int k = threadIdx.x; k < cols; k += blockDim.x) {
         colacc[k] = make_double2(0, 0);
         if (mode) coef[k] = cf[k];
@@ -407,19 +419,38 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
     T2* wr = w + rhs * n;
     double nrm = 0;
     const int64_t tiles = (n + TR - 1) / TR;
-    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const T2 zero = from_d2<T2>(make_double2(0, 0));
+    auto stage = [&](int64_t tile, int buf) {
         const int64_t r0 = tile * TR;
-        __syncthreads();  // the previous tile's readers are done (and coef is visible)
+        T2* Vs = Vsb + (size_t)buf * mc * ld;
+        T2* ws = wsb + (size_t)buf * TR;
         for (int t = threadIdx.x; t < cols * TR; t += blockDim.x) {
             const int k = t / TR, r = t - k * TR;
             const int64_t row = r0 + r;
-            Vs[k * ld + r] = row < n ? V[((int64_t)k * nrhs + rhs) * n + row] : from_d2<T2>(make_double2(0, 0));
+            if (row < n) cp_async<sizeof(T2)>(&Vs[k * ld + r], &V[((int64_t)k * nrhs + rhs) * n + row]);
+            else Vs[k * ld + r] = zero;
         }
         for (int r = threadIdx.x; r < TR; r += blockDim.x) {
             const int64_t row = r0 + r;
-            ws[r] = row < n ? wr[row] : from_d2<T2>(make_double2(0, 0));
+            if (row < n) cp_async<sizeof(T2)>(&ws[r], &wr[row]);
+            else ws[r] = zero;
         }
-        __syncthreads();
+        cp_async_commit();
+    };
+    int buf = 0;
+    if ((int64_t)blockIdx.x < tiles) stage(blockIdx.x, 0);
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t next = tile + gridDim.x;
+        if (next < tiles) {
+            stage(next, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();  // this tile's copies (and coef, colacc) are visible
+        const int64_t r0 = tile * TR;
+        T2* Vs = Vsb + (size_t)buf * mc * ld;
+        T2* ws = wsb + (size_t)buf * TR;
         if (mode) {
             for (int r = threadIdx.x; r < TR; r += blockDim.x) {
                 double2 v = to_d2(ws[r]);
@@ -453,9 +484,10 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
                 colacc[k] = acc;
             }
         }
+        __syncthreads();  // the buffer is free for the stage after next
+        buf ^= 1;
     }
-    __syncthreads();
-    double2* part = ar.part + (int64_t)rhs * gridDim.x * (ar.m + 1);
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * mc;
     if (mode < 2) {
         for (int k = threadIdx.x; k < cols; k += blockDim.x) part[(int64_t)k * gridDim.x + blockIdx.x] = colacc[k];
     } else {
@@ -479,20 +511,21 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
             v.y += __shfl_down_sync(0xffffffffu, v.y, o);
         }
         if (lane == 0) {
-            double2* h = ar.h + (int64_t)rhs * (ar.m + 1);
-            ar.c[(int64_t)rhs * (ar.m + 1) + k] = v;
+            double2* h = ar.h + (int64_t)rhs * mc;
+            ar.c[(int64_t)rhs * mc + k] = v;
             h[k] = mode == 0 ? v : dadd(h[k], v);
         }
     }
 }
 
-// Rows per tile and shared bytes of k_gm_orth for a basis of up to m + 1 columns.
+// Rows per tile and shared bytes of k_gm_orth (two buffers) for a basis of up to m + 1 columns.
 template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
     const size_t fixed = (size_t)(2 * (m + 1) + std::max(kRT, m + 1)) * sizeof(double2);
-    int tr = 256;
-    while (tr > 32 && fixed + (size_t)tr * sizeof(T2) + (size_t)(m + 1) * (tr + 1) * sizeof(T2) > 96 * 1024) tr -= 32;
+    auto bytes = [&](int tr) { return fixed + 2 * ((size_t)tr + (size_t)(m + 1) * (tr + 1)) * sizeof(T2); };
+    int tr = 128;
+    while (tr > 16 && bytes(tr) > 100 * 1024) tr -= 16;
     *TR = tr;
-    *smem = fixed + (size_t)tr * sizeof(T2) + (size_t)(m + 1) * (tr + 1) * sizeof(T2);
+    *smem = bytes(tr);
 }
 
 // (the dynamic shared-memory attributes are set before any capture, in gmres())
@@ -502,7 +535,7 @@ template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, in
     size_t smem;
     orth_config<T2>(ar.m, &TR, &smem);
     const int64_t tiles = (n + TR - 1) / TR;
-    const int blocks = (int)std::min<int64_t>(tiles, reduce_blocks(n));
+    const int blocks = (int)std::min<int64_t>({tiles, (int64_t)reduce_blocks(n), 2 * 148});
     k_gm_orth<T2><<<dim3(blocks, nrhs), kRT, smem, s>>>(V, w, n, nrhs, st, ar, mode, TR);
     count_launch();
 }
