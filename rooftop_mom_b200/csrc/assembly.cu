@@ -352,7 +352,8 @@ int assemble_generators(int cx, int cy, double a, double b, double k, int near_o
     std::vector<double> extv(28);
     for (int r = 0; r < 7; ++r)
         for (int c = 0; c < 4; ++c) extv[r * 4 + c] = ext[r][c];
-    DeviceBuffer d_nx, d_ny, d_nw, d_ext, d_near;
+    DeviceBuffer d_nx, d_ny, d_nw, d_ext, d_near, d_pts, d_qw, d_sums, d_terms;
+    StreamSyncGuard guard(s);
     RTM_TRY(upload(d_nx, nnx, s));
     RTM_TRY(upload(d_ny, nny, s));
     RTM_TRY(upload(d_nw, nw, s));
@@ -393,7 +394,6 @@ int assemble_generators(int cx, int cy, double a, double b, double k, int near_o
                         qw[((size_t)q * 7 + m) * o * o + px + (size_t)o * py] = fw[(size_t)m * P2 * P2 + col];
                     }
         }
-    DeviceBuffer d_pts, d_qw, d_sums, d_terms;
     RTM_TRY(upload(d_pts, points, s));
     RTM_TRY(upload(d_qw, qw, s));
     const int64_t nblocks = (int64_t)(cx + 1) * (cy + 1);

@@ -18,6 +18,10 @@ struct rtm_generators {
     int device = 0;
     cudaStream_t stream = nullptr;
     ~rtm_generators() {
+        if (stream) cudaStreamSynchronize(stream);
+        g.xx.reset();
+        g.yy.reset();
+        g.e.reset();
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -29,6 +33,7 @@ struct rtm_operator {
     int device = 0;
     cudaStream_t stream = nullptr;
     ~rtm_operator() {
+        if (stream) cudaStreamSynchronize(stream);
         op.reset();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -39,6 +44,7 @@ struct rtm_preconditioner {
     int device = 0;
     cudaStream_t stream = nullptr;
     ~rtm_preconditioner() {
+        if (stream) cudaStreamSynchronize(stream);
         op.reset();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -51,6 +57,17 @@ int make_stream(cudaStream_t* s) {
     return RTM_OK;
 }
 
+// A stream made for one call; declared before the call's staging buffers, it outlives them.
+struct CallStream {
+    cudaStream_t s = nullptr;
+    ~CallStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+};
+
 cudaStream_t pick(void* user, cudaStream_t own) { return user ? static_cast<cudaStream_t>(user) : own; }
 
 int check_where(int where) {
@@ -59,9 +76,15 @@ int check_where(int where) {
 }
 
 // Input vectors of an operator call as device pointers in the operator's precision.
+// Staging blocks go back to the allocator's cache when these leave scope, so any copy or kernel
+// still using them on the call's stream is waited for first.
 struct Staged {
     DeviceBuffer buf64, buf32;
     const void* ptr = nullptr;
+    cudaStream_t stream = nullptr;
+    ~Staged() {
+        if (buf64.ptr || buf32.ptr) cudaStreamSynchronize(stream);
+    }
 };
 
 int stage_in(const void* src, int64_t count, int precision, int where, Staged& st, cudaStream_t s) {
@@ -73,6 +96,7 @@ int stage_in(const void* src, int64_t count, int precision, int where, Staged& s
         st.ptr = nullptr;
         return RTM_OK;
     }
+    st.stream = s;
     RTM_TRY(st.buf64.alloc((size_t)count * sizeof(double2)));
     RTM_CUDA(cudaMemcpyAsync(st.buf64.ptr, src, (size_t)count * sizeof(double2), cudaMemcpyHostToDevice, s));
     if (precision == RTM_FP64) {
@@ -89,13 +113,18 @@ int stage_in(const void* src, int64_t count, int precision, int where, Staged& s
 struct Out {
     DeviceBuffer buf64, buf32;
     void* ptr = nullptr;
+    cudaStream_t stream = nullptr;
+    ~Out() {
+        if (buf64.ptr || buf32.ptr) cudaStreamSynchronize(stream);
+    }
 };
 
-int out_prepare(void* dst, int64_t count, int precision, int where, Out& o) {
+int out_prepare(void* dst, int64_t count, int precision, int where, Out& o, cudaStream_t s) {
     if (where == RTM_DEVICE) {
         o.ptr = dst;
         return RTM_OK;
     }
+    o.stream = s;
     if (precision == RTM_FP64) {
         RTM_TRY(o.buf64.alloc((size_t)count * sizeof(double2)));
         o.ptr = o.buf64.ptr;
@@ -326,7 +355,7 @@ int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int 
     Out o;
     const int prec = op->op->precision;
     RTM_TRY(stage_in(x, n * nrhs, prec, where, in, s));
-    RTM_TRY(out_prepare(y, n * nrhs, prec, where, o));
+    RTM_TRY(out_prepare(y, n * nrhs, prec, where, o, s));
     RTM_TRY(op->op->apply(in.ptr, o.ptr, nrhs, s, SkipFlags{}));
     RTM_TRY(out_finish(y, n * nrhs, prec, where, o, s));
     if (where == RTM_DEVICE && !stream) RTM_CUDA(cudaStreamSynchronize(s));
@@ -413,7 +442,7 @@ int rtm_preconditioner_apply(rtm_preconditioner* pc, const void* x, void* y, int
     Out o;
     const int prec = pc->op->precision;
     RTM_TRY(stage_in(x, n * nrhs, prec, where, in, s));
-    RTM_TRY(out_prepare(y, n * nrhs, prec, where, o));
+    RTM_TRY(out_prepare(y, n * nrhs, prec, where, o, s));
     RTM_TRY(pc->op->apply(in.ptr, o.ptr, nrhs, s, SkipFlags{}));
     RTM_TRY(out_finish(y, n * nrhs, prec, where, o, s));
     if (where == RTM_DEVICE && !stream) RTM_CUDA(cudaStreamSynchronize(s));
@@ -472,7 +501,7 @@ int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_config* 
     Out o;
     RTM_TRY(stage_in(b, n * nrhs, prec, where, sb, s));
     RTM_TRY(stage_in(x0, n * nrhs, prec, where, sx0, s));
-    RTM_TRY(out_prepare(x, n * nrhs, prec, where, o));
+    RTM_TRY(out_prepare(x, n * nrhs, prec, where, o, s));
     SolveConfig cfg;
     cfg.method = config->method;
     cfg.tolerance = config->tolerance;
@@ -515,7 +544,7 @@ int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner
     Out o;
     RTM_TRY(stage_in(b, n * nrhs, RTM_FP64, where, sb, s));
     RTM_TRY(stage_in(x0, n * nrhs, RTM_FP64, where, sx0, s));
-    RTM_TRY(out_prepare(x, n * nrhs, RTM_FP64, where, o));
+    RTM_TRY(out_prepare(x, n * nrhs, RTM_FP64, where, o, s));
     SolveConfig cfg;
     cfg.method = config->method;
     cfg.tolerance = config->tolerance;
@@ -549,18 +578,17 @@ int rtm_plane_wave(int count_x, int count_y, double size_x, double size_y, int o
     if (!directions || !polarizations || !intensities || !out || nrhs < 1) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
     if (count_x < 1 || count_y < 1 || order < 1) return fail(RTM_ERR_ARG, "invalid grid or order");
-    cudaStream_t own = nullptr;
-    RTM_TRY(make_stream(&own));
-    cudaStream_t s = pick(stream, own);
+    CallStream own;
+    RTM_TRY(make_stream(&own.s));
+    cudaStream_t s = pick(stream, own.s);
     const int64_t n = (int64_t)(count_x - 1) * count_y + (int64_t)count_x * (count_y - 1);
     Out o;
-    int st = out_prepare(out, n * nrhs, RTM_FP64, where, o);
+    int st = out_prepare(out, n * nrhs, RTM_FP64, where, o, s);
     if (st == RTM_OK)
         st = plane_wave(count_x, count_y, size_x, size_y, order, wavenumber, directions, polarizations, intensities,
                         nrhs, static_cast<double2*>(o.ptr), s);
     if (st == RTM_OK) st = out_finish(out, n * nrhs, RTM_FP64, where, o, s);
     cudaStreamSynchronize(s);
-    cudaStreamDestroy(own);
     return st;
 }
 
@@ -599,15 +627,15 @@ int rtm_radar_cross_section(double wavenumber, const void* excitation, const voi
                             double intensity, int where, double* out) {
     if (!excitation || !current || !out || n < 1) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
-    cudaStream_t s;
-    RTM_TRY(make_stream(&s));
+    CallStream own;
+    RTM_TRY(make_stream(&own.s));
+    cudaStream_t s = own.s;
     Staged e, j;
     int st = stage_in(excitation, n, RTM_FP64, where, e, s);
     if (st == RTM_OK) st = stage_in(current, n, RTM_FP64, where, j, s);
     if (st == RTM_OK)
         st = radar_cross_section(wavenumber, static_cast<const double2*>(e.ptr), static_cast<const double2*>(j.ptr), n,
                                  intensity, out, s);
-    cudaStreamDestroy(s);
     return st;
 }
 
@@ -616,14 +644,14 @@ int rtm_input_impedance(int count_x, int count_y, double size_x, double size_y, 
     if (!current || !port || port_count < 1 || !out) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
     const int64_t n = (int64_t)(count_x - 1) * count_y + (int64_t)count_x * (count_y - 1);
-    cudaStream_t s;
-    RTM_TRY(make_stream(&s));
+    CallStream own;
+    RTM_TRY(make_stream(&own.s));
+    cudaStream_t s = own.s;
     Staged j;
     int st = stage_in(current, n, RTM_FP64, where, j, s);
     if (st == RTM_OK)
         st = input_impedance(count_x, count_y, size_x, size_y, static_cast<const double2*>(j.ptr), port, port_count,
                              voltage, out, s);
-    cudaStreamDestroy(s);
     return st;
 }
 

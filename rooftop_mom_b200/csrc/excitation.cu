@@ -75,6 +75,7 @@ int plane_wave(int cx, int cy, double a, double b, int order, double k, const do
         }
     }
     DeviceBuffer d_dirs, d_refs;
+    StreamSyncGuard guard(s);
     RTM_TRY(d_dirs.alloc(sizeof(double) * 3 * nrhs));
     RTM_TRY(d_refs.alloc(sizeof(double2) * 2 * nrhs));
     RTM_CUDA(cudaMemcpyAsync(d_dirs.ptr, dirs, sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, s));
@@ -145,6 +146,7 @@ __global__ void k_port_sum(const double2* __restrict__ J, const int64_t* __restr
 int radar_cross_section(double k, const double2* e, const double2* J, int64_t n, double intensity, double* out,
                         cudaStream_t s) {
     DeviceBuffer r;
+    StreamSyncGuard guard(s);
     RTM_TRY(r.alloc(sizeof(double2)));
     k_dot_u<<<1, 1024, 0, s>>>(e, J, n, r.as<double2>());
     count_launch();
@@ -162,6 +164,7 @@ int input_impedance(int cx, int cy, double a, double b, const double2* J, const 
     std::vector<double> w(count);
     for (int i = 0; i < count; ++i) w[i] = port_host[i] < nx ? b : a;  // edge lengths (UniformRooftops.m:89-101)
     DeviceBuffer d_port, d_w, r;
+    StreamSyncGuard guard(s);
     RTM_TRY(d_port.alloc(sizeof(int64_t) * count));
     RTM_TRY(d_w.alloc(sizeof(double) * count));
     RTM_TRY(r.alloc(sizeof(double2)));

@@ -760,6 +760,7 @@ int build_product(const DeviceGenerators& g, double size_x, double size_y, int p
     if (out.content == RTM_BOTH) {
         out.mode = kGen3;
         DeviceBuffer raw;
+        StreamSyncGuard guard(s);
         RTM_TRY(raw.alloc((size_t)nsub * 3 * G * sizeof(double2)));
         RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
         for (int sub = 0; sub < nsub; ++sub) {
@@ -790,6 +791,7 @@ int build_product(const DeviceGenerators& g, double size_x, double size_y, int p
     const int L = xs ? out.P : out.Q;
     const int ns = xs ? out.nsx : out.nsy;
     DeviceBuffer raw, blocks64;
+    StreamSyncGuard guard(s);
     RTM_TRY(raw.alloc((size_t)ns * 2 * G * sizeof(double2)));
     RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
     for (int sub = 0; sub < ns; ++sub) {
@@ -859,7 +861,8 @@ int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int
     a.twQ = out.tQ->tw64;
     a.realify = 0;
     const int64_t G = (int64_t)cx * cy;
-    DeviceBuffer raw;
+    DeviceBuffer raw, inv, flag;
+    StreamSyncGuard guard(s);
     RTM_TRY(raw.alloc(3 * (size_t)G * sizeof(double2)));
     RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
     const double2* gens[3] = {g.e.as<double2>(), g.xx.as<double2>(), g.yy.as<double2>()};
@@ -875,7 +878,6 @@ int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int
         it.dst = raw.as<double2>() + k * G;
     }
     RTM_TRY(run_gen(a, s));
-    DeviceBuffer inv, flag;
     RTM_TRY(inv.alloc(4 * (size_t)G * sizeof(double2)));
     RTM_TRY(flag.alloc(sizeof(int)));
     RTM_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(int), s));
@@ -908,6 +910,7 @@ int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int
         const bool xs = out.content == RTM_XONLY;
         const int L = xs ? cx : cy;
         DeviceBuffer line;
+        StreamSyncGuard line_guard(s);
         RTM_TRY(line.alloc((size_t)L * sizeof(double2)));
         RTM_CUDA(cudaMemcpyAsync(line.ptr, inv.as<double2>() + (xs ? 0 : 3 * G), L * sizeof(double2),
                                  cudaMemcpyDeviceToDevice, s));

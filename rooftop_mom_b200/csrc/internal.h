@@ -37,11 +37,17 @@ inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (int64_t)n
 int budget_require(double bytes, const char* what);
 void budget_hold(double bytes);
 void budget_release(double bytes);
+// Returns the cached idle blocks of the current device to the driver.
+void release_cached_blocks();
 
 // Device buffer owned by a handle; its bytes are held in the budget while it lives.
+// Blocks come from a per-device cache of freed blocks (no cudaFree, whose implicit device-wide
+// synchronisation would stall concurrent solves); the cache is emptied when cudaMalloc fails.
 struct DeviceBuffer {
     void* ptr = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;     // requested (held in the budget)
+    size_t capacity = 0;  // size of the cached block
+    int device = 0;
     DeviceBuffer() = default;
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
@@ -49,6 +55,20 @@ struct DeviceBuffer {
     int alloc(size_t n);
     void reset();
     template <typename T> T* as() const { return reinterpret_cast<T*>(ptr); }
+    // Moves another buffer's block into this one.
+    void take(DeviceBuffer& o) {
+        reset();
+        ptr = o.ptr; bytes = o.bytes; capacity = o.capacity; device = o.device;
+        o.ptr = nullptr; o.bytes = 0; o.capacity = 0;
+    }
+};
+
+// Synchronises a stream when it leaves scope. Declared after a function's device buffers, it runs
+// before their blocks return to the cache, on every path out of the function.
+struct StreamSyncGuard {
+    cudaStream_t s;
+    explicit StreamSyncGuard(cudaStream_t st) : s(st) {}
+    ~StreamSyncGuard() { cudaStreamSynchronize(s); }
 };
 
 // ---------------------------------------------------------------------------------------------

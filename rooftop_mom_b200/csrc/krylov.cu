@@ -761,6 +761,7 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
     const int nb = reduce_blocks(n);
     const size_t vec = (size_t)n * nrhs * sizeof(T2);
     DeviceBuffer r, z, d, q, stb, part, hist, resb, cnt;
+    StreamSyncGuard guard(s);
     RTM_TRY(r.alloc(vec));
     if (M) RTM_TRY(z.alloc(vec));
     RTM_TRY(d.alloc(vec));
@@ -866,6 +867,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     // residual is the residual of A x = b itself. Left preconditioning is the reference's form.
     const bool right = M != nullptr && cfg.right_preconditioned;
     DeviceBuffer V, Z, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
+    StreamSyncGuard guard(s);
     RTM_TRY(V.alloc(vec * (m + 1)));
     if (right) RTM_TRY(Z.alloc(vec * m));
     RTM_TRY(w.alloc(vec));
@@ -1060,6 +1062,7 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     const size_t vec64 = (size_t)n * nrhs * sizeof(double2), vec32 = (size_t)n * nrhs * sizeof(float2);
     const int m = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)cfg.restart, n));
     DeviceBuffer r64, t64, r32, d32, part, resb, cnt, done, conv, hist;
+    StreamSyncGuard guard(s);
     RTM_TRY(r64.alloc(vec64));
     RTM_TRY(t64.alloc(vec64));
     RTM_TRY(r32.alloc(vec32));

@@ -225,6 +225,7 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
     op->nblocks = g.nbx * g.nby;
     const size_t nb = (size_t)op->nblocks;
     DeviceBuffer inv64, flag;
+    StreamSyncGuard guard(s);
     if ((*status = op->counts.alloc(nb * sizeof(int))) != RTM_OK) return nullptr;
     if ((*status = op->index.alloc(nb * kMaxBlockUnknowns * sizeof(int64_t))) != RTM_OK) return nullptr;
     if ((*status = inv64.alloc(nb * kMaxBlockUnknowns * kMaxBlockUnknowns * sizeof(double2))) != RTM_OK) return nullptr;
@@ -249,10 +250,7 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
         return nullptr;
     }
     if (precision == RTM_FP64) {
-        op->inv.ptr = inv64.ptr;
-        op->inv.bytes = inv64.bytes;
-        inv64.ptr = nullptr;
-        inv64.bytes = 0;
+        op->inv.take(inv64);
     } else {
         const int64_t cnt = (int64_t)nb * kMaxBlockUnknowns * kMaxBlockUnknowns;
         if ((*status = op->inv.alloc(cnt * sizeof(float2))) != RTM_OK) return nullptr;

@@ -72,15 +72,57 @@ void budget_release(double bytes) {
     g_held -= bytes;
 }
 
+// Per-device cache of idle device blocks, by capacity.
+static std::mutex g_pool_mu;
+static std::multimap<size_t, void*> g_pool[64];
+
+static size_t block_capacity(size_t n) {
+    if (n <= (1u << 20)) {
+        size_t c = 512;
+        while (c < n) c <<= 1;
+        return c;
+    }
+    const size_t mb = 1u << 20;
+    return (n + mb - 1) / mb * mb;
+}
+
+void release_cached_blocks() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (auto& kv : g_pool[dev & 63]) cudaFree(kv.second);
+    g_pool[dev & 63].clear();
+}
+
 int DeviceBuffer::alloc(size_t n) {
     reset();
     if (n == 0) return RTM_OK;
-    cudaError_t e = cudaMalloc(&ptr, n);
-    if (e != cudaSuccess) {
-        ptr = nullptr;
-        cudaGetLastError();
-        return fail(RTM_ERR_OOM_BUDGET, "device allocation of " + format_bytes((double)n) + " failed: " +
-                                            cudaGetErrorString(e));
+    cudaGetDevice(&device);
+    const size_t cap = block_capacity(n);
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        auto& pool = g_pool[device & 63];
+        auto it = pool.lower_bound(cap);
+        if (it != pool.end() && it->first <= cap + cap / 2) {
+            ptr = it->second;
+            capacity = it->first;
+            pool.erase(it);
+        }
+    }
+    if (!ptr) {
+        cudaError_t e = cudaMalloc(&ptr, cap);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            release_cached_blocks();
+            e = cudaMalloc(&ptr, cap);
+        }
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            cudaGetLastError();
+            return fail(RTM_ERR_OOM_BUDGET, "device allocation of " + format_bytes((double)n) + " failed: " +
+                                                cudaGetErrorString(e));
+        }
+        capacity = cap;
     }
     bytes = n;
     budget_hold((double)n);
@@ -89,11 +131,15 @@ int DeviceBuffer::alloc(size_t n) {
 
 void DeviceBuffer::reset() {
     if (ptr) {
-        cudaFree(ptr);
+        {
+            std::lock_guard<std::mutex> lk(g_pool_mu);
+            g_pool[device & 63].emplace(capacity, ptr);
+        }
         budget_release((double)bytes);
     }
     ptr = nullptr;
     bytes = 0;
+    capacity = 0;
 }
 
 // ---------------------------------------------------------------------------------------------
