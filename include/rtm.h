@@ -131,6 +131,19 @@ RTM_API int rtm_operator_create(const rtm_generators* g, double size_x, double s
  * are complex floats when where == RTM_DEVICE and complex doubles (converted) when RTM_HOST. */
 RTM_API int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int nrhs, int where, void* stream);
 
+/* y = A x like rtm_operator_apply with where == RTM_DEVICE, but allocating no device memory: the
+ * product's working grid lives in one fixed array compiled into the library
+ * (rtm_fixed_scratch_bytes, 32 MiB) instead of the operator's own buffer. No counterpart in the
+ * reference: it exists for callers whose device memory belongs to another allocator or ledger and
+ * that must not allocate per call. FFT products only; RTM_ERR_SIZE when the working grids of nrhs
+ * vectors exceed the array. The first call on a device looks the array up (make it before any stream
+ * capture). All calls on a device share the array: calls that can overlap in time race, so the
+ * caller serialises them. A null stream runs on the operator's stream and waits for the result. */
+RTM_API int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void* x, void* y, int64_t n, int nrhs,
+                                             void* stream);
+/* Size of the fixed scratch array in bytes. */
+RTM_API int rtm_fixed_scratch_bytes(double* bytes);
+
 /* A dense n x n complex operator (column-major), for solving any small system with the same solvers
  * (the matrix operator of IterativeMethod.solve, convertToHandle.m:10-16). */
 RTM_API int rtm_operator_create_dense(const double* matrix, int64_t n, int where, rtm_operator** out);

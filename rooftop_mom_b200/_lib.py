@@ -73,6 +73,8 @@ _SIGNATURES = {
     "rtm_generators_destroy": [_P],
     "rtm_operator_create": [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _PP],
     "rtm_operator_apply": [_P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
+    "rtm_operator_apply_fixed_scratch": [_P, _P, _P, C.c_int64, C.c_int, _P],
+    "rtm_fixed_scratch_bytes": [_P],
     "rtm_operator_create_dense": [_P, C.c_int64, C.c_int, _PP],
     "rtm_operator_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                           C.POINTER(C.c_double)],

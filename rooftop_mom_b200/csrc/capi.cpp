@@ -362,6 +362,23 @@ int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int 
     return RTM_OK;
 }
 
+int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void* x, void* y, int64_t n, int nrhs,
+                                     void* stream) {
+    if (!op || !x || !y) return fail(RTM_ERR_ARG, "null argument");
+    if (!op->grid) return fail(RTM_ERR_UNSUPPORTED, "the fixed scratch serves FFT products only");
+    if (n != op->op->n) return fail(RTM_ERR_SIZE, "The input must be a numeric " + std::to_string(op->op->n) + "x1 vector.");
+    cudaStream_t s = pick(stream, op->stream);
+    RTM_TRY(apply_fixed_scratch(*op->grid, x, y, nrhs, s));
+    if (!stream) RTM_CUDA(cudaStreamSynchronize(s));
+    return RTM_OK;
+}
+
+int rtm_fixed_scratch_bytes(double* bytes) {
+    if (!bytes) return fail(RTM_ERR_ARG, "null argument");
+    *bytes = (double)fixed_scratch_bytes();
+    return RTM_OK;
+}
+
 int rtm_operator_info(const rtm_operator* op, int64_t* n, int* fft_x, int* fft_y, double* spectra_bytes,
                       double* working_bytes) {
     if (!op) return fail(RTM_ERR_ARG, "null handle");

@@ -16,6 +16,7 @@
 // w = exp(-i pi / P), which is the same number as subsampling the 2P x 2Q transform.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 
 #include "fft.cuh"
@@ -351,7 +352,8 @@ size_t GridApplicator::work_bytes_per_rhs() const {
 }
 
 template <typename T>
-static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip) {
+static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip,
+                   void* work) {
     using T2 = typename Cx<T>::T2;
     set_smem_attrs<T>();
     const T2* x = static_cast<const T2*>(xv);
@@ -401,7 +403,7 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
         return RTM_OK;
     }
     a.scale = (T)(1.0 / ((double)g.P * g.Q));
-    a.work = g.work.as<T2>();
+    a.work = static_cast<T2*>(work);
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
     const int passes = g.lean ? g.nsy : 1;
     const int npy = g.lean ? 1 : g.nsy;
@@ -456,8 +458,53 @@ int GridApplicator::reserve(int nrhs) {
 
 int GridApplicator::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) {
     if (nrhs < 1 || nrhs > max_rhs) return fail(RTM_ERR_ARG, "more right-hand sides than the product reserved");
-    return precision == RTM_FP64 ? apply_t<double>(*this, x, y, nrhs, s, skip)
-                                 : apply_t<float>(*this, x, y, nrhs, s, skip);
+    return precision == RTM_FP64 ? apply_t<double>(*this, x, y, nrhs, s, skip, work.ptr)
+                                 : apply_t<float>(*this, x, y, nrhs, s, skip, work.ptr);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fixed scratch: a working grid W in a file-scope device array, for callers that must not allocate
+// device memory per call. Such callers are the ones whose device memory is owned by someone else: a
+// MATLAB MEX gateway whose gpuArray memory pool already holds the device, or a serving process
+// whose admission ledger has handed out all of HBM and cannot let a call take more behind its back.
+// Every call on a device shares the one array, so calls that may overlap in time (other streams,
+// other host threads) race on it: the caller serialises them. Nothing in it has to start at zero:
+// the y-forward pass writes every entry of W that the later passes read.
+constexpr size_t kFixedScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
+
+// The array's address per device, looked up on the first call with that device current (the lookup
+// may load the module on the device, so make that first call before any stream capture).
+static int fixed_scratch(void** out) {
+    static std::mutex mu;
+    static void* addr[64] = {};
+    int dev = 0;
+    RTM_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(RTM_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_fixed_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fixed_scratch)");
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return RTM_OK;
+}
+
+size_t fixed_scratch_bytes() { return kFixedScratchBytes; }
+
+int apply_fixed_scratch(const GridApplicator& g, const void* x, void* y, int nrhs, cudaStream_t s) {
+    if (nrhs < 1) return fail(RTM_ERR_ARG, "nrhs must be positive");
+    const size_t need = g.work_bytes_per_rhs() * (size_t)nrhs;
+    if (need > kFixedScratchBytes)
+        return fail(RTM_ERR_SIZE, "the working grid of " + std::to_string(nrhs) + " right-hand sides needs " +
+                                      std::to_string(need) + " bytes, above the fixed scratch of " +
+                                      std::to_string(kFixedScratchBytes) + " bytes");
+    void* work = nullptr;
+    if (g.mode != kStrip) RTM_TRY(fixed_scratch(&work));
+    return g.precision == RTM_FP64 ? apply_t<double>(g, x, y, nrhs, s, SkipFlags{}, work)
+                                   : apply_t<float>(g, x, y, nrhs, s, SkipFlags{}, work);
 }
 
 // ============================================================================================

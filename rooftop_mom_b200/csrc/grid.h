@@ -48,6 +48,11 @@ struct GridApplicator : LinearOp {
     double working_bytes() const override { return (double)work.bytes; }
 };
 
+// y = A x with the working grid in a fixed device array of fixed_scratch_bytes() instead of the
+// product's own buffer; allocates nothing (RTM_ERR_SIZE when nrhs working grids do not fit).
+int apply_fixed_scratch(const GridApplicator& g, const void* x, void* y, int nrhs, cudaStream_t s);
+size_t fixed_scratch_bytes();
+
 // Generator set on the device (FP64 complex, column-major).
 struct DeviceGenerators {
     int count_x = 0, count_y = 0;
