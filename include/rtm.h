@@ -231,6 +231,77 @@ RTM_API int rtm_input_impedance(int count_x, int count_y, double size_x, double 
                         const int64_t* port, int port_count, double voltage, int where, double* out);
 /* (out of rtm_input_impedance: out[0] + i out[1], the complex input impedance in ohms) */
 
+/* Serving: a request loop of plate solves ------------------------------------------------------
+ * No counterpart in the reference, whose closest analogue is the admission check of its memory
+ * ledger (Budget.require, src/+rooftopMoM/+resources/Budget.m:82-106, fed by the byte models
+ * estimate*.m). A server admits submitted requests first-fit in arrival order while a slot is free
+ * and their estimated device bytes fit under the budget; each admitted request runs the whole
+ * pipeline (assembly, split-FFT product, preconditioner, excitation, solve, RCS or input impedance)
+ * on its own worker thread and CUDA streams, so the device work of admitted requests overlaps, and
+ * requests that arrive meanwhile are admitted as slots and bytes free up. A request's result does not
+ * depend on what else runs: every kernel's launch shape follows from the request alone. */
+typedef struct rtm_server rtm_server;
+
+typedef struct rtm_server_config {
+    double budget_bytes;   /* device bytes the admitted requests may hold together (<= 0: 150e9) */
+    int max_active;        /* requests admitted at once, one worker thread each (<= 0: 8) */
+    int precision;         /* RTM_FP64, or RTM_FP32 for the mixed form (FP32 inner FGMRES, FP64 refinement) */
+    int device;            /* CUDA device of the workers */
+} rtm_server_config;
+
+typedef enum rtm_excitation { RTM_EXCITE_PLANE_WAVE = 0, RTM_EXCITE_DELTA_GAP = 1 } rtm_excitation;
+typedef enum rtm_request_state {
+    RTM_REQUEST_QUEUED = 0,
+    RTM_REQUEST_RUNNING = 1,
+    RTM_REQUEST_DONE = 2,
+    RTM_REQUEST_FAILED = 3,
+    RTM_REQUEST_CANCELLED = 4
+} rtm_request_state;
+
+typedef struct rtm_request {
+    int count_x, count_y;       /* faces of the plate (count_y = 1: a strip) */
+    double size_x, size_y;      /* face sizes in metres */
+    double wavenumber;          /* k = 2 pi f / c */
+    int excitation;             /* rtm_excitation */
+    double direction[3];        /* plane wave: unit propagation direction */
+    double polarization[3];     /* plane wave: unit polarisation (intensity 1) */
+    int port_direction;         /* delta gap: middle port across x (0) or y (1) rooftops */
+    double voltage;             /* delta gap: gap voltage */
+    int method;                 /* RTM_METHOD_CG or RTM_METHOD_GMRES (right-preconditioned) */
+    int block_jacobi;           /* nonzero: 2 x 2-face block-Jacobi preconditioner */
+    double tolerance;
+    int max_iterations;
+    int restart;
+    int keep_current;           /* nonzero: keep the solution for rtm_server_poll to copy out */
+} rtm_request;
+
+typedef struct rtm_request_result {
+    int state;                  /* rtm_request_state */
+    int status;                 /* rtm_status of a failed request */
+    int converged, iteration_count;
+    double residual_norm;       /* true FP64 relative residual */
+    double rcs;                 /* plane wave: monostatic radar cross section (m^2) */
+    double impedance[2];        /* delta gap: input impedance, re and im (ohm) */
+    int64_t unknowns;
+    double bytes;               /* estimated device bytes the request held */
+    double submitted_s, started_s, finished_s; /* host clock, seconds since the server was created */
+    double solve_s;             /* device time of the solve */
+} rtm_request_result;
+
+RTM_API int rtm_server_create(const rtm_server_config* config, rtm_server** out);
+/* Queues a request; *id identifies it. A request whose estimate alone exceeds the budget fails at once
+ * with RTM_ERR_OOM_BUDGET (rooftopMoM:resources:insufficientMemory). */
+RTM_API int rtm_server_submit(rtm_server* server, const rtm_request* request, uint64_t* id);
+/* Copies the request's state and result, waiting up to wait_ms for it to finish (0: no wait, < 0:
+ * until it finishes). current (host, n complex doubles) receives the solution of a finished request
+ * that kept it; release != 0 forgets a finished request afterwards. */
+RTM_API int rtm_server_poll(rtm_server* server, uint64_t id, int wait_ms, rtm_request_result* out, double* current,
+                            int64_t n, int release);
+/* Cancels a queued request at once, a running one at its solver's next host check. */
+RTM_API int rtm_server_cancel(rtm_server* server, uint64_t id);
+/* Cancels what is queued, lets running requests stop, joins the workers and frees the server. */
+RTM_API int rtm_server_destroy(rtm_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,5 +15,6 @@ from .api import (  # noqa: F401
     Solver,
     fast_fft_size,
 )
+from .server import Request, Server  # noqa: F401
 
 __version__ = "3.5.0"

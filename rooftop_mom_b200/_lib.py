@@ -56,6 +56,28 @@ class SolveStats(C.Structure):
 
 _P = C.c_void_p
 _PP = C.POINTER(C.c_void_p)
+class ServerConfig(C.Structure):
+    _fields_ = [("budget_bytes", C.c_double), ("max_active", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("count_x", C.c_int), ("count_y", C.c_int), ("size_x", C.c_double), ("size_y", C.c_double),
+                ("wavenumber", C.c_double), ("excitation", C.c_int), ("direction", C.c_double * 3),
+                ("polarization", C.c_double * 3), ("port_direction", C.c_int), ("voltage", C.c_double),
+                ("method", C.c_int), ("block_jacobi", C.c_int), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int), ("restart", C.c_int), ("keep_current", C.c_int)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("converged", C.c_int), ("iteration_count", C.c_int),
+                ("residual_norm", C.c_double), ("rcs", C.c_double), ("impedance", C.c_double * 2),
+                ("unknowns", C.c_int64), ("bytes", C.c_double), ("submitted_s", C.c_double),
+                ("started_s", C.c_double), ("finished_s", C.c_double), ("solve_s", C.c_double)]
+
+
+EXCITATIONS = {"planeWave": 0, "deltaGap": 1}
+STATES = ("queued", "running", "done", "failed", "cancelled")
+
 _SIGNATURES = {
     "rtm_version": [C.POINTER(C.c_int)] * 3,
     "rtm_last_error": [C.c_char_p, C.c_size_t],
@@ -94,6 +116,11 @@ _SIGNATURES = {
     "rtm_radar_cross_section": [C.c_double, _P, _P, C.c_int64, C.c_double, C.c_int, C.POINTER(C.c_double)],
     "rtm_input_impedance": [C.c_int, C.c_int, C.c_double, C.c_double, _P, _P, C.c_int, C.c_double, C.c_int,
                             C.POINTER(C.c_double)],
+    "rtm_server_create": [C.POINTER(ServerConfig), _PP],
+    "rtm_server_submit": [_P, C.POINTER(Request), C.POINTER(C.c_uint64)],
+    "rtm_server_poll": [_P, C.c_uint64, C.c_int, C.POINTER(RequestResult), _P, C.c_int64, C.c_int],
+    "rtm_server_cancel": [_P, C.c_uint64],
+    "rtm_server_destroy": [_P],
 }
 
 _lock = threading.Lock()

@@ -7,48 +7,28 @@
 #include <vector>
 
 #include "excitation.h"
-#include "grid.h"
+#include "handles.h"
 #include "krylov.h"
-#include "ops.h"
 
 using namespace rtm;
 
-struct rtm_generators {
-    DeviceGenerators g;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    ~rtm_generators() {
-        if (stream) cudaStreamSynchronize(stream);
-        g.xx.reset();
-        g.yy.reset();
-        g.e.reset();
-        if (stream) cudaStreamDestroy(stream);
+namespace rtm {
+int middle_port(int count_x, int count_y, int direction, std::vector<int64_t>& p) {
+    // generateMiddlePort.m:14-28
+    const int64_t nx = (int64_t)(count_x - 1) * count_y, n = nx + (int64_t)count_x * (count_y - 1);
+    p.clear();
+    if (direction == 0) {
+        if (nx == 0) return fail(RTM_ERR_ARG, "The mesh has no x-directed rooftops.");
+        const int row = count_x / 2 - 1;
+        for (int c = 0; c < count_y; ++c) p.push_back(row + (int64_t)c * (count_x - 1));
+    } else {
+        if (n - nx == 0) return fail(RTM_ERR_ARG, "The mesh has no y-directed rooftops.");
+        const int col = count_y / 2 - 1;
+        for (int r = 0; r < count_x; ++r) p.push_back(nx + r + (int64_t)col * count_x);
     }
-};
-
-struct rtm_operator {
-    std::unique_ptr<LinearOp> op;
-    GridApplicator* grid = nullptr;  // the same object when the product is an FFT product
-    int kind = 0;                    // rtm_product, or -1 for a dense matrix
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    ~rtm_operator() {
-        if (stream) cudaStreamSynchronize(stream);
-        op.reset();
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-struct rtm_preconditioner {
-    std::unique_ptr<LinearOp> op;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    ~rtm_preconditioner() {
-        if (stream) cudaStreamSynchronize(stream);
-        op.reset();
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
+    return RTM_OK;
+}
+}  // namespace rtm
 
 namespace {
 
@@ -622,16 +602,7 @@ int rtm_delta_gap(int count_x, int count_y, double size_x, double size_y, const 
         if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end() || sorted.front() < 0 || sorted.back() >= n)
             return fail(RTM_ERR_ARG, "The port must hold distinct rooftop indices up to " + std::to_string(n) + ".");
     } else {
-        // generateMiddlePort.m:14-28
-        if (direction == 0) {
-            if (nx == 0) return fail(RTM_ERR_ARG, "The mesh has no x-directed rooftops.");
-            const int row = count_x / 2 - 1;
-            for (int c = 0; c < count_y; ++c) p.push_back(row + (int64_t)c * (count_x - 1));
-        } else {
-            if (n - nx == 0) return fail(RTM_ERR_ARG, "The mesh has no y-directed rooftops.");
-            const int col = count_y / 2 - 1;
-            for (int r = 0; r < count_x; ++r) p.push_back(nx + r + (int64_t)col * count_x);
-        }
+        RTM_TRY(middle_port(count_x, count_y, direction, p));
     }
     std::vector<double2> v((size_t)n, make_double2(0, 0));
     for (int64_t i : p) v[(size_t)i] = make_double2(voltage * (i < nx ? size_y : size_x), 0.0);

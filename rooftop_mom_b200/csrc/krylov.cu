@@ -824,7 +824,7 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
         RTM_CUDA(cudaStreamSynchronize(s));
         bool all = true;
         for (auto& h : host) all = all && h.done;
-        if (all || launched >= cfg.max_iterations) break;
+        if (all || launched >= cfg.max_iterations || (cfg.cancel && *cfg.cancel)) break;
         RTM_TRY(graph.run(s, chunk_body));
         launched += every;
     }
@@ -976,7 +976,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         RTM_CUDA(cudaStreamSynchronize(s));
         bool all = true;
         for (auto& hh : host) all = all && hh.done;
-        if (all || cycles > cfg.max_iterations) break;
+        if (all || cycles > cfg.max_iterations || (cfg.cancel && *cfg.cancel)) break;
         RTM_TRY(graph.run(s, cycle_body));
         ++cycles;
         res.matvecs += 1;
@@ -1102,7 +1102,8 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         steps = step;
         bool all = true;
         for (int v : hd) all = all && v;
-        if (all || step >= cfg.max_refinements || inner_total >= cfg.max_iterations) break;
+        if (all || step >= cfg.max_refinements || inner_total >= cfg.max_iterations || (cfg.cancel && *cfg.cancel))
+            break;
         k_ir_to32<<<grid, kRT, 0, s>>>(r64.as<double2>(), r32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
         // The inner FP32 solve of A32 d = r / ||r||: COCG, or restarted flexible GMRES(m).
@@ -1113,6 +1114,7 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         ic.restart = m;
         ic.check_every = cfg.check_every;
         ic.right_preconditioned = 1;
+        ic.cancel = cfg.cancel;
         SolveResult ir;
         if (inner_cg) RTM_TRY(cocg<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
         else RTM_TRY(gmres<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));

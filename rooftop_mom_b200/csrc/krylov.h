@@ -16,6 +16,7 @@ struct SolveConfig {
     double inner_tolerance = 1e-4;
     int max_refinements = 20;
     int right_preconditioned = 0;  // GMRES: 0 left (the reference's form), 1 right (flexible)
+    const volatile int* cancel = nullptr;  // nonzero: stop at the next host check (unconverged result)
 };
 
 struct SolveResult {

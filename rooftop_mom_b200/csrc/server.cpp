@@ -1,0 +1,335 @@
+// The serving form: a request loop of plate solves (include/rtm.h, rtm_server_*).
+//
+// Admission follows the reference's memory ledger (src/+rooftopMoM/+resources/Budget.m:82-106): a
+// request is admitted only when its estimated device bytes (the byte models of
+// estimateGenerators.m:11, estimateProduct.m:13-37 and estimateSolver.m:19-26, as rtm_estimate_bytes)
+// fit under what the admitted requests leave of the budget. Admission scans the queue in arrival
+// order and takes every request that fits while a slot is free, so a large request at the head does
+// not hold back small ones behind it.
+//
+// Each slot is a host worker thread. An admitted request runs its whole pipeline on that thread with
+// the handles' own non-blocking streams: assembly, split-FFT product, block-Jacobi preconditioner,
+// excitation on the device, the solve, the RCS or input impedance. Device work of different requests
+// overlaps; no call here synchronises the whole device. Results depend on the request alone, since
+// every launch shape follows from the request's sizes.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "handles.h"
+#include "krylov.h"
+
+using namespace rtm;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kBlockJacobiUnknowns = 16;  // storage per block of the block-Jacobi inverse (ops.cu)
+
+struct Record {
+    uint64_t id = 0;
+    rtm_request req{};
+    rtm_request_result res{};
+    std::vector<double> current;  // interleaved complex
+    volatile int cancel = 0;
+};
+
+double seconds_since(Clock::time_point t0) {
+    return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+int check_request(const rtm_request& q) {
+    if (q.count_x < 1 || q.count_y < 1) return fail(RTM_ERR_ARG, "The face counts must be positive.");
+    if ((int64_t)(q.count_x - 1) * q.count_y + (int64_t)q.count_x * (q.count_y - 1) < 1)
+        return fail(RTM_ERR_ARG, "The plate is a single face, which carries no rooftop.");
+    if (!(q.size_x > 0) || !(q.size_y > 0) || !(q.wavenumber > 0)) return fail(RTM_ERR_ARG, "invalid sizes");
+    if (q.excitation != RTM_EXCITE_PLANE_WAVE && q.excitation != RTM_EXCITE_DELTA_GAP)
+        return fail(RTM_ERR_ARG, "unknown excitation");
+    if (q.method != RTM_METHOD_CG && q.method != RTM_METHOD_GMRES) return fail(RTM_ERR_ARG, "unknown method");
+    if (!(q.tolerance > 0) || q.max_iterations < 1 || q.restart < 1) return fail(RTM_ERR_ARG, "invalid solver");
+    return RTM_OK;
+}
+
+// Device bytes of a request's pipeline (generators, product spectra and working grids, preconditioner,
+// solver vectors, excitation and solution), in the server's precision.
+int request_bytes(const rtm_request& q, int precision, double* bytes) {
+    double est[6];
+    RTM_TRY(rtm_estimate_bytes(q.count_x, q.count_y, RTM_PRODUCT_SPLIT, q.method, q.block_jacobi != 0, q.restart,
+                               q.max_iterations, est));
+    const double n = (double)(q.count_x - 1) * q.count_y + (double)q.count_x * (q.count_y - 1);
+    const double blocks = (double)((q.count_x + 1) / 2) * ((q.count_y + 1) / 2);
+    const double bj = q.block_jacobi
+                          ? blocks * (kBlockJacobiUnknowns * kBlockJacobiUnknowns * 16.0 + kBlockJacobiUnknowns * 8.0 + 4)
+                          : 0;
+    double total = est[0] + est[1] + est[2] + bj + est[5] + 2 * 16 * n;
+    if (precision == RTM_FP32) total += 0.5 * (est[1] + est[2] + est[5]) + 4 * 16 * n;  // inner FP32 copies
+    *bytes = total;
+    return RTM_OK;
+}
+
+}  // namespace
+
+struct rtm_server {
+    rtm_server_config cfg{};
+    Clock::time_point epoch;
+    std::mutex mu;
+    std::condition_variable work_cv, done_cv;
+    std::deque<uint64_t> queue;  // waiting, in arrival order
+    std::deque<uint64_t> ready;  // admitted, not yet taken by a worker
+    std::map<uint64_t, std::unique_ptr<Record>> records;
+    double held = 0;
+    int admitted = 0;
+    uint64_t next_id = 1;
+    bool stopping = false;
+    std::vector<std::thread> workers;
+
+    void admit_locked() {
+        for (auto it = queue.begin(); it != queue.end() && admitted < cfg.max_active;) {
+            Record& r = *records.at(*it);
+            if (held + r.res.bytes <= cfg.budget_bytes) {
+                held += r.res.bytes;
+                ++admitted;
+                ready.push_back(*it);
+                it = queue.erase(it);
+                work_cv.notify_one();
+            } else {
+                ++it;
+            }
+        }
+    }
+
+    void worker() {
+        cudaSetDevice(cfg.device);
+        while (true) {
+            Record* r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                work_cv.wait(lk, [&] { return stopping || !ready.empty(); });
+                if (ready.empty()) return;  // stopping
+                r = records.at(ready.front()).get();
+                ready.pop_front();
+                if (r->cancel) {
+                    r->res.state = RTM_REQUEST_CANCELLED;
+                    r->res.finished_s = seconds_since(epoch);
+                } else {
+                    r->res.state = RTM_REQUEST_RUNNING;
+                    r->res.started_s = seconds_since(epoch);
+                }
+            }
+            int st = RTM_OK;
+            if (r->res.state == RTM_REQUEST_RUNNING) st = run(*r);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (r->res.state == RTM_REQUEST_RUNNING) {
+                    r->res.finished_s = seconds_since(epoch);
+                    r->res.status = st;
+                    r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
+                                             : (st == RTM_OK ? RTM_REQUEST_DONE : RTM_REQUEST_FAILED);
+                }
+                held -= r->res.bytes;
+                --admitted;
+                admit_locked();
+            }
+            done_cv.notify_all();
+        }
+    }
+
+    // The whole pipeline of one request on this thread.
+    int run(Record& r) {
+        const rtm_request& q = r.req;
+        struct Handles {
+            rtm_generators* g = nullptr;
+            rtm_operator* op = nullptr;
+            rtm_operator* op32 = nullptr;
+            rtm_preconditioner* pc = nullptr;
+            ~Handles() {
+                rtm_preconditioner_destroy(pc);
+                rtm_operator_destroy(op32);
+                rtm_operator_destroy(op);
+                rtm_generators_destroy(g);
+            }
+        } h;
+        const bool mixed = cfg.precision == RTM_FP32;
+        RTM_TRY(rtm_generators_assemble(q.count_x, q.count_y, q.size_x, q.size_y, q.wavenumber, 16, 8, nullptr, &h.g));
+        RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP64, 1, &h.op));
+        if (mixed) RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP32, 1, &h.op32));
+        if (q.block_jacobi)
+            RTM_TRY(rtm_preconditioner_create_block_jacobi(h.g, q.size_x, q.size_y, 2, 2, mixed ? RTM_FP32 : RTM_FP64,
+                                                           &h.pc));
+        const int64_t n = h.op->op->n;
+        r.res.unknowns = n;
+        cudaStream_t s = h.op->stream;
+        DeviceBuffer b, x;
+        StreamSyncGuard guard(s);
+        RTM_TRY(b.alloc((size_t)n * sizeof(double2)));
+        RTM_TRY(x.alloc((size_t)n * sizeof(double2)));
+        std::vector<int64_t> port;
+        if (q.excitation == RTM_EXCITE_PLANE_WAVE) {
+            const double one = 1.0;
+            RTM_TRY(rtm_plane_wave(q.count_x, q.count_y, q.size_x, q.size_y, 8, q.wavenumber, q.direction,
+                                   q.polarization, &one, 1, b.ptr, RTM_DEVICE, s));
+        } else {
+            RTM_TRY(middle_port(q.count_x, q.count_y, q.port_direction, port));
+            RTM_TRY(rtm_delta_gap(q.count_x, q.count_y, q.size_x, q.size_y, port.data(), (int)port.size(), 0,
+                                  q.voltage, b.ptr, RTM_DEVICE));
+        }
+        SolveConfig sc;
+        sc.method = q.method;
+        sc.tolerance = q.tolerance;
+        sc.max_iterations = q.max_iterations;
+        sc.restart = q.restart;
+        sc.right_preconditioned = 1;
+        sc.cancel = &r.cancel;
+        SolveResult res;
+        cudaEvent_t e0, e1;
+        RTM_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDefault));
+        RTM_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDefault));
+        cudaEventRecord(e0, s);
+        int st;
+        if (mixed) {
+            sc.inner_tolerance = 1e-4;
+            st = solve_mixed(h.op->op.get(), h.op32->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr,
+                             x.ptr, n, 1, res, s);
+        } else {
+            st = solve(h.op->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr, x.ptr, n, 1, res, s);
+        }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st != RTM_OK) return st;
+        r.res.solve_s = ms * 1e-3;
+        if (!res.stats.empty()) {
+            r.res.converged = res.stats[0].converged;
+            r.res.iteration_count = res.stats[0].iteration_count;
+            r.res.residual_norm = res.stats[0].residual_norm;
+        }
+        if (q.excitation == RTM_EXCITE_PLANE_WAVE)
+            RTM_TRY(rtm_radar_cross_section(q.wavenumber, b.ptr, x.ptr, n, 1.0, RTM_DEVICE, &r.res.rcs));
+        else
+            RTM_TRY(rtm_input_impedance(q.count_x, q.count_y, q.size_x, q.size_y, x.ptr, port.data(), (int)port.size(),
+                                        q.voltage, RTM_DEVICE, r.res.impedance));
+        if (q.keep_current) {
+            r.current.resize((size_t)2 * n);
+            RTM_CUDA(cudaMemcpyAsync(r.current.data(), x.ptr, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+            RTM_CUDA(cudaStreamSynchronize(s));
+        }
+        return RTM_OK;
+    }
+};
+
+extern "C" {
+
+int rtm_server_create(const rtm_server_config* config, rtm_server** out) {
+    if (!out) return fail(RTM_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto srv = std::make_unique<rtm_server>();
+    if (config) srv->cfg = *config;
+    if (!(srv->cfg.budget_bytes > 0)) srv->cfg.budget_bytes = 150e9;
+    if (srv->cfg.max_active <= 0) srv->cfg.max_active = 8;
+    if (srv->cfg.precision != RTM_FP64 && srv->cfg.precision != RTM_FP32)
+        return fail(RTM_ERR_ARG, "precision must be RTM_FP64 or RTM_FP32");
+    if (srv->cfg.max_active > 256) return fail(RTM_ERR_ARG, "at most 256 active requests");
+    srv->epoch = Clock::now();
+    rtm_server* p = srv.get();
+    for (int i = 0; i < srv->cfg.max_active; ++i) srv->workers.emplace_back([p] { p->worker(); });
+    *out = srv.release();
+    return RTM_OK;
+}
+
+int rtm_server_submit(rtm_server* srv, const rtm_request* request, uint64_t* id) {
+    if (!srv || !request || !id) return fail(RTM_ERR_ARG, "null argument");
+    RTM_TRY(check_request(*request));
+    auto rec = std::make_unique<Record>();
+    rec->req = *request;
+    RTM_TRY(request_bytes(*request, srv->cfg.precision, &rec->res.bytes));
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return fail(RTM_ERR_ARG, "the server is stopping");
+    rec->id = srv->next_id++;
+    rec->res.submitted_s = seconds_since(srv->epoch);
+    *id = rec->id;
+    if (rec->res.bytes > srv->cfg.budget_bytes) {
+        rec->res.state = RTM_REQUEST_FAILED;
+        rec->res.status = RTM_ERR_OOM_BUDGET;
+        rec->res.finished_s = rec->res.submitted_s;
+        srv->records.emplace(rec->id, std::move(rec));
+        srv->done_cv.notify_all();
+        return RTM_OK;
+    }
+    rec->res.state = RTM_REQUEST_QUEUED;
+    srv->queue.push_back(rec->id);
+    srv->records.emplace(rec->id, std::move(rec));
+    srv->admit_locked();
+    return RTM_OK;
+}
+
+int rtm_server_poll(rtm_server* srv, uint64_t id, int wait_ms, rtm_request_result* out, double* current, int64_t n,
+                    int release) {
+    if (!srv || !out) return fail(RTM_ERR_ARG, "null argument");
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->records.find(id);
+    if (it == srv->records.end()) return fail(RTM_ERR_ARG, "unknown request " + std::to_string(id));
+    Record* r = it->second.get();
+    auto finished = [&] { return r->res.state >= RTM_REQUEST_DONE; };
+    if (wait_ms < 0) srv->done_cv.wait(lk, finished);
+    else if (wait_ms > 0) srv->done_cv.wait_for(lk, std::chrono::milliseconds(wait_ms), finished);
+    *out = r->res;
+    if (current && finished() && !r->current.empty()) {
+        if ((int64_t)r->current.size() != 2 * n)
+            return fail(RTM_ERR_SIZE, "The request has " + std::to_string(r->current.size() / 2) + " unknowns.");
+        std::memcpy(current, r->current.data(), r->current.size() * sizeof(double));
+    }
+    if (release && finished()) srv->records.erase(it);
+    return RTM_OK;
+}
+
+int rtm_server_cancel(rtm_server* srv, uint64_t id) {
+    if (!srv) return fail(RTM_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->records.find(id);
+    if (it == srv->records.end()) return fail(RTM_ERR_ARG, "unknown request " + std::to_string(id));
+    Record* r = it->second.get();
+    r->cancel = 1;
+    if (r->res.state == RTM_REQUEST_QUEUED) {
+        for (auto q = srv->queue.begin(); q != srv->queue.end(); ++q)
+            if (*q == id) {
+                srv->queue.erase(q);
+                r->res.state = RTM_REQUEST_CANCELLED;
+                r->res.finished_s = seconds_since(srv->epoch);
+                srv->done_cv.notify_all();
+                break;
+            }
+    }
+    return RTM_OK;
+}
+
+int rtm_server_destroy(rtm_server* srv) {
+    if (!srv) return RTM_OK;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stopping = true;
+        for (uint64_t id : srv->queue) {
+            Record& r = *srv->records.at(id);
+            r.res.state = RTM_REQUEST_CANCELLED;
+            r.res.finished_s = seconds_since(srv->epoch);
+        }
+        srv->queue.clear();
+        for (auto& kv : srv->records) kv.second->cancel = 1;
+    }
+    srv->work_cv.notify_all();
+    for (auto& t : srv->workers) t.join();
+    delete srv;
+    return RTM_OK;
+}
+
+}  // extern "C"

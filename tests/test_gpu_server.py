@@ -1,0 +1,125 @@
+"""The serving form on the GPU: each request's result is the same alone and in a mix of other requests
+running at the same time, equals the direct API solve of the same plate, requests overlap on the device,
+the byte budget serialises what does not fit together, queued requests can be cancelled, and the
+mixed-precision server stays within 1e-5 of the FP64 currents."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LAM = 1.0
+K = 2 * math.pi / LAM
+TOL = 1e-8
+
+
+def _plate(cx, cy, d=(0.5, 0.0, -math.sqrt(0.75)), p=(0.0, 1.0, 0.0), **kw):
+    import rooftop_mom_b200 as R
+
+    return R.Request.planeWave(cx, cy, LAM / 20, LAM / 20, K, direction=d, polarization=p, tolerance=TOL,
+                               keepCurrent=True, **kw)
+
+
+def _strip(cx, **kw):
+    import rooftop_mom_b200 as R
+
+    return R.Request.deltaGap(cx, 1, LAM / 20, LAM / 20, K, portDirection="x", tolerance=TOL, keepCurrent=True,
+                              **kw)
+
+
+def _mix():
+    return [_plate(32, 28), _strip(41), _plate(17, 29, method="cg"), _plate(48, 40), _strip(64, method="cg"),
+            _plate(20, 20, blockJacobi=False), _plate(36, 12)]
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_results_are_the_same_alone_and_in_the_mix():
+    import rooftop_mom_b200 as R
+
+    with R.Server(maxActive=4) as srv:
+        alone = [srv.wait(srv.submit(q)) for q in (_plate(24, 20), _strip(33))]
+        mix = _mix()
+        ids = [srv.submit(q) for q in mix[:3]]
+        again = [srv.submit(_plate(24, 20))]
+        ids += [srv.submit(q) for q in mix[3:]]
+        again.append(srv.submit(_strip(33)))
+        together = [srv.wait(r) for r in again]
+        others = [srv.wait(r) for r in ids]
+    for a, b in zip(alone, together):
+        assert a["state"] == b["state"] == "done"
+        assert a["converged"] and b["converged"]
+        assert a["iterations"] == b["iterations"]
+        assert _rel(b["current"], a["current"]) < 1e-12
+        assert a["rcs"] == pytest.approx(b["rcs"], rel=1e-12)
+        assert abs(a["impedance"] - b["impedance"]) <= 1e-12 * max(1.0, abs(a["impedance"]))
+    assert all(o["state"] == "done" and o["converged"] and o["residual"] <= TOL for o in others)
+
+
+def test_served_plate_equals_the_direct_solve():
+    import rooftop_mom_b200 as R
+
+    d, p = (0.5, 0.0, -math.sqrt(0.75)), (0.0, 1.0, 0.0)
+    with R.Server(maxActive=2) as srv:
+        served = srv.wait(srv.submit(_plate(30, 26, d=d, p=p)))
+    prob = R.Problem(R.Mesh(30, 26, LAM / 20, LAM / 20), K)
+    op = R.Operator(prob)
+    pc = R.Preconditioner.blockJacobi(prob)
+    exc = R.Excitation.planeWave(prob, direction=d, polarization=p)
+    res = R.Solver(method="gmres", tolerance=TOL, restart=50, maxIterationCount=10000, side="right").solve(
+        op, exc, preconditioner=pc)
+    assert served["iterations"] == res.iterationCount()
+    assert _rel(served["current"], res.solution()) < 1e-12
+    assert served["rcs"] == pytest.approx(res.radarCrossSection(), rel=1e-10)
+
+
+def test_admitted_requests_overlap_on_the_device():
+    import rooftop_mom_b200 as R
+
+    with R.Server(maxActive=4) as srv:
+        ids = [srv.submit(_plate(40, 40)) for _ in range(6)]
+        res = [srv.wait(r) for r in ids]
+    spans = sorted((r["started"], r["finished"]) for r in res)
+    overlaps = sum(1 for a, b in zip(spans, spans[1:]) if b[0] < a[1])
+    assert overlaps >= 1
+
+
+def test_the_budget_serialises_requests_that_do_not_fit_together():
+    import rooftop_mom_b200 as R
+
+    with R.Server(budgetBytes=1e9, maxActive=8) as srv:
+        probe = srv.poll(srv.submit(_plate(48, 48)), wait=math.inf)["bytes"]
+    with R.Server(budgetBytes=1.5 * probe, maxActive=8) as srv:
+        res = [srv.wait(r) for r in [srv.submit(_plate(48, 48)) for _ in range(3)]]
+    spans = sorted((r["started"], r["finished"]) for r in res)
+    assert all(b[0] >= a[1] for a, b in zip(spans, spans[1:]))
+    assert all(r["state"] == "done" for r in res)
+
+
+def test_queued_requests_can_be_cancelled():
+    import rooftop_mom_b200 as R
+
+    with R.Server(maxActive=1) as srv:
+        ids = [srv.submit(_plate(40, 36)) for _ in range(4)]
+        srv.cancel(ids[-1])
+        res = [srv.wait(r) for r in ids]
+    assert res[-1]["state"] == "cancelled"
+    assert all(r["state"] == "done" for r in res[:-1])
+
+
+def test_mixed_precision_server_stays_close_to_fp64():
+    import rooftop_mom_b200 as R
+
+    qs = [_plate(32, 28), _strip(41)]
+    with R.Server(maxActive=2) as srv:
+        ref = [srv.wait(srv.submit(q)) for q in qs]
+    with R.Server(maxActive=2, precision="single") as srv:
+        mixed = [srv.wait(srv.submit(q)) for q in qs]
+    for a, b in zip(ref, mixed):
+        assert b["state"] == "done" and b["converged"] and b["residual"] <= TOL
+        assert _rel(b["current"], a["current"]) < 1e-5
