@@ -1,6 +1,6 @@
 """Benchmark of the rooftop-mom solve path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|c3|c4|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c1|c2|c3|c4|c5]
 
 A step is one complete plate solve of the workload: generator assembly, spectra, preconditioner,
 plane-wave excitation, the iterative solve to the workload's tolerance (the FP64 true residual is
@@ -39,7 +39,195 @@ WORKLOADS = {
                pc="blockJacobi", precision="double"),
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
                pc=None, precision="mixed"),
+    # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32 COCG
+    # with a FP32 block-Jacobi preconditioner inside FP64 iterative refinement
+    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=50, pc="blockJacobi",
+               precision="mixed", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
+    # request stream of plate solves (see serving_requests)
+    "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
+               theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
 }
+
+SPEED_OF_LIGHT = 299792458.0
+
+
+def random_waves(count, rng):
+    """Directions and polarisations of `count` plane waves: theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE or
+    TM with probability 1/2 each."""
+    dirs, pols = [], []
+    for _ in range(count):
+        t, p = rng.uniform(0.0, 80.0), rng.uniform(0.0, 360.0)
+        d, e = plane_wave_vectors(t, p, "TE" if rng.random() < 0.5 else "TM")
+        dirs.append(d)
+        pols.append(e)
+    return np.array(dirs), np.array(pols)
+
+
+def batch_rhs(R, prob, dirs, pols):
+    """The plane waves of dirs / pols as one device tensor of nrhs * N complex doubles (rtm_plane_wave)."""
+    import ctypes as C
+
+    import torch
+    from rooftop_mom_b200 import _lib as L
+
+    cx, cy = prob.mesh().count()
+    a, b = prob.mesh().faceSize()
+    nrhs, n = len(dirs), prob.rooftopCount()
+    out = torch.empty(nrhs * n, dtype=torch.complex128, device="cuda")
+    d = np.ascontiguousarray(dirs, dtype=np.float64)
+    p = np.ascontiguousarray(pols, dtype=np.float64)
+    inten = np.ones(nrhs)
+    L.call("rtm_plane_wave", cx, cy, a, b, prob.quadratureOrder()[1], prob.wavenumber(),
+           d.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p), inten.ctypes.data_as(C.c_void_p), nrhs,
+           C.c_void_p(out.data_ptr()), L.DEVICE, None)
+    return out
+
+
+def solve_batch(R, w, b=None):
+    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 COCG solve."""
+    prob = build_plate(R, w)
+    dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
+    op = R.Operator(prob, maxRhs=w["rhs"])
+    inner = R.Operator(prob, precision="single", maxRhs=w["rhs"])
+    pc = R.Preconditioner.blockJacobi(prob, (2, 2), precision="single")
+    if b is None:
+        b = batch_rhs(R, prob, dirs, pols)
+    res = R.Solver(method="fgmres", innerMethod="cg", tolerance=w["tol"], innerTolerance=1e-4,
+                   maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc, nrhs=w["rhs"])
+    return prob, res
+
+
+def serving_requests(R, count, seed):
+    """The c5 request stream: faces Nx (and Ny) log-uniform in [16, 768]; with probability 1/2 a strip one
+    face wide fed by a 1 V delta gap at its middle, else a plate under a random plane wave; cell lambda/N
+    with N ~ U[10, 25]; frequency ~ U[0.5, 3] GHz; GMRES(50) with block-Jacobi to 1e-6."""
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(16), math.log(768)
+    out = []
+    for _ in range(count):
+        nx = int(round(math.exp(rng.uniform(lo, hi))))
+        strip = rng.random() < 0.5
+        ny = 1 if strip else int(round(math.exp(rng.uniform(lo, hi))))
+        cells = rng.uniform(10.0, 25.0)
+        f = rng.uniform(0.5e9, 3e9)
+        h = SPEED_OF_LIGHT / f / cells
+        k = 2 * math.pi * f / SPEED_OF_LIGHT
+        kw = dict(method="gmres", blockJacobi=True, tolerance=1e-6, restart=50, maxIterationCount=20000)
+        if strip:
+            out.append(R.Request.deltaGap(nx, 1, h, h, k, portDirection="x", voltage=1.0, **kw))
+        else:
+            d, p = random_waves(1, rng)
+            out.append(R.Request.planeWave(nx, ny, h, h, k, direction=d[0], polarization=p[0], **kw))
+    return out
+
+
+def run_serving(args):
+    """c5: a closed-loop burst measures capacity; then the stream arrives as a Poisson process at 0.8 x
+    capacity; per-request latency (submission to result) gives p50 / p99."""
+    import torch
+
+    import rooftop_mom_b200 as R
+
+    R.load()
+    reqs = serving_requests(R, args.requests, 0)
+    prec = "single" if args.serving_precision == "mixed" else "double"
+    with R.Server(budgetBytes=150e9, maxActive=args.slots, precision=prec) as srv:
+        warm = serving_requests(R, 4, 1)
+        for r in [srv.submit(q) for q in warm]:
+            srv.wait(r, release=True)
+        burst = reqs[: min(len(reqs), args.slots * 4)]
+        ids = [srv.submit(q) for q in burst]
+        res = [srv.wait(r, release=True) for r in ids]
+        span = max(x["finished"] for x in res) - min(x["submitted"] for x in res)
+        capacity = len(burst) / span
+        rate = 0.8 * capacity
+        rng = np.random.default_rng(2)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        torch.cuda.synchronize()
+        with Clocks(0) as clk:
+            t0 = time.perf_counter()
+            ids = []
+            for q, ta in zip(reqs, arrivals):
+                dt = ta - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(q))
+            res = [srv.wait(r, release=True) for r in ids]
+    done = [x for x in res if x["state"] == "done"]
+    lat = np.array([x["latency"] for x in done])
+    span = max(x["finished"] for x in res) - min(x["submitted"] for x in res)
+    ok = [x for x in done if x["converged"] and x["residual"] <= 1e-6]
+    line = {
+        "metric": "serving: solves/s and p50/p99 latency of a Poisson request stream at 0.8 x measured capacity",
+        "value": len(ok) / span, "unit": "solves/s", "n_gpus": 1, "steps": len(reqs), "warmup": len(warm),
+        "ms_per_step": span / len(reqs) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128" if prec == "double" else "c64/c128", "data": "synthetic request stream, seed 0",
+        "config": {"workload": f"c5: {len(reqs)} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
+                               f"cell lambda/U[10,25], f U[0.5,3] GHz, GMRES(50) + block-Jacobi to 1e-6, "
+                               f"{args.serving_precision}", "slots": args.slots, "budget_bytes": 150e9,
+                   "capacity_solves_per_s": capacity, "arrival_rate": rate},
+        "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "converged": len(ok), "failed": len(res) - len(done),
+        "max_unknowns": int(max(x["unknowns"] for x in res)),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+def run_batched(args, w):
+    """c4: K batched solves of 64 right-hand sides; value = right-hand sides solved per second."""
+    import torch
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    R.load()
+    for _ in range(args.warmup):
+        solve_batch(R, w)
+    torch.cuda.synchronize()
+    launches0 = L.launch_count()
+    its, res_max = [], 0.0
+    with Clocks(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            prob, res = solve_batch(R, w)
+            its.append(max(r.iterationCount() for r in res))
+            res_max = max(res_max, max(r.residualNorm() for r in res))
+        e1.record()
+        torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    # e2e: the right-hand sides from pinned host memory, the currents back to it
+    prob = build_plate(R, w)
+    dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
+    host = batch_rhs(R, prob, dirs, pols).cpu().pin_memory()
+    out = torch.empty_like(host).pin_memory()
+    torch.cuda.synchronize()
+    e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e2[0].record()
+    for _ in range(args.steps):
+        b = host.to("cuda", non_blocking=True)
+        _, res = solve_batch(R, w, b=b)
+        out.copy_(torch.cat([r.solution() for r in res]), non_blocking=True)
+    e2[1].record()
+    torch.cuda.synchronize()
+    t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
+    n, N = w["n"], prob.rooftopCount()
+    line = {
+        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 COCG inside FP64 refinement",
+        "value": w["rhs"] * args.steps / t, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64/c128", "data": "synthetic plate and 64 plane waves, seed 0",
+        "config": {"workload": f"c4: {n}x{n} plate, cell lambda/{w['density']}, {N} unknowns, {w['rhs']} plane "
+                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 block-Jacobi inside FP64 "
+                               f"refinement to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
+                   "l2": "working set per batch re-created every step"},
+        "iterations": its[0], "true_residual": res_max, "all_converged_to_tolerance": res_max <= w["tol"],
+        "e2e": {"value": w["rhs"] * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 16 * N * w["rhs"],
+                "d2h_bytes_per_step": 16 * N * w["rhs"]},
+        "gpu_launches": int(L.launch_count() - launches0), "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
 
 
 def plane_wave_vectors(theta_deg, phi_deg, pol):
@@ -265,8 +453,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--once", action="store_true",
                     help="one untimed solve of the workload, no JSON line (the command profiler captures run)")
+    ap.add_argument("--requests", type=int, default=100, help="c5: requests in the stream (2000 in the full form)")
+    ap.add_argument("--slots", type=int, default=8, help="c5: requests on the device at once")
+    ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if args.workload in ("c4", "c5"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": f"the CPU oracle arm times single-plate solves "
+                                                                  f"(c1, c2, c3), not {args.workload}"}))
+        elif int(os.environ.get("RANK", "0")) == 0:
+            run_serving(args) if args.workload == "c5" else run_batched(args, w)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
