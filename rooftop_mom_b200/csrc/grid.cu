@@ -509,14 +509,14 @@ int apply_fixed_scratch(const GridApplicator& g, const void* x, void* y, int nrh
 
 // ============================================================================================
 // Spectra builders: 2-D DFTs (P x Q) of generated inputs, in FP64.
-enum SourceKind { kSrcEmbed = 0, kSrcCirculant = 1 };
+enum SourceKind { kSrcEmbed = 0, kSrcCirculant = 1, kSrcTwoSided = 2, kSrcPart = 3 };
 enum Window { kWinStrang = 0, kWinTChan = 1, kWinRChan = 2, kWinHuckle = 3 };
 constexpr int kMaxItems = 12;
 
 struct GenItem {
-    const double2* g;  // generator, column-major rows x cols
+    const double2* g;  // generator, column-major rows x cols (two-sided sources: (2P - 1) x (2Q - 1))
     int rows, cols;
-    int px, py;
+    int px, py;        // subband parities; part (m, n) of kSrcPart
     double2* dst;      // P x Q output (column-major, x fastest)
 };
 
@@ -573,6 +573,30 @@ __device__ double2 gen_value(const GenArgs& a, const GenItem& it, int i, int j) 
         double2 v = make_double2(re * a.scale, im * a.scale);
         if (it.px) v = cmul(v, a.modP[i]);
         if (it.py) v = cmul(v, a.modQ[j]);
+        return v;
+    }
+    if (a.kind == kSrcTwoSided || a.kind == kSrcPart) {
+        // A two-sided source, offsets -(P-1)..P-1 by -(Q-1)..Q-1. kSrcTwoSided: the windowed fold onto the
+        // face grid (foldGenerator.m:47-60). kSrcPart: part (m, n) of generatePartSpectra.m:15-49, the
+        // halved sum (m = 0) or difference (m = 1) of the offsets i and i - P, likewise along y, times
+        // exp(i pi i / P) for m = 1 and exp(i pi j / Q) for n = 1.
+        const bool part = a.kind == kSrcPart;
+        for (int ca = 0; ca < 2; ++ca) {
+            if (ca == 1 && i == 0) continue;
+            const int ox = ca ? i - a.P : i;
+            const double wa = part ? ((it.px && ca) ? -0.5 : 0.5) : window_weight(a.window, ox, a.P, a.bw_x);
+            for (int cb = 0; cb < 2; ++cb) {
+                if (cb == 1 && j == 0) continue;
+                const int oy = cb ? j - a.Q : j;
+                const double wb = part ? ((it.py && cb) ? -0.5 : 0.5) : window_weight(a.window, oy, a.Q, a.bw_y);
+                const double2 g = it.g[(ox + a.P - 1) + (int64_t)(oy + a.Q - 1) * it.rows];
+                re += wa * wb * g.x;
+                im += wa * wb * g.y;
+            }
+        }
+        double2 v = make_double2(re, im);
+        if (part && it.px) v = cmulc(v, a.modP[i]);
+        if (part && it.py) v = cmulc(v, a.modQ[j]);
         return v;
     }
     // Circulant fold of the even generator onto the face grid (foldGenerator.m:38-45).
@@ -878,11 +902,303 @@ int build_product(const DeviceGenerators& g, double size_x, double size_y, int p
     return RTM_OK;
 }
 
+// --------------------------------------------------------------------------------------------
+// Superoptimal kernel and the blockwise / hybrid builders (generateSuperoptimal.m:14-25,
+// generateOptimalOfProduct.m:18-62, generateSpatialBlocks.m:19-61, generateBlockwiseSpectra.m:17-33,
+// generateHybridSpectra.m:16-26). Sources are two-sided arrays of (2P - 1) x (2Q - 1) offsets on the
+// P x Q face grid; everything runs in FP64 at set-up.
+
+// Two-sided even extension of a generator padded to P x Q (extendEvenly.m:12-13 of the padded array).
+__global__ void k_two_sided_even(int P, int Q, const double2* __restrict__ g, int rows, int cols,
+                                 double2* __restrict__ out) {
+    const int64_t W = 2 * P - 1, n = W * (2 * Q - 1);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int ox = abs((int)(t % W) - (P - 1)), oy = abs((int)(t / W) - (Q - 1));
+        out[t] = (ox < rows && oy < cols) ? g[ox + (int64_t)oy * rows] : make_double2(0, 0);
+    }
+}
+
+// Spatial blocks of the Green's matrix by offset between first faces (generateSpatialBlocks.m:19-61):
+// XX = MXX - (2E - E(-1,0) - E(1,0)) / a^2, YY likewise along y, XY = -(E - E(0,-1) - E(1,0) + E(1,-1)) / ab,
+// with E evenly extended and zero outside the offsets, and the offsets no rooftop pair has set to zero.
+__global__ void k_spatial_blocks(int P, int Q, const double2* __restrict__ E, const double2* __restrict__ mxx,
+                                 const double2* __restrict__ myy, double inv_a2, double inv_b2, double inv_ab,
+                                 double2* __restrict__ bxx, double2* __restrict__ bxy, double2* __restrict__ byy) {
+    const int64_t W = 2 * P - 1, n = W * (2 * Q - 1);
+    auto e2 = [&](int ox, int oy) -> double2 {
+        if (ox < -(P - 1) || ox > P - 1 || oy < -(Q - 1) || oy > Q - 1) return make_double2(0, 0);
+        return E[abs(ox) + (int64_t)abs(oy) * P];
+    };
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int ox = (int)(t % W) - (P - 1), oy = (int)(t / W) - (Q - 1);
+        const double2 c = e2(ox, oy);
+        if (bxx) {
+            double2 v = make_double2(0, 0);
+            if (abs(ox) <= P - 2) {
+                const double2 l = e2(ox - 1, oy), r = e2(ox + 1, oy);
+                const double2 m = abs(ox) < P - 1 ? mxx[abs(ox) + (int64_t)abs(oy) * (P - 1)] : make_double2(0, 0);
+                v = make_double2(m.x - (2 * c.x - l.x - r.x) * inv_a2, m.y - (2 * c.y - l.y - r.y) * inv_a2);
+            }
+            bxx[t] = v;
+        }
+        if (byy) {
+            double2 v = make_double2(0, 0);
+            if (abs(oy) <= Q - 2) {
+                const double2 d = e2(ox, oy - 1), u = e2(ox, oy + 1);
+                const double2 m = abs(oy) < Q - 1 ? myy[abs(ox) + (int64_t)abs(oy) * P] : make_double2(0, 0);
+                v = make_double2(m.x - (2 * c.x - d.x - u.x) * inv_b2, m.y - (2 * c.y - d.y - u.y) * inv_b2);
+            }
+            byy[t] = v;
+        }
+        if (bxy) {
+            double2 v = make_double2(0, 0);
+            if (ox <= P - 2 && oy >= -(Q - 2)) {
+                const double2 a1 = e2(ox, oy - 1), a2 = e2(ox + 1, oy), a3 = e2(ox + 1, oy - 1);
+                v = make_double2(-(c.x - a1.x - a2.x + a3.x) * inv_ab, -(c.y - a1.y - a2.y + a3.y) * inv_ab);
+            }
+            bxy[t] = v;
+        }
+    }
+}
+
+// Circular convolution along x (dim 0) or y (dim 1) of a P x Q array in place:
+// ifft(K fft(values)) with K the kernel's spectrum (generateOptimalOfProduct.m:52-62). One CTA per line
+// along x; TI lines per CTA along y.
+__global__ void __launch_bounds__(kMaxThreads, 1) k_line_conv_x(int P, int Q, FftPlan plan, const double2* tw,
+                                                                const double2* __restrict__ K, double2* v) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    double2* line = v + (int64_t)blockIdx.x * P;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) A[sk(i)] = line[i];
+    __syncthreads();
+    fft_inplace<false, false>(A, 1, P, 1, plan, tw);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) A[sk(i)] = cmul(A[sk(i)], K[i]);
+    __syncthreads();
+    fft_inplace<true, false>(A, 1, P, 1, plan, tw);
+    const double sc = 1.0 / P;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) line[i] = cscale(A[sk(i)], sc);
+}
+
+__global__ void __launch_bounds__(kMaxThreads, 1) k_line_conv_y(int P, int Q, int TI, FftPlan plan, const double2* tw,
+                                                                const double2* __restrict__ K, double2* v) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    const int i0 = blockIdx.x * TI;
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        A[sk(j) * TI + l] = i < P ? v[(int64_t)j * P + i] : make_double2(0, 0);
+    }
+    __syncthreads();
+    fft_inplace<false, false>(A, TI, 1, TI, plan, tw);
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI;
+        A[sk(j) * TI + l] = cmul(A[sk(j) * TI + l], K[j]);
+    }
+    __syncthreads();
+    fft_inplace<true, false>(A, TI, 1, TI, plan, tw);
+    const double sc = 1.0 / Q;
+    for (int it = threadIdx.x; it < TI * Q; it += blockDim.x) {
+        const int l = it % TI, j = it / TI, i = i0 + l;
+        if (i < P) v[(int64_t)j * P + i] = cscale(A[sk(j) * TI + l], sc);
+    }
+}
+
+// op 0: out = a conj(b); op 1: out += a; op 2: out = a / conj(b).
+__global__ void k_spectra_arith(int op, int64_t n, const double2* __restrict__ a, const double2* __restrict__ b,
+                                double2* __restrict__ out) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        if (op == 0) {
+            out[t] = cmulc(a[t], b[t]);
+        } else if (op == 1) {
+            out[t] = cadd(out[t], a[t]);
+        } else {
+            const double2 d = cconj(b[t]);
+            const double m = d.x * d.x + d.y * d.y;
+            const double2 q = cmulc(a[t], d);
+            out[t] = make_double2(q.x / m, q.y / m);
+        }
+    }
+}
+
+// Explicit 2x2 blocks and their inverse per frequency (Spectra.invert, invert.m:12-20). XX, YY given;
+// mode 0 (blockwise): XY given, YX(i, j) = XY(-i, -j); mode 1 (hybrid): XY = qc E, YX = conj(qc) E with
+// qc = -(1 - s_x) conj(1 - s_y) / ab (generateBlockSpectra.m:43-47). Flags any non-finite value.
+__global__ void k_blocks_invert(int P, int Q, int content, int mode, const double2* __restrict__ xx,
+                                const double2* __restrict__ xy, const double2* __restrict__ yy,
+                                const double2* __restrict__ u, const double2* __restrict__ v, double inv_ab,
+                                double2* __restrict__ out, int* __restrict__ bad) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t G = (int64_t)P * Q;
+    if (idx >= G) return;
+    const int i = (int)(idx % P), j = (int)(idx / P);
+    double2 r[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    if (content == RTM_XONLY) {
+        const double2 XX = xx[idx];
+        const double d = XX.x * XX.x + XX.y * XX.y;
+        r[0] = make_double2(XX.x / d, -XX.y / d);
+    } else if (content == RTM_YONLY) {
+        const double2 YY = yy[idx];
+        const double d = YY.x * YY.x + YY.y * YY.y;
+        r[3] = make_double2(YY.x / d, -YY.y / d);
+    } else {
+        const double2 XX = xx[idx], YY = yy[idx];
+        double2 XY, YX;
+        if (mode == 0) {
+            XY = xy[idx];
+            YX = xy[(i ? P - i : 0) + (int64_t)(j ? Q - j : 0) * P];
+        } else {
+            const double2 E = xy[idx];
+            double2 qc = cmulc(u[i], v[j]);
+            qc.x = -qc.x * inv_ab;
+            qc.y = -qc.y * inv_ab;
+            XY = cmul(qc, E);
+            YX = cmul(cconj(qc), E);
+        }
+        const double2 det = csub(cmul(XX, YY), cmul(XY, YX));
+        const double dd = det.x * det.x + det.y * det.y;
+        const double2 inv = make_double2(det.x / dd, -det.y / dd);
+        r[0] = cmul(YY, inv);
+        r[1] = cmul(make_double2(-XY.x, -XY.y), inv);
+        r[2] = cmul(make_double2(-YX.x, -YX.y), inv);
+        r[3] = cmul(XX, inv);
+    }
+    for (int b = 0; b < 4; ++b) {
+        if (!isfinite(r[b].x) || !isfinite(r[b].y)) atomicExch(bad, 1);
+        out[b * G + idx] = r[b];
+    }
+}
+
+// Spectrum of 1 / (n^2 sin^2(pi (2d + 1) / (2n))), d < n (generateOptimalOfProduct.m:52-55), by a direct
+// DFT in long double on the host.
+static std::vector<double2> convolution_kernel(int n) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<long double> k(n);
+    for (int d = 0; d < n; ++d) {
+        const long double sn = sinl(pi * (2 * d + 1) / (2.0L * n));
+        k[d] = 1.0L / ((long double)n * n * sn * sn);
+    }
+    std::vector<double2> out(n);
+    for (int f = 0; f < n; ++f) {
+        long double re = 0, im = 0;
+        for (int d = 0; d < n; ++d) {
+            const long double ang = -2 * pi * (long double)(((int64_t)f * d) % n) / n;
+            re += k[d] * cosl(ang);
+            im += k[d] * sinl(ang);
+        }
+        out[f] = make_double2((double)re, (double)im);
+    }
+    return out;
+}
+
+struct TwoSidedSpectra {
+    int P, Q;
+    int window;
+    int bw_x, bw_y;
+    const FftTables* tP;
+    const FftTables* tQ;
+};
+
+static int line_conv(const TwoSidedSpectra& t, int dim, const double2* K, double2* v, cudaStream_t s) {
+    static bool attrs = false;
+    if (!attrs) {
+        cudaFuncSetAttribute(k_line_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_line_conv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attrs = true;
+    }
+    if (dim == 0) {
+        const size_t smem = (size_t)(sk(t.P - 1) + 1) * sizeof(double2);
+        const int thr = fft_threads(1, t.tP->plan);
+        if (smem > (size_t)kSmemBudget || thr > kMaxThreads) return fail(RTM_ERR_UNSUPPORTED, "grid too large");
+        k_line_conv_x<<<t.Q, thr, smem, s>>>(t.P, t.Q, t.tP->plan, t.tP->tw64, K, v);
+    } else {
+        int ti = 4;
+        while (ti > 1 && ((size_t)ti * (sk(t.Q - 1) + 1) * sizeof(double2) > (size_t)kSmemBudget ||
+                          fft_threads(ti, t.tQ->plan) > kMaxThreads))
+            ti /= 2;
+        const size_t smem = (size_t)ti * (sk(t.Q - 1) + 1) * sizeof(double2);
+        const int thr = fft_threads(ti, t.tQ->plan);
+        if (smem > (size_t)kSmemBudget || thr > kMaxThreads) return fail(RTM_ERR_UNSUPPORTED, "grid too large");
+        k_line_conv_y<<<(t.P + ti - 1) / ti, thr, smem, s>>>(t.P, t.Q, ti, t.tQ->plan, t.tQ->tw64, K, v);
+    }
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
+static int run_two_sided(const TwoSidedSpectra& t, int kind, int window, const double2* src, int px, int py,
+                         double2* dst, cudaStream_t s) {
+    GenArgs a{};
+    a.kind = kind;
+    a.P = t.P;
+    a.Q = t.Q;
+    a.window = window;
+    a.bw_x = t.bw_x;
+    a.bw_y = t.bw_y;
+    a.planP = t.tP->plan;
+    a.planQ = t.tQ->plan;
+    a.twP = t.tP->tw64;
+    a.twQ = t.tQ->tw64;
+    a.modP = t.tP->mod64;
+    a.modQ = t.tQ->mod64;
+    GenItem& it = a.items[a.nitems++];
+    it.g = src;
+    it.rows = 2 * t.P - 1;
+    it.cols = 2 * t.Q - 1;
+    it.px = px;
+    it.py = py;
+    it.dst = dst;
+    return run_gen(a, s);
+}
+
+// Spectrum (P x Q) of the kernel applied to a two-sided source: the windowed fold for strang, tChan,
+// rChan and huckle; for superoptimal c(T T^H) / conj(c(T)) with c the T. Chan approximation.
+static int two_sided_spectrum(const TwoSidedSpectra& t, int kernel, const double2* src, double2* dst, cudaStream_t s) {
+    if (kernel != RTM_KERNEL_SUPEROPTIMAL) return run_two_sided(t, kSrcTwoSided, t.window, src, 0, 0, dst, s);
+    const int64_t G = (int64_t)t.P * t.Q;
+    DeviceBuffer parts, tmp, kx, ky;
+    StreamSyncGuard guard(s);
+    RTM_TRY(parts.alloc(4 * (size_t)G * sizeof(double2)));  // part (m, n) at m + 2 n
+    RTM_TRY(tmp.alloc(4 * (size_t)G * sizeof(double2)));    // va, vb, product, T. Chan spectrum
+    double2* P4 = parts.as<double2>();
+    double2* va = tmp.as<double2>();
+    double2* vb = va + G;
+    double2* pr = vb + G;
+    double2* opt = pr + G;
+    for (int q = 0; q < 4; ++q) RTM_TRY(run_two_sided(t, kSrcPart, 0, src, q & 1, q >> 1, P4 + q * G, s));
+    RTM_TRY(run_two_sided(t, kSrcTwoSided, kWinTChan, src, 0, 0, opt, s));
+    const std::vector<double2> hx = convolution_kernel(t.P), hy = convolution_kernel(t.Q);
+    RTM_TRY(kx.alloc(hx.size() * sizeof(double2)));
+    RTM_TRY(ky.alloc(hy.size() * sizeof(double2)));
+    RTM_CUDA(cudaMemcpyAsync(kx.ptr, hx.data(), kx.bytes, cudaMemcpyHostToDevice, s));
+    RTM_CUDA(cudaMemcpyAsync(ky.ptr, hy.data(), ky.bytes, cudaMemcpyHostToDevice, s));
+    const double2* K[2] = {kx.as<double2>(), ky.as<double2>()};
+    RTM_CUDA(cudaMemsetAsync(dst, 0, (size_t)G * sizeof(double2), s));
+    const unsigned blocks = (unsigned)std::min<int64_t>((G + 255) / 256, 1184);
+    // generateOptimalOfProduct.m:34-49: sum over the part types of a and b
+    for (int ta = 0; ta < 4; ++ta)
+        for (int tb = 0; tb < 4; ++tb) {
+            const int a2[2] = {ta & 1, ta >> 1}, b2[2] = {tb & 1, tb >> 1};
+            RTM_CUDA(cudaMemcpyAsync(va, P4 + ta * G, G * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+            RTM_CUDA(cudaMemcpyAsync(vb, P4 + tb * G, G * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+            for (int d = 0; d < 2; ++d)
+                if (a2[d] == 1 && b2[d] == 0) RTM_TRY(line_conv(t, d, K[d], va, s));
+            for (int d = 0; d < 2; ++d)
+                if (a2[d] == 0 && b2[d] == 1) RTM_TRY(line_conv(t, d, K[d], vb, s));
+            k_spectra_arith<<<blocks, 256, 0, s>>>(0, G, va, vb, pr);
+            count_launch();
+            for (int d = 0; d < 2; ++d)
+                if (a2[d] == 1 && b2[d] == 1) RTM_TRY(line_conv(t, d, K[d], pr, s));
+            k_spectra_arith<<<blocks, 256, 0, s>>>(1, G, pr, nullptr, dst);
+            count_launch();
+        }
+    k_spectra_arith<<<blocks, 256, 0, s>>>(2, G, dst, opt, dst);
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
 int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int kernel, int builder,
                     const int* bandwidth, int precision, GridApplicator& out, cudaStream_t s) {
-    if (builder != RTM_BUILDER_PARTWISE || kernel == RTM_KERNEL_SUPEROPTIMAL)
-        return fail(RTM_ERR_UNSUPPORTED, "only the partwise builder with the strang, tChan, rChan and huckle kernels "
-                                         "is built on the device in this version");
     const int cx = g.count_x, cy = g.count_y;
     layout(out, cx, cy);
     out.precision = precision;
@@ -912,19 +1228,6 @@ int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int
     StreamSyncGuard guard(s);
     RTM_TRY(raw.alloc(3 * (size_t)G * sizeof(double2)));
     RTM_CUDA(cudaMemsetAsync(raw.ptr, 0, raw.bytes, s));
-    const double2* gens[3] = {g.e.as<double2>(), g.xx.as<double2>(), g.yy.as<double2>()};
-    const int grows[3] = {cx, cx - 1, cx};
-    const int gcols[3] = {cy, cy, cy - 1};
-    for (int k = 0; k < 3; ++k) {
-        if (!gens[k]) continue;
-        GenItem& it = a.items[a.nitems++];
-        it.g = gens[k];
-        it.rows = grows[k];
-        it.cols = gcols[k];
-        it.px = it.py = 0;
-        it.dst = raw.as<double2>() + k * G;
-    }
-    RTM_TRY(run_gen(a, s));
     RTM_TRY(inv.alloc(4 * (size_t)G * sizeof(double2)));
     RTM_TRY(flag.alloc(sizeof(int)));
     RTM_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(int), s));
@@ -933,11 +1236,74 @@ int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int
     const float2* f = nullptr;
     RTM_TRY(shift_factors(cx, 0, &u, &f));
     RTM_TRY(shift_factors(cy, 0, &v, &f));
-    k_circulant_invert<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(cx, cy, out.content, raw.as<double2>(), u, v,
-                                                                   1.0 / (size_x * size_x), 1.0 / (size_y * size_y),
-                                                                   1.0 / (size_x * size_y), inv.as<double2>(),
-                                                                   flag.as<int>());
-    count_launch();
+    const double2* gens[3] = {g.e.as<double2>(), g.xx.as<double2>(), g.yy.as<double2>()};
+    const int grows[3] = {cx, cx - 1, cx};
+    const int gcols[3] = {cy, cy, cy - 1};
+    if (builder == RTM_BUILDER_PARTWISE && kernel != RTM_KERNEL_SUPEROPTIMAL) {
+        for (int k = 0; k < 3; ++k) {
+            if (!gens[k]) continue;
+            GenItem& it = a.items[a.nitems++];
+            it.g = gens[k];
+            it.rows = grows[k];
+            it.cols = gcols[k];
+            it.px = it.py = 0;
+            it.dst = raw.as<double2>() + k * G;
+        }
+        RTM_TRY(run_gen(a, s));
+    } else {
+        TwoSidedSpectra t{cx, cy, a.window, a.bw_x, a.bw_y, out.tP, out.tQ};
+        const int64_t T = (int64_t)(2 * cx - 1) * (2 * cy - 1);
+        const unsigned tb = (unsigned)std::min<int64_t>((T + 255) / 256, 1184);
+        DeviceBuffer two;
+        StreamSyncGuard two_guard(s);
+        RTM_TRY(two.alloc(3 * (size_t)T * sizeof(double2)));
+        RTM_CUDA(cudaMemsetAsync(two.ptr, 0, two.bytes, s));
+        double2* S0 = two.as<double2>();
+        if (builder == RTM_BUILDER_PARTWISE) {
+            // generatePartwiseSpectra.m:16-30 with the superoptimal kernel: E, MXX, MYY one by one
+            for (int k = 0; k < 3; ++k) {
+                if (!gens[k]) continue;
+                k_two_sided_even<<<tb, 256, 0, s>>>(cx, cy, gens[k], grows[k], gcols[k], S0);
+                count_launch();
+                RTM_TRY(two_sided_spectrum(t, kernel, S0, raw.as<double2>() + k * G, s));
+            }
+        } else {
+            const bool has_x = out.content != RTM_YONLY, has_y = out.content != RTM_XONLY;
+            double2* bxx = has_x ? S0 : nullptr;
+            double2* bxy = has_x && has_y ? S0 + T : nullptr;
+            double2* byy = has_y ? S0 + 2 * T : nullptr;
+            k_spatial_blocks<<<tb, 256, 0, s>>>(cx, cy, gens[0], gens[1], gens[2], 1.0 / (size_x * size_x),
+                                                 1.0 / (size_y * size_y), 1.0 / (size_x * size_y), bxx, bxy, byy);
+            count_launch();
+            double2* sxx = raw.as<double2>();  // reuse of raw: XX, coupling (XY or E), YY
+            double2* sxy = sxx + G;
+            double2* syy = sxy + G;
+            if (bxx) RTM_TRY(two_sided_spectrum(t, kernel, bxx, sxx, s));
+            if (byy) RTM_TRY(two_sided_spectrum(t, kernel, byy, syy, s));
+            if (bxy) {
+                if (builder == RTM_BUILDER_BLOCKWISE) {
+                    RTM_TRY(two_sided_spectrum(t, kernel, bxy, sxy, s));
+                } else {
+                    // generateHybridSpectra.m:16-26: the coupling from the electric generator alone
+                    k_two_sided_even<<<tb, 256, 0, s>>>(cx, cy, gens[0], cx, cy, bxy);
+                    count_launch();
+                    RTM_TRY(two_sided_spectrum(t, kernel, bxy, sxy, s));
+                }
+            }
+            k_blocks_invert<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(
+                cx, cy, out.content, builder == RTM_BUILDER_BLOCKWISE ? 0 : 1, sxx, sxy, syy, u, v,
+                1.0 / (size_x * size_y), inv.as<double2>(), flag.as<int>());
+            count_launch();
+        }
+        RTM_CUDA(cudaGetLastError());
+    }
+    if (builder == RTM_BUILDER_PARTWISE) {
+        k_circulant_invert<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(cx, cy, out.content, raw.as<double2>(), u, v,
+                                                                       1.0 / (size_x * size_x), 1.0 / (size_y * size_y),
+                                                                       1.0 / (size_x * size_y), inv.as<double2>(),
+                                                                       flag.as<int>());
+        count_launch();
+    }
     RTM_CUDA(cudaGetLastError());
     int bad = 0;
     RTM_CUDA(cudaMemcpyAsync(&bad, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));

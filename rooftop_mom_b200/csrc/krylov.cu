@@ -528,9 +528,161 @@ template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
     *smem = bytes(tr);
 }
 
+// --------------------------------------------------------------------------------------------
+// The same three passes, streamed from global memory with no per-tile barriers. Each CTA owns one
+// contiguous chunk of rows. The update w -= V c runs one thread per row, loading eight basis entries
+// before using them (coalesced across the warp), in the column order of k_gm_orth. The dots run one
+// warp per column: lanes stride the chunk's rows and keep the column's sum in registers until the
+// chunk ends; the chunk of w sits in shared memory. With fewer columns than warps, the rows of a
+// column are split between warps. Mode 1 reads the basis twice (the second read mostly from L2).
+// Serves bases of up to kStreamCols columns.
+constexpr int kStreamCols = 64;
+constexpr int kStreamRows = 3072;  // rows per CTA chunk the launcher aims at (bounds the shared w chunk)
+
+template <typename T2>
+__global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict__ V, T2* __restrict__ w, int64_t n,
+                                                           int nrhs, GmState* st, GmArrays ar, int mode, int chunk) {
+    constexpr int NW = kRT / 32, KQ = kStreamCols / NW;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double2 coef[kStreamCols];
+    __shared__ double2 red[NW][KQ];
+    T2* ws = reinterpret_cast<T2*>(smem_raw);  // [chunk]
+    const int rhs = blockIdx.y;
+    GmState& S = st[rhs];
+    if (!S.active) return;
+    const int cols = S.step + 1;
+    const int mc = ar.m + 1;
+    const int64_t c0 = (int64_t)blockIdx.x * chunk < n ? (int64_t)blockIdx.x * chunk : n;
+    const int len = (int)(n - c0 < (int64_t)chunk ? n - c0 : (int64_t)chunk);
+    const double2* cf = mode == 1 ? ar.h + (int64_t)rhs * mc : ar.c + (int64_t)rhs * mc;
+    for (int k = threadIdx.x; k < cols; k += kRT) coef[k] = mode ? cf[k] : make_double2(0, 0);
+    T2* wr = w + (int64_t)rhs * n + c0;
+    const T2* Vr = V + (int64_t)rhs * n + c0;        // column k at Vr + k * col
+    const int64_t col = (int64_t)nrhs * n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double nrm = 0;
+    __syncthreads();  // coef
+    if (mode) {
+        for (int r = threadIdx.x; r < len; r += kRT) {
+            double2 v = to_d2(wr[r]);
+            int k = 0;
+            for (; k + 8 <= cols; k += 8) {
+                T2 t[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) t[u] = Vr[(k + u) * col + r];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const double2 p = dmul(to_d2(t[u]), coef[k + u]);
+                    v.x -= p.x;
+                    v.y -= p.y;
+                }
+            }
+            for (; k < cols; ++k) {
+                const double2 p = dmul(to_d2(Vr[k * col + r]), coef[k]);
+                v.x -= p.x;
+                v.y -= p.y;
+            }
+            const T2 vs = from_d2<T2>(v);
+            wr[r] = vs;
+            if (mode == 1) ws[r] = vs;
+            const double2 vd = to_d2(vs);
+            nrm += vd.x * vd.x + vd.y * vd.y;
+        }
+    } else {
+        for (int r = threadIdx.x; r < len; r += kRT) ws[r] = wr[r];
+    }
+    double2* part = ar.part + (int64_t)rhs * gridDim.x * mc;
+    if (mode < 2) {
+        __syncthreads();  // the chunk of w
+        const bool wide = cols >= NW;
+        const int G = wide ? 1 : NW / cols;  // warps per column
+        double2 acc[KQ];
+#pragma unroll
+        for (int q = 0; q < KQ; ++q) acc[q] = make_double2(0, 0);
+        if (wide || warp < G * cols) {
+            const int kw = wide ? warp : warp % cols;
+            const int slice = wide ? 0 : warp / cols;
+            const int rs = (int)((int64_t)len * slice / G), re = (int)((int64_t)len * (slice + 1) / G);
+            for (int r = rs + lane; r < re; r += 32) {
+                T2 t[KQ];
+#pragma unroll
+                for (int q = 0; q < KQ; ++q) {
+                    const int k = kw + NW * q;
+                    t[q] = ((wide || q == 0) && k < cols) ? Vr[k * col + r] : from_d2<T2>(make_double2(0, 0));
+                }
+                const double2 x = to_d2(ws[r]);
+#pragma unroll
+                for (int q = 0; q < KQ; ++q) acc[q] = dadd(acc[q], dmulc(to_d2(t[q]), x));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < KQ; ++q) {
+            double2 v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+                v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+            }
+            if (lane == 0) red[warp][q] = v;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < cols; k += kRT) {
+            double2 v;
+            if (wide) {
+                v = red[k % NW][k / NW];
+            } else {
+                v = make_double2(0, 0);
+                for (int g = 0; g < G; ++g) v = dadd(v, red[k + g * cols][0]);
+            }
+            part[(int64_t)k * gridDim.x + blockIdx.x] = v;
+        }
+    } else {
+        double2 v[1] = {make_double2(nrm, 0)};
+        block_sum<1>(v, part + blockIdx.x);
+    }
+    if (!arrive(&S.counter)) return;
+    if (mode == 2) {
+        const double tot = cta_total(part, gridDim.x).x;
+        if (threadIdx.x == 0) arnoldi_finish(S, ar, rhs, tot);
+        return;
+    }
+    for (int k = warp; k < cols; k += NW) {
+        double2 v = make_double2(0, 0);
+        const double2* pk = part + (int64_t)k * gridDim.x;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v = dadd(v, pk[b]);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+        }
+        if (lane == 0) {
+            double2* h = ar.h + (int64_t)rhs * mc;
+            ar.c[(int64_t)rhs * mc + k] = v;
+            h[k] = mode == 0 ? v : dadd(h[k], v);
+        }
+    }
+}
+
+// CTAs and rows per CTA of k_gm_orth_stream: at least two CTAs per SM, chunks of at most about
+// kStreamRows rows, no more CTAs than the partial buffers hold.
+static void stream_config(int64_t n, int* blocks, int* chunk) {
+    const int64_t want = std::max<int64_t>(2 * 148, (n + kStreamRows - 1) / kStreamRows);
+    const int64_t b = std::max<int64_t>(1, std::min<int64_t>(want, reduce_blocks(n)));
+    int64_t c = (n + b - 1) / b;
+    c = (c + 31) / 32 * 32;
+    *chunk = (int)c;
+    *blocks = (int)((n + c - 1) / c);
+}
+
 // (the dynamic shared-memory attributes are set before any capture, in gmres())
 template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, int nrhs, GmState* st, const GmArrays& ar,
                                                int mode, cudaStream_t s) {
+    if (ar.m + 1 <= kStreamCols) {
+        int blocks, chunk;
+        stream_config(n, &blocks, &chunk);
+        k_gm_orth_stream<T2><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar, mode,
+                                                                                        chunk);
+        count_launch();
+        return;
+    }
     int TR;
     size_t smem;
     orth_config<T2>(ar.m, &TR, &smem);
@@ -928,6 +1080,12 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     count_launch();
     // function attributes are set before the capture
     RTM_CUDA(cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    {
+        int sb, sc;
+        stream_config(n, &sb, &sc);
+        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      std::max<int>(sc * (int)sizeof(T2), 48 * 1024)));
+    }
     RTM_CUDA(cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     std::vector<GmState> host(nrhs);
     T2* Vp = V.as<T2>();
