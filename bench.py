@@ -40,8 +40,8 @@ WORKLOADS = {
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
                pc=None, precision="mixed"),
     # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32 COCG
-    # with a FP32 block-Jacobi preconditioner inside FP64 iterative refinement
-    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=50, pc="blockJacobi",
+    # with the FP32 rChan circulant preconditioner (the reference's default) inside FP64 iterative refinement
+    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=50, pc="rChan",
                precision="mixed", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
     "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
@@ -89,7 +89,7 @@ def solve_batch(R, w, b=None):
     dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
     op = R.Operator(prob, maxRhs=w["rhs"])
     inner = R.Operator(prob, precision="single", maxRhs=w["rhs"])
-    pc = R.Preconditioner.blockJacobi(prob, (2, 2), precision="single")
+    pc = R.Preconditioner(prob, kernel="rChan", precision="single")
     if b is None:
         b = batch_rhs(R, prob, dirs, pols)
     res = R.Solver(method="fgmres", innerMethod="cg", tolerance=w["tol"], innerTolerance=1e-4,
@@ -219,7 +219,7 @@ def run_batched(args, w):
         "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64/c128", "data": "synthetic plate and 64 plane waves, seed 0",
         "config": {"workload": f"c4: {n}x{n} plate, cell lambda/{w['density']}, {N} unknowns, {w['rhs']} plane "
-                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 block-Jacobi inside FP64 "
+                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 rChan circulant inside FP64 "
                                f"refinement to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
                    "l2": "working set per batch re-created every step"},
         "iterations": its[0], "true_residual": res_max, "all_converged_to_tolerance": res_max <= w["tol"],
@@ -453,6 +453,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--once", action="store_true",
                     help="one untimed solve of the workload, no JSON line (the command profiler captures run)")
+    ap.add_argument("--matvec", action="store_true",
+                    help="only the product of the workload, applied --steps times (the command profiler captures run)")
     ap.add_argument("--requests", type=int, default=100, help="c5: requests in the stream (2000 in the full form)")
     ap.add_argument("--slots", type=int, default=8, help="c5: requests on the device at once")
     ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
@@ -490,6 +492,11 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.matvec:
+        rf = roofline_matvec(R, w, args.steps, torch.cuda.current_stream().cuda_stream)
+        print(f"product {rf['precision']} {rf['P']}x{rf['Q']}: {rf['seconds'] * 1e6:.1f} us, "
+              f"{rf['bytes'] / rf['seconds'] / 1e9:.0f} GB/s")
+        return
     if args.once:
         _, _, res, rcs = solve_plate(R, w)
         torch.cuda.synchronize()
