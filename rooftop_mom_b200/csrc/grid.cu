@@ -21,44 +21,14 @@
 
 #include "fft.cuh"
 #include "grid.h"
+#include "grid_args.cuh"
 
 namespace rtm {
 
 static constexpr int kSmemBudget = 200 * 1024;
 static constexpr int kMaxThreads = 256;  // CTA size of the FFT kernels (up to 255 registers a thread)
 
-template <typename T> struct GridArgs {
-    using T2 = typename Cx<T>::T2;
-    int P, Q, nsx, nsy;
-    int rows[2], cols[2];
-    int64_t off[2];
-    int64_t n;
-    int ncomp;
-    int ti;          // x columns per y-tile
-    int py0, npy;    // y subbands handled by this launch (lean: one at a time)
-    int accumulate;  // y-inverse adds into y (second parity of the lean product)
-    FftPlan planP, planQ;
-    const T2* twP;
-    const T2* twQ;
-    const T2* modP;
-    const T2* modQ;
-    T2* work;
-    int64_t work_rhs;  // elements of W per right-hand side
-    int mode;
-    const T2* spec;
-    const T2* ux0;
-    const T2* ux1;
-    const T2* vy0;
-    const T2* vy1;
-    T inv_a2, inv_b2, inv_ab, scale;
-    const int* skip;  // per right-hand side, nonzero: leave it alone
-    int skip_stride;
-    int cb, ls;  // x-mix: y frequencies per CTA and the padded line stride
-};
-
-template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rhs) {
-    return a.skip != nullptr && a.skip[(int64_t)rhs * a.skip_stride] != 0;
-}
+// GridArgs and skipped(): grid_args.cuh
 
 // Copies the n roots of unity into shared memory (ordered before use by the caller's barrier).
 template <typename T2> __device__ __forceinline__ void stage_roots(T2* dst, const T2* __restrict__ src, int n) {
@@ -405,6 +375,12 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     a.scale = (T)(1.0 / ((double)g.P * g.Q));
     a.work = static_cast<T2*>(work);
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
+    if (g.mode == kGen3 && g.nsx == 2 && g.nsy == 2 && !g.lean && fast_split_eligible(g.P, g.Q, sizeof(T) == 8)) {
+        a.py0 = 0;
+        a.npy = 2;
+        a.accumulate = 0;
+        return launch_fast_split<T>(a, nrhs, x, y, s);
+    }
     const int passes = g.lean ? g.nsy : 1;
     const int npy = g.lean ? 1 : g.nsy;
     // y passes: TI x columns per CTA (rows of 64 bytes) for every y subband at once; fewer columns

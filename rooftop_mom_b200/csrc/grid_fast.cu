@@ -1,0 +1,393 @@
+// Power-of-two split products with register-resident line transforms.
+//
+// The same product as k_grid_y_fwd / k_grid_x_mix / k_grid_y_inv in grid.cu (the reference's
+// src/+rooftopMoM/+assembler/+greensMatrix/@SplitFFTApplicator/applyBothDirections_.m:14-85) for
+// transform sizes that are powers of two. A line of n = R1 R2 points is transformed by a group of R2
+// threads, each holding R1 values in registers (four-step form, decimation in time):
+//   thread m2 holds x[R2 m1 + m2], m1 < R1
+//   -> R1-point DFT over m1 in registers -> twiddle w_n^(m2 k1)
+//   -> one exchange through shared memory
+//   -> R1 / R2 DFTs of R2 points over m2 -> X[k1 + R1 k2], thread t holding k1 = t + R2 s (s < R1 / R2)
+//      for every k2, at register s R2 + k2.
+// The inverse runs the same steps backwards from that layout. The x-mix multiplies the spectra in this
+// layout without reordering; every global load and store is coalesced (consecutive threads touch
+// consecutive elements). The line buffers are padded (row stride R2 + 1) against bank conflicts.
+#include "grid.h"
+#include "grid_args.cuh"
+
+namespace rtm {
+namespace {
+
+// CTA size and CTAs per SM: FP32 256 threads x 2 (128 registers a thread), FP64 128 threads x 3 (170).
+template <typename T> struct Fast {
+    static constexpr int threads = sizeof(T) == 8 ? 128 : 256;
+    static constexpr int blocks = sizeof(T) == 8 ? 3 : 2;
+};
+
+template <int N> struct Shape;
+template <> struct Shape<32> { static constexpr int R1 = 8, R2 = 4; };
+template <> struct Shape<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Shape<128> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct Shape<256> { static constexpr int R1 = 16, R2 = 16; };
+template <> struct Shape<512> { static constexpr int R1 = 32, R2 = 16; };
+template <> struct Shape<1024> { static constexpr int R1 = 32, R2 = 32; };
+
+// In-register DFT of R points, natural order in and out. R = 32 splits by decimation in frequency
+// into two 16-point transforms with the roots w_32^k = tw[k n / 32] of the length-n table.
+template <int R, bool INV, typename T2>
+__device__ __forceinline__ void dft_reg(T2 (&v)[R], const T2* __restrict__ tw, int n) {
+    if constexpr (R == 4) {
+        dft4<INV>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 8) {
+        dft8<INV>(v);
+    } else if constexpr (R == 16) {
+        dft16<INV>(v);
+    } else {
+        static_assert(R == 32, "radix");
+        T2 a[16], b[16];
+        const int st = n / 32;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            a[k] = cadd(v[k], v[k + 16]);
+            b[k] = csub(v[k], v[k + 16]);
+            if (k) {
+                const T2 w = __ldg(&tw[k * st]);
+                b[k] = INV ? cmulc(b[k], w) : cmul(b[k], w);
+            }
+        }
+        dft16<INV>(a);
+        dft16<INV>(b);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            v[2 * k] = a[k];
+            v[2 * k + 1] = b[k];
+        }
+    }
+}
+
+// Element (r, c) of a line buffer at base[r * RS + c * CS].
+template <typename T2> struct LineBuf {
+    T2* base;
+    int RS, CS;
+    __device__ __forceinline__ T2& at(int r, int c) const { return base[r * RS + c * CS]; }
+};
+
+// Forward transform of the group's line, steps before the exchange: v[m1] = x[R2 m1 + t] in,
+// written to buf(k1, t).
+template <int N, typename T2>
+__device__ __forceinline__ void fwd_first(T2 (&v)[Shape<N>::R1], int t, const T2* __restrict__ tw,
+                                          const LineBuf<T2>& buf) {
+    constexpr int R1 = Shape<N>::R1;
+    dft_reg<R1, false>(v, tw, N);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        const T2 w = k1 ? cmul(v[k1], __ldg(&tw[t * k1])) : v[k1];
+        buf.at(k1, t) = w;
+    }
+}
+
+// After the exchange: v[s R2 + k2] = X[(t + R2 s) + R1 k2].
+template <int N, typename T2>
+__device__ __forceinline__ void fwd_second(T2 (&v)[Shape<N>::R1], int t, const T2* __restrict__ tw,
+                                           const LineBuf<T2>& buf) {
+    constexpr int R1 = Shape<N>::R1, R2 = Shape<N>::R2, S = R1 / R2;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        T2 u[R2];
+#pragma unroll
+        for (int m2 = 0; m2 < R2; ++m2) u[m2] = buf.at(t + R2 * s, m2);
+        dft_reg<R2, false>(u, tw, N);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[s * R2 + k2] = u[k2];
+    }
+}
+
+// Inverse from the transformed layout, steps before the exchange: written to buf(k1, m2) twiddled.
+template <int N, typename T2>
+__device__ __forceinline__ void inv_first(T2 (&v)[Shape<N>::R1], int t, const T2* __restrict__ tw,
+                                          const LineBuf<T2>& buf) {
+    constexpr int R1 = Shape<N>::R1, R2 = Shape<N>::R2, S = R1 / R2;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        T2 u[R2];
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) u[k2] = v[s * R2 + k2];
+        dft_reg<R2, true>(u, tw, N);
+        const int k1 = t + R2 * s;
+#pragma unroll
+        for (int m2 = 0; m2 < R2; ++m2) buf.at(k1, m2) = (m2 && k1) ? cmulc(u[m2], __ldg(&tw[m2 * k1])) : u[m2];
+    }
+}
+
+// After the exchange: v[m1] = N x[R2 m1 + t] (unnormalised).
+template <int N, typename T2>
+__device__ __forceinline__ void inv_second(T2 (&v)[Shape<N>::R1], int t, const T2* __restrict__ tw,
+                                           const LineBuf<T2>& buf) {
+    constexpr int R1 = Shape<N>::R1;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = buf.at(k1, t);
+    dft_reg<R1, true>(v, tw, N);
+}
+
+// --------------------------------------------------------------------------------------------
+// y-forward: TI x-columns of one component; a group per (column, y subband). Thread index
+// l + TI (py + 2 t): consecutive threads take consecutive columns, so rows of TI elements are read
+// and written at once. W[py][c][k][i] = FFT_y(x_c(i, j) mod_y(j)^py).
+template <typename T, int NQ>
+__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+    using T2 = typename Cx<T>::T2;
+    constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* sm = reinterpret_cast<T2*>(smem_raw);
+    const int c = blockIdx.y, rhs = blockIdx.z;
+    if (skipped(a, rhs)) return;
+    const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
+    const int g = l + TI * py;
+    const int rows = a.rows[c], cols = a.cols[c];
+    const int i = blockIdx.x * TI + l;
+    const bool on = i < rows;
+    const LineBuf<T2> buf{sm + g, (R2 + 1) * G, G};
+    const T2* xr = x + (int64_t)rhs * a.n + a.off[c];
+    T2 v[R1];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int j = R2 * m1 + t;
+        T2 e = (on && j < cols) ? xr[i + (int64_t)j * rows] : czero<T2>();
+        if (py) e = cmul(e, __ldg(&a.modQ[j]));
+        v[m1] = e;
+    }
+    fwd_first<NQ>(v, t, a.twQ, buf);
+    __syncthreads();
+    fwd_second<NQ>(v, t, a.twQ, buf);
+    if (!on) return;
+    T2* dst = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * NQ * a.P + i;
+#pragma unroll
+    for (int s = 0; s < R1 / R2; ++s)
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) dst[(int64_t)((t + R2 * s) + R1 * k2) * a.P] = v[s * R2 + k2];
+}
+
+// x-mix: teams of four groups (component c, x subband px) per y frequency j of subband py. Thread
+// index t + R2 (team * 4 + 2 px + c). Forward transform along x of W mod_x^px, the 2x2 block mix
+// with the subband spectra (the two components of a group pair meet through shared memory), inverse
+// transform, demodulation, the sum over px, scaled by 1 / (PQ), in place in W.
+template <typename T, int NP>
+__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_x_mix(const GridArgs<T> a) {
+    using T2 = typename Cx<T>::T2;
+    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, S = R1 / R2;
+    constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* sm = reinterpret_cast<T2*>(smem_raw);
+    const int py = blockIdx.y, rhs = blockIdx.z;
+    if (skipped(a, rhs)) return;
+    const int t = threadIdx.x % R2, gid = threadIdx.x / R2;
+    const int team = gid / 4, c = gid % 2, px = (gid / 2) % 2;
+    const int j = blockIdx.x * TEAMS + team;
+    const bool on = j < a.Q;
+    const int Q = a.Q;
+    const int64_t QP = (int64_t)Q * NP;
+    const LineBuf<T2> buf{sm + gid * LB, R2 + 1, 1};
+    T2* own = sm + gid * LB;
+    const T2* partner = sm + (gid ^ 1) * LB;
+    const int rows = a.rows[c];
+    T2* row = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * QP + (int64_t)(on ? j : 0) * NP;
+    T2 v[R1];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int i = R2 * m1 + t;
+        T2 e = (on && i < rows) ? row[i] : czero<T2>();
+        if (px) e = cmul(e, __ldg(&a.modP[i]));
+        v[m1] = e;
+    }
+    fwd_first<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    fwd_second<NP>(v, t, a.twP, buf);
+    __syncthreads();  // the buffers are read; they now carry the spectra values to the partner
+#pragma unroll
+    for (int r = 0; r < R1; ++r) own[r * R2 + t] = v[r];
+    __syncthreads();
+    if (on) {
+        const int sub = px + 2 * py;
+        const T2* spec = a.spec + (int64_t)(sub * 3) * QP + (int64_t)j * NP;
+        const T2* ux = px ? a.ux1 : a.ux0;
+        const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
+        const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) {
+                const int k = (t + R2 * s) + R1 * k2;
+                const T2 E = __ldg(&spec[k]);
+                const T2 M = __ldg(&spec[(1 + c) * QP + k]);
+                const T2 uu = __ldg(&ux[k]);
+                const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
+                T2 qc = cmulc(uu, vv);
+                qc.x = -qc.x * a.inv_ab;
+                qc.y = -qc.y * a.inv_ab;
+                const T2 coupling = c ? cconj(qc) : qc;
+                const T cself = c ? cv : cu;
+                const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
+                T2 o = cmul(M, me);
+                o = csub(o, cscale(cmul(E, me), cself));
+                o = cadd(o, cmul(coupling, cmul(E, other)));
+                v[s * R2 + k2] = o;
+            }
+    }
+    __syncthreads();  // the partner values are read
+    inv_first<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    inv_second<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    if (px) {
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) own[m1 * R2 + t] = cmulc(v[m1], __ldg(&a.modP[R2 * m1 + t]));
+    }
+    __syncthreads();
+    if (px || !on) return;
+    const T2* odd = sm + (gid + 2) * LB;
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int i = R2 * m1 + t;
+        if (i < rows) row[i] = cscale(cadd(v[m1], odd[m1 * R2 + t]), a.scale);
+    }
+}
+
+// y-inverse: TI columns of one component, a group per (column, y subband); inverse transform along y,
+// demodulation, the sum over py through shared memory, cropped into y.
+template <typename T, int NQ>
+__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+    using T2 = typename Cx<T>::T2;
+    constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* sm = reinterpret_cast<T2*>(smem_raw);
+    const int c = blockIdx.y, rhs = blockIdx.z;
+    if (skipped(a, rhs)) return;
+    const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
+    const int g = l + TI * py;
+    const int rows = a.rows[c], cols = a.cols[c];
+    const int i = blockIdx.x * TI + l;
+    const bool on = i < rows;
+    const LineBuf<T2> buf{sm + g, (R2 + 1) * G, G};
+    const T2* src = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * NQ * a.P + (on ? i : 0);
+    T2 v[R1];
+#pragma unroll
+    for (int s = 0; s < R1 / R2; ++s)
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2)
+            v[s * R2 + k2] = on ? src[(int64_t)((t + R2 * s) + R1 * k2) * a.P] : czero<T2>();
+    inv_first<NQ>(v, t, a.twQ, buf);
+    __syncthreads();
+    inv_second<NQ>(v, t, a.twQ, buf);
+    __syncthreads();
+    if (py) {
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) buf.at(m1, t) = cmulc(v[m1], __ldg(&a.modQ[R2 * m1 + t]));
+    }
+    __syncthreads();
+    if (py || !on) return;
+    const LineBuf<T2> odd{sm + g + TI, (R2 + 1) * G, G};
+    T2* yr = y + (int64_t)rhs * a.n + a.off[c];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int j = R2 * m1 + t;
+        if (j < cols) yr[i + (int64_t)j * rows] = cadd(v[m1], odd.at(m1, t));
+    }
+}
+
+template <typename T, int NQ> size_t y_smem() {
+    constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2);
+    return (size_t)2 * TI * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
+}
+template <typename T, int NP> size_t x_smem() {
+    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, TEAMS = Fast<T>::threads / (4 * R2);
+    return (size_t)4 * TEAMS * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
+}
+
+template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd,
+                                           cudaStream_t s) {
+    using T2 = typename Cx<T>::T2;
+    constexpr int TI = Fast<T>::threads / (2 * Shape<NQ>::R2);
+    const size_t smem = y_smem<T, NQ>();
+    static bool attrs[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attrs[dev & 63]) {
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_fwd<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_inv<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attrs[dev & 63] = true;
+    }
+    const int rows_max = a.rows[0] > a.rows[1] ? a.rows[0] : a.rows[1];
+    const dim3 grid((rows_max + TI - 1) / TI, 2, nrhs);
+    if (fwd) k_fast_y_fwd<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<const T2*>(x));
+    else k_fast_y_inv<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<T2*>(y));
+    count_launch();
+    return RTM_OK;
+}
+
+template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
+    constexpr int TEAMS = Fast<T>::threads / (4 * Shape<NP>::R2);
+    const size_t smem = x_smem<T, NP>();
+    static bool attrs[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attrs[dev & 63]) {
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attrs[dev & 63] = true;
+    }
+    const dim3 grid((a.Q + TEAMS - 1) / TEAMS, 2, nrhs);
+    k_fast_x_mix<T, NP><<<grid, Fast<T>::threads, smem, s>>>(a);
+    count_launch();
+    return RTM_OK;
+}
+
+template <typename T> int dispatch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd, cudaStream_t s) {
+    switch (a.Q) {
+        case 32: return launch_y<T, 32>(a, nrhs, x, y, fwd, s);
+        case 64: return launch_y<T, 64>(a, nrhs, x, y, fwd, s);
+        case 128: return launch_y<T, 128>(a, nrhs, x, y, fwd, s);
+        case 256: return launch_y<T, 256>(a, nrhs, x, y, fwd, s);
+        default:
+            if constexpr (sizeof(T) == 4) {
+                if (a.Q == 512) return launch_y<T, 512>(a, nrhs, x, y, fwd, s);
+                return launch_y<T, 1024>(a, nrhs, x, y, fwd, s);
+            }
+            return fail(RTM_ERR_UNSUPPORTED, "transform size");
+    }
+}
+
+template <typename T> int dispatch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
+    switch (a.P) {
+        case 32: return launch_x<T, 32>(a, nrhs, s);
+        case 64: return launch_x<T, 64>(a, nrhs, s);
+        case 128: return launch_x<T, 128>(a, nrhs, s);
+        case 256: return launch_x<T, 256>(a, nrhs, s);
+        default:
+            if constexpr (sizeof(T) == 4) {
+                if (a.P == 512) return launch_x<T, 512>(a, nrhs, s);
+                return launch_x<T, 1024>(a, nrhs, s);
+            }
+            return fail(RTM_ERR_UNSUPPORTED, "transform size");
+    }
+}
+
+}  // namespace
+
+bool fast_split_eligible(int P, int Q, bool fp64) {
+    auto ok = [&](int n) { return n >= 32 && n <= (fp64 ? 256 : 1024) && (n & (n - 1)) == 0; };
+    return ok(P) && ok(Q);
+}
+
+template <typename T>
+int launch_fast_split(const GridArgs<T>& a, int nrhs, const void* x, void* y, cudaStream_t s) {
+    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, true, s));
+    RTM_TRY(dispatch_x<T>(a, nrhs, s));
+    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, false, s));
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
+template int launch_fast_split<float>(const GridArgs<float>&, int, const void*, void*, cudaStream_t);
+template int launch_fast_split<double>(const GridArgs<double>&, int, const void*, void*, cudaStream_t);
+
+}  // namespace rtm

@@ -6,7 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import rel
+from conftest import random_vector, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -162,3 +162,37 @@ def test_mixed_precision_refinement_reaches_fp64_tolerance():
                    maxIterationCount=5000).solve(op64, exc, innerOperator=op32)
     assert mix.converged() and mix.residualNorm() < 1e-8
     assert rel(mix.solution(), ref.solution()) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_batched_circulant_apply_equals_single_applies(precision):
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(32, 24, 0.05, 0.05), 2 * np.pi)
+    n = prob.rooftopCount()
+    pc = R.Preconditioner(prob, kernel="rChan", precision=precision)
+    vs = [random_vector(n, seed=30 + k) for k in range(3)]
+    ys = pc.apply(np.concatenate(vs), nrhs=3)
+    for k in range(3):
+        assert rel(ys[k * n:(k + 1) * n], pc.apply(vs[k])) < 1e-14
+
+
+def test_mixed_cocg_with_a_circulant_solves_several_right_hand_sides():
+    """The batching form's solver on a small plate: FP32 COCG preconditioned by the FP32 rChan circulant
+    inside FP64 refinement, four plane waves at once, each to its FP64 tolerance."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(48, 40, 1 / 20, 1 / 20), 2 * np.pi)
+    n = prob.rooftopCount()
+    op64 = R.Operator(prob, maxRhs=4)
+    op32 = R.Operator(prob, precision="single", maxRhs=4)
+    pc32 = R.Preconditioner(prob, kernel="rChan", precision="single")
+    dirs = [(0, 0, -1), (0.5, 0, -np.sqrt(0.75)), (0, 0.6, -0.8), (0.3, 0.4, -np.sqrt(0.75))]
+    pols = [(1, 0, 0), (0, 1, 0), (1, 0, 0), (0.8, -0.6, 0)]
+    b = np.concatenate([R.Excitation.planeWave(prob, direction=d, polarization=p).vector() for d, p in zip(dirs, pols)])
+    res = R.Solver(method="fgmres", innerMethod="cg", tolerance=1e-6, innerTolerance=1e-4,
+                   maxIterationCount=5000).solve(op64, b, innerOperator=op32, innerPreconditioner=pc32, nrhs=4)
+    for k, r in enumerate(res):
+        assert r.converged() and r.residualNorm() <= 1e-6
+        single = R.Solver(method="cg", tolerance=1e-10, maxIterationCount=5000).solve(op64, b[k * n:(k + 1) * n])
+        assert rel(r.solution(), single.solution()) < 1e-4
