@@ -39,9 +39,11 @@ WORKLOADS = {
                pc="blockJacobi", precision="double"),
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
                pc=None, precision="mixed"),
-    # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32 COCG
-    # with the FP32 rChan circulant preconditioner (the reference's default) inside FP64 iterative refinement
-    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=50, pc="rChan",
+    # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32
+    # flexible GMRES(30) right-preconditioned by the FP32 rChan circulant (the reference's default) inside
+    # FP64 iterative refinement (FP32 COCG stagnated above the inner tolerance on this batch and its
+    # corrections diverged)
+    "c4": dict(n=512, density=20, rhs=64, seed=0, method="fgmres", tol=1e-6, restart=30, pc="rChan",
                precision="mixed", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
     "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
@@ -84,7 +86,7 @@ def batch_rhs(R, prob, dirs, pols):
 
 
 def solve_batch(R, w, b=None):
-    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 COCG solve."""
+    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 FGMRES solve."""
     prob = build_plate(R, w)
     dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
     op = R.Operator(prob, maxRhs=w["rhs"])
@@ -92,8 +94,9 @@ def solve_batch(R, w, b=None):
     pc = R.Preconditioner(prob, kernel="rChan", precision="single")
     if b is None:
         b = batch_rhs(R, prob, dirs, pols)
-    res = R.Solver(method="fgmres", innerMethod="cg", tolerance=w["tol"], innerTolerance=1e-4,
-                   maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc, nrhs=w["rhs"])
+    res = R.Solver(method="fgmres", innerMethod="fgmres", tolerance=w["tol"], restart=w["restart"],
+                   innerTolerance=1e-4, maxIterationCount=20000).solve(op, b, innerOperator=inner,
+                                                                     innerPreconditioner=pc, nrhs=w["rhs"])
     return prob, res
 
 
@@ -214,12 +217,12 @@ def run_batched(args, w):
     t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
     n, N = w["n"], prob.rooftopCount()
     line = {
-        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 COCG inside FP64 refinement",
+        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 FGMRES inside FP64 refinement",
         "value": w["rhs"] * args.steps / t, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64/c128", "data": "synthetic plate and 64 plane waves, seed 0",
         "config": {"workload": f"c4: {n}x{n} plate, cell lambda/{w['density']}, {N} unknowns, {w['rhs']} plane "
-                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 rChan circulant inside FP64 "
+                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 FGMRES(30) + FP32 rChan circulant inside FP64 "
                                f"refinement to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
                    "l2": "working set per batch re-created every step"},
         "iterations": its[0], "true_residual": res_max, "all_converged_to_tolerance": res_max <= w["tol"],
@@ -460,7 +463,7 @@ def main():
     ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
-    if args.workload in ("c4", "c5"):
+    if args.workload in ("c4", "c5") and not args.matvec:
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": f"the CPU oracle arm times single-plate solves "
                                                                   f"(c1, c2, c3), not {args.workload}"}))
