@@ -153,42 +153,54 @@ __global__ void k_bj_build(const BjArgs g) {
         for (int c = 0; c < cnt; ++c) out[r * kMaxBlockUnknowns + c] = B[r][c];
 }
 
+// The inverses packed to S = 2 bx by unknowns a block, column-major inside the block (entry (r, c) at
+// blk S^2 + c S + r), so the S threads of a block read S consecutive entries per column.
 template <typename T2>
-__global__ void k_bj_apply(int nblocks, const int* __restrict__ counts, const int64_t* __restrict__ index,
+__global__ void k_bj_pack(int nblocks, int S, const double2* __restrict__ inv64, const int64_t* __restrict__ index,
+                          T2* __restrict__ out, int64_t* __restrict__ packed_index) {
+    const int64_t total = (int64_t)nblocks * S * S;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t blk = t / ((int64_t)S * S);
+        const int e = (int)(t - blk * S * S), c = e / S, r = e % S;
+        const double2 v = inv64[(blk * kMaxBlockUnknowns + r) * kMaxBlockUnknowns + c];
+        out[t] = cmake<T2>(v.x, v.y);
+        if (e < S) packed_index[blk * S + e] = index[blk * kMaxBlockUnknowns + e];
+    }
+}
+
+// y(idx_r) = sum_c inv(r, c) x(idx_c) over the block's unknowns, one thread per (block, row).
+template <typename T2>
+__global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, const int64_t* __restrict__ index,
                            const T2* __restrict__ inv, const T2* __restrict__ x, T2* __restrict__ y, int64_t n,
                            const int* skip, int stride) {
     const int rhs = blockIdx.y;
     if (skip && skip[(int64_t)rhs * stride]) return;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int blk = (int)(t / kMaxBlockUnknowns), r = (int)(t % kMaxBlockUnknowns);
+    const int blk = (int)(t / S), r = (int)(t % S);
     if (blk >= nblocks) return;
     const int cnt = counts[blk];
     if (r >= cnt) return;
-    const int64_t* idx = index + (int64_t)blk * kMaxBlockUnknowns;
-    const T2* row = inv + ((int64_t)blk * kMaxBlockUnknowns + r) * kMaxBlockUnknowns;
+    const int64_t* idx = index + (int64_t)blk * S;
+    const T2* col = inv + (int64_t)blk * S * S + r;
     const T2* xr = x + rhs * n;
     T2 acc = czero<T2>();
-    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(row[c], xr[idx[c]]));
+    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
     y[rhs * n + idx[r]] = acc;
-}
-
-__global__ void k_d2f_bj(const double2* __restrict__ in, float2* __restrict__ out, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = make_float2((float)in[i].x, (float)in[i].y);
 }
 
 struct BlockJacobi : LinearOp {
     int nblocks = 0;
+    int S = kMaxBlockUnknowns;  // unknowns a block at most (packed stride)
     DeviceBuffer counts, index, inv;
     int apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) override {
-        const int64_t threads = (int64_t)nblocks * kMaxBlockUnknowns;
+        const int64_t threads = (int64_t)nblocks * S;
         dim3 g((unsigned)((threads + 255) / 256), nrhs);
         if (precision == RTM_FP64)
-            k_bj_apply<double2><<<g, 256, 0, s>>>(nblocks, counts.as<int>(), index.as<int64_t>(), inv.as<double2>(),
+            k_bj_apply<double2><<<g, 256, 0, s>>>(nblocks, S, counts.as<int>(), index.as<int64_t>(), inv.as<double2>(),
                                                   static_cast<const double2*>(x), static_cast<double2*>(y), n, skip.ptr,
                                                   skip.stride);
         else
-            k_bj_apply<float2><<<g, 256, 0, s>>>(nblocks, counts.as<int>(), index.as<int64_t>(), inv.as<float2>(),
+            k_bj_apply<float2><<<g, 256, 0, s>>>(nblocks, S, counts.as<int>(), index.as<int64_t>(), inv.as<float2>(),
                                                  static_cast<const float2*>(x), static_cast<float2*>(y), n, skip.ptr,
                                                  skip.stride);
         count_launch();
@@ -224,15 +236,15 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
     g.nx_roof = nx_roof;
     op->nblocks = g.nbx * g.nby;
     const size_t nb = (size_t)op->nblocks;
-    DeviceBuffer inv64, flag;
+    DeviceBuffer inv64, index16, flag;
     StreamSyncGuard guard(s);
     if ((*status = op->counts.alloc(nb * sizeof(int))) != RTM_OK) return nullptr;
-    if ((*status = op->index.alloc(nb * kMaxBlockUnknowns * sizeof(int64_t))) != RTM_OK) return nullptr;
+    if ((*status = index16.alloc(nb * kMaxBlockUnknowns * sizeof(int64_t))) != RTM_OK) return nullptr;
     if ((*status = inv64.alloc(nb * kMaxBlockUnknowns * kMaxBlockUnknowns * sizeof(double2))) != RTM_OK) return nullptr;
     if ((*status = flag.alloc(sizeof(int))) != RTM_OK) return nullptr;
     cudaMemsetAsync(flag.ptr, 0, sizeof(int), s);
     g.counts = op->counts.as<int>();
-    g.index = op->index.as<int64_t>();
+    g.index = index16.as<int64_t>();
     g.inv = inv64.as<double2>();
     g.singular = flag.as<int>();
     cudaFuncSetAttribute(k_bj_build, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
@@ -249,14 +261,23 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
         *status = fail(RTM_ERR_SINGULAR, "a block of the block-Jacobi preconditioner is singular");
         return nullptr;
     }
-    if (precision == RTM_FP64) {
-        op->inv.take(inv64);
-    } else {
-        const int64_t cnt = (int64_t)nb * kMaxBlockUnknowns * kMaxBlockUnknowns;
-        if ((*status = op->inv.alloc(cnt * sizeof(float2))) != RTM_OK) return nullptr;
-        k_d2f_bj<<<592, 256, 0, s>>>(inv64.as<double2>(), op->inv.as<float2>(), cnt);
-        count_launch();
-        cudaStreamSynchronize(s);
+    const int S = 2 * bx * by;
+    op->S = S;
+    const int64_t cnt = (int64_t)nb * S * S;
+    if ((*status = op->index.alloc(nb * S * sizeof(int64_t))) != RTM_OK) return nullptr;
+    if ((*status = op->inv.alloc(cnt * (precision == RTM_FP64 ? sizeof(double2) : sizeof(float2)))) != RTM_OK)
+        return nullptr;
+    const unsigned pb = (unsigned)std::min<int64_t>((cnt + 255) / 256, 2368);
+    if (precision == RTM_FP64)
+        k_bj_pack<double2><<<pb, 256, 0, s>>>(op->nblocks, S, inv64.as<double2>(), index16.as<int64_t>(),
+                                              op->inv.as<double2>(), op->index.as<int64_t>());
+    else
+        k_bj_pack<float2><<<pb, 256, 0, s>>>(op->nblocks, S, inv64.as<double2>(), index16.as<int64_t>(),
+                                             op->inv.as<float2>(), op->index.as<int64_t>());
+    count_launch();
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        *status = cuda_fail(e, "block-Jacobi packing");
+        return nullptr;
     }
     *status = RTM_OK;
     return op;

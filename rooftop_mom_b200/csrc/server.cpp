@@ -32,7 +32,7 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-constexpr int kBlockJacobiUnknowns = 16;  // storage per block of the block-Jacobi inverse (ops.cu)
+constexpr int kBlockJacobiUnknowns = 8;  // packed unknowns a 2 x 2-face block of the block-Jacobi inverse (ops.cu)
 
 struct Record {
     uint64_t id = 0;
