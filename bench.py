@@ -40,10 +40,10 @@ WORKLOADS = {
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
                pc=None, precision="mixed"),
     # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32
-    # flexible GMRES(30) right-preconditioned by the FP32 rChan circulant (the reference's default) inside
-    # FP64 iterative refinement (FP32 COCG stagnated above the inner tolerance on this batch and its
-    # corrections diverged)
-    "c4": dict(n=512, density=20, rhs=64, seed=0, method="fgmres", tol=1e-6, restart=30, pc="rChan",
+    # COCG preconditioned by the FP32 rChan circulant (the reference's default) inside FP64 iterative
+    # refinement, each inner solve to 1e-2 (long FP32 COCG runs toward 1e-4 lost accuracy and their
+    # corrections diverged on this batch)
+    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=30, pc="rChan", inner_tol=1e-2,
                precision="mixed", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
     "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
@@ -86,7 +86,7 @@ def batch_rhs(R, prob, dirs, pols):
 
 
 def solve_batch(R, w, b=None):
-    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 FGMRES solve."""
+    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 COCG solve."""
     prob = build_plate(R, w)
     dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
     op = R.Operator(prob, maxRhs=w["rhs"])
@@ -94,9 +94,9 @@ def solve_batch(R, w, b=None):
     pc = R.Preconditioner(prob, kernel="rChan", precision="single")
     if b is None:
         b = batch_rhs(R, prob, dirs, pols)
-    res = R.Solver(method="fgmres", innerMethod="fgmres", tolerance=w["tol"], restart=w["restart"],
-                   innerTolerance=1e-4, maxIterationCount=20000).solve(op, b, innerOperator=inner,
-                                                                     innerPreconditioner=pc, nrhs=w["rhs"])
+    res = R.Solver(method="fgmres", innerMethod=w["method"] if w["method"] == "cg" else "fgmres",
+                   tolerance=w["tol"], restart=w["restart"], innerTolerance=w["inner_tol"], maxRefinements=40,
+                   maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc, nrhs=w["rhs"])
     return prob, res
 
 
@@ -217,12 +217,12 @@ def run_batched(args, w):
     t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
     n, N = w["n"], prob.rooftopCount()
     line = {
-        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 FGMRES inside FP64 refinement",
+        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 COCG inside FP64 refinement",
         "value": w["rhs"] * args.steps / t, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64/c128", "data": "synthetic plate and 64 plane waves, seed 0",
         "config": {"workload": f"c4: {n}x{n} plate, cell lambda/{w['density']}, {N} unknowns, {w['rhs']} plane "
-                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 FGMRES(30) + FP32 rChan circulant inside FP64 "
+                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 rChan circulant inside FP64 "
                                f"refinement to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
                    "l2": "working set per batch re-created every step"},
         "iterations": its[0], "true_residual": res_max, "all_converged_to_tolerance": res_max <= w["tol"],
@@ -434,6 +434,10 @@ REFERENCE_ITERATIONS = {"c2": 2511, "c1": 300, "c3": 300}
 
 METRIC = "solves/s at rel. residual 1e-6, mixed vs FP64 GPU; matvec HBM GB/s; p99 ms"
 
+# DRAM bytes (read + write) of one product, summed over its three kernels, from one ncu capture each
+# (profiles/product_fast_path.md); None where no capture was made.
+TRAFFIC = {"c2": 23.2e6, "c3": 200.3e6}
+
 
 def config_of(args, w):
     n = w["n"]
@@ -579,7 +583,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": kind, "kernel": f"split-FFT product ({rf['precision']}, {rf['P']}x{rf['Q']} grid, "
                                                    f"3 kernels)", "bytes_per_launch": rf["bytes"],
-                     "seconds_per_launch": rf["seconds"], "traffic": None},
+                     "seconds_per_launch": rf["seconds"], "traffic": TRAFFIC.get(args.workload)},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 16 * N,
                 "d2h_bytes_per_step": 16 * N},
         "gpu_launches": int(launches),
