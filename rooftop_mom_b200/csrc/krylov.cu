@@ -603,16 +603,24 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
             const int kw = wide ? warp : warp % cols;
             const int slice = wide ? 0 : warp / cols;
             const int rs = (int)((int64_t)len * slice / G), re = (int)((int64_t)len * (slice + 1) / G);
-            for (int r = rs + lane; r < re; r += 32) {
-                T2 t[KQ];
+            // two rows a lane per step: up to 2 KQ loads in flight
+            for (int r = rs + lane; r < re; r += 64) {
+                const bool second = r + 32 < re;
+                T2 t[KQ], u[KQ];
 #pragma unroll
                 for (int q = 0; q < KQ; ++q) {
                     const int k = kw + NW * q;
-                    t[q] = ((wide || q == 0) && k < cols) ? Vr[k * col + r] : from_d2<T2>(make_double2(0, 0));
+                    const bool use = (wide || q == 0) && k < cols;
+                    t[q] = use ? Vr[k * col + r] : from_d2<T2>(make_double2(0, 0));
+                    u[q] = (use && second) ? Vr[k * col + r + 32] : from_d2<T2>(make_double2(0, 0));
                 }
                 const double2 x = to_d2(ws[r]);
+                const double2 x2 = second ? to_d2(ws[r + 32]) : make_double2(0, 0);
 #pragma unroll
-                for (int q = 0; q < KQ; ++q) acc[q] = dadd(acc[q], dmulc(to_d2(t[q]), x));
+                for (int q = 0; q < KQ; ++q) {
+                    acc[q] = dadd(acc[q], dmulc(to_d2(t[q]), x));
+                    acc[q] = dadd(acc[q], dmulc(to_d2(u[q]), x2));
+                }
             }
         }
 #pragma unroll
