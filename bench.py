@@ -39,12 +39,13 @@ WORKLOADS = {
                pc="blockJacobi", precision="double"),
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
                pc=None, precision="mixed"),
-    # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; FP32
-    # COCG preconditioned by the FP32 rChan circulant (the reference's default) inside FP64 iterative
-    # refinement, each inner solve to 1e-2 (long FP32 COCG runs toward 1e-4 lost accuracy and their
-    # corrections diverged on this batch)
-    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=30, pc="rChan", inner_tol=1e-2,
-               precision="mixed", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
+    # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; COCG
+    # preconditioned by the rChan circulant (the reference's default) in FP64 for all right-hand sides at
+    # once. FP32 COCG inside FP64 refinement diverges on this plate (its FP32 recurrences break down
+    # within the first inner solve, while FP64 COCG converges in about 1100 iterations), and restarted
+    # FP32 GMRES(30) needs more than 20000 iterations, so the precision form is measured on c3.
+    "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=30, pc="rChan",
+               precision="double", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
     "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
                theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
@@ -86,17 +87,15 @@ def batch_rhs(R, prob, dirs, pols):
 
 
 def solve_batch(R, w, b=None):
-    """One batched solve of the c4 workload: all right-hand sides in one FP64-refined FP32 COCG solve."""
+    """One batched solve of the c4 workload: all right-hand sides in one preconditioned COCG solve."""
     prob = build_plate(R, w)
     dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
     op = R.Operator(prob, maxRhs=w["rhs"])
-    inner = R.Operator(prob, precision="single", maxRhs=w["rhs"])
-    pc = R.Preconditioner(prob, kernel="rChan", precision="single")
+    pc = R.Preconditioner(prob, kernel="rChan")
     if b is None:
         b = batch_rhs(R, prob, dirs, pols)
-    res = R.Solver(method="fgmres", innerMethod=w["method"] if w["method"] == "cg" else "fgmres",
-                   tolerance=w["tol"], restart=w["restart"], innerTolerance=w["inner_tol"], maxRefinements=40,
-                   maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc, nrhs=w["rhs"])
+    res = R.Solver(method=w["method"], tolerance=w["tol"], maxIterationCount=20000).solve(op, b, preconditioner=pc,
+                                                                                        nrhs=w["rhs"])
     return prob, res
 
 
@@ -217,13 +216,13 @@ def run_batched(args, w):
     t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
     n, N = w["n"], prob.rooftopCount()
     line = {
-        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, FP32 COCG inside FP64 refinement",
+        "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, rChan-preconditioned COCG, FP64",
         "value": w["rhs"] * args.steps / t, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64/c128", "data": "synthetic plate and 64 plane waves, seed 0",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic plate and 64 plane waves, seed 0",
         "config": {"workload": f"c4: {n}x{n} plate, cell lambda/{w['density']}, {N} unknowns, {w['rhs']} plane "
-                               f"waves theta U[0,80] phi U[0,360) TE/TM, FP32 COCG + FP32 rChan circulant inside FP64 "
-                               f"refinement to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
+                               f"waves theta U[0,80] phi U[0,360) TE/TM, COCG + rChan circulant, FP64, all right-hand "
+                               f"sides in one solve, to {w['tol']:g}", "unknowns": N, "rhs": w["rhs"],
                    "l2": "working set per batch re-created every step"},
         "iterations": its[0], "true_residual": res_max, "all_converged_to_tolerance": res_max <= w["tol"],
         "e2e": {"value": w["rhs"] * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 16 * N * w["rhs"],
@@ -510,18 +509,22 @@ def main():
         print(f"iterations {res.iterationCount()} residual {res.residualNorm():.3e} rcs {rcs:.6g}")
         return
 
-    # warm-up: context, FFT tables, kernels
-    for _ in range(args.warmup):
+    # warm-up: context, FFT tables, kernels; the clock sampler starts before the last warm-up step so that
+    # its start-up stays out of the timed region
+    for _ in range(max(0, args.warmup - 1)):
         solve_plate(R, w)
     torch.cuda.synchronize()
-
-    # timed region: K full solves with the inputs on the device
-    launches0 = L.launch_count()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    its, residuals = [], []
     with Clocks(local) as clk:
+        if args.warmup > 0:
+            solve_plate(R, w)
+        torch.cuda.synchronize()
+
+        # timed region: K full solves with the inputs on the device
+        launches0 = L.launch_count()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        its, residuals = [], []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         lat = []
