@@ -330,16 +330,17 @@ __global__ void __launch_bounds__(kRT) k_gm_v0(const T2* __restrict__ w, T2* __r
 
 // The rest of an Arnoldi step once ||w|| is known: the Hessenberg column, its previous rotations,
 // the new rotation, the rotated right-hand side, the history and the stopping tests (one thread).
-__device__ void arnoldi_finish(GmState& S, GmArrays& ar, int rhs, double s) {
+// col, cs, sn: the Hessenberg column being formed and the rotations, in global memory or staged in
+// shared memory by the caller with col already holding h (the rotation chain is sequential; staged, each
+// step costs a shared-memory access instead of a global one).
+__device__ void arnoldi_finish(GmState& S, GmArrays& ar, int rhs, double s, double2* col, double2* cs, double2* sn,
+                               bool staged) {
     const double sub = sqrt(s);
     const int m = ar.m, j = S.step;
-    double2* H = ar.H + (int64_t)rhs * (m + 1) * m;
     double2* g = ar.g + (int64_t)rhs * (m + 1);
-    double2* cs = ar.cs + (int64_t)rhs * m;
-    double2* sn = ar.sn + (int64_t)rhs * m;
     const double2* h = ar.h + (int64_t)rhs * (m + 1);
-    double2* col = H + (int64_t)j * (m + 1);
-    for (int k = 0; k <= j; ++k) col[k] = h[k];
+    if (!staged)
+        for (int k = 0; k <= j; ++k) col[k] = h[k];
     col[j + 1] = make_double2(sub, 0);
     for (int k = 0; k < j; ++k) {
         const double2 a0 = col[k], a1 = col[k + 1];
@@ -497,7 +498,11 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
     if (!arrive(&S.counter)) return;
     if (mode == 2) {
         const double tot = cta_total(part, gridDim.x).x;
-        if (threadIdx.x == 0) arnoldi_finish(S, ar, rhs, tot);
+        if (threadIdx.x == 0) {
+            const int m = ar.m;
+            arnoldi_finish(S, ar, rhs, tot, ar.H + ((int64_t)rhs * m + S.step) * (m + 1), ar.cs + (int64_t)rhs * m,
+                           ar.sn + (int64_t)rhs * m, false);
+        }
         return;
     }
     // One warp per column: lanes sum strided partials, then a shuffle tree (fixed order).
@@ -650,7 +655,26 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
     if (!arrive(&S.counter)) return;
     if (mode == 2) {
         const double tot = cta_total(part, gridDim.x).x;
-        if (threadIdx.x == 0) arnoldi_finish(S, ar, rhs, tot);
+        // stage h, the rotations and the column in shared memory; thread 0 runs the chain there
+        __shared__ double2 scol[kStreamCols + 1], scs[kStreamCols], ssn[kStreamCols];
+        const int m = ar.m, j = S.step;
+        const double2* h = ar.h + (int64_t)rhs * mc;
+        double2* cs = ar.cs + (int64_t)rhs * m;
+        double2* sn = ar.sn + (int64_t)rhs * m;
+        for (int k = threadIdx.x; k <= j; k += kRT) scol[k] = h[k];
+        for (int k = threadIdx.x; k < j; k += kRT) {
+            scs[k] = cs[k];
+            ssn[k] = sn[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) arnoldi_finish(S, ar, rhs, tot, scol, scs, ssn, true);
+        __syncthreads();
+        double2* col = ar.H + ((int64_t)rhs * m + j) * mc;
+        for (int k = threadIdx.x; k <= j + 1; k += kRT) col[k] = scol[k];
+        if (threadIdx.x == 0) {
+            cs[j] = scs[j];
+            sn[j] = ssn[j];
+        }
         return;
     }
     for (int k = warp; k < cols; k += NW) {
