@@ -37,8 +37,10 @@ WORKLOADS = {
                precision="double"),
     "c2": dict(n=256, density=20, theta=30.0, phi=0.0, pol="TE", method="gmres", tol=1e-6, restart=50,
                pc="blockJacobi", precision="double"),
+    # the inner FP32 FGMRES(30) is right-preconditioned by the FP32 rChan circulant (the reference's default
+    # preconditioner); the error against an FP64 GPU solve of the same plate is reported beside the line
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
-               pc=None, precision="mixed"),
+               pc="rChan", precision="mixed"),
     # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; COCG
     # preconditioned by the rChan circulant (the reference's default) in FP64 for all right-hand sides at
     # once. FP32 COCG inside FP64 refinement diverges on this plate (its FP32 recurrences break down
@@ -314,8 +316,9 @@ def solve_plate(R, w, rhs_host=None):
         inner = R.Operator(prob, precision="single")
         exc = R.Excitation.planeWave(prob, direction=d, polarization=p, device=rhs_host is None)
         b = rhs_host if rhs_host is not None else exc.vector()
+        pc = R.Preconditioner(prob, kernel=w["pc"], precision="single") if w["pc"] else None
         res = R.Solver(method="fgmres", tolerance=w["tol"], restart=w["restart"], innerTolerance=1e-4,
-                       maxIterationCount=20000).solve(op, b, innerOperator=inner)
+                       maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc)
     else:
         op = R.Operator(prob)
         pc = R.Preconditioner.blockJacobi(prob, (2, 2)) if w["pc"] == "blockJacobi" else None
@@ -326,6 +329,23 @@ def solve_plate(R, w, rhs_host=None):
     res._excitation = exc
     rcs = res.radarCrossSection()
     return prob, op, res, rcs
+
+
+def precision_error(R, w):
+    """The precision form's error: the mixed solve against an FP64 GPU solve of the same plate (FP64
+    right-preconditioned GMRES with the FP64 rChan circulant to a residual 100 times below the form's)."""
+    prob, op, res, rcs = solve_plate(R, w)
+    d, p = plane_wave_vectors(w["theta"], w["phi"], w["pol"])
+    exc = R.Excitation.planeWave(prob, direction=d, polarization=p, device=True)
+    pc = R.Preconditioner(prob, kernel=w["pc"] or "rChan")
+    ref = R.Solver(method="gmres", tolerance=w["tol"] / 100, restart=w["restart"], maxIterationCount=50000,
+                   side="right").solve(op, exc.vector(), preconditioner=pc)
+    ref._excitation = exc
+    x, x64 = res.solution(), ref.solution()
+    err = float((x - x64).norm() / x64.norm()) if hasattr(x, "norm") else float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
+    rcs64 = ref.radarCrossSection()
+    return {"current_rel": err, "rcs_rel": abs(rcs - rcs64) / abs(rcs64), "fp64_residual": ref.residualNorm(),
+            "fp64_iterations": ref.iterationCount(), "mixed_residual": res.residualNorm()}
 
 
 def roofline_matvec(R, w, steps, stream_ptr):
@@ -600,6 +620,8 @@ def main():
             "sample": f"oracle setup (assembly, spectra, preconditioner, plane wave) timed once, plus 20 iterations "
                       f"timed and scaled to the GPU solve's {its[0]} iterations: {t_setup:.2f} s + "
                       f"{its[0]} x {t_iter * 1e3:.1f} ms (extrapolated)"}
+    if rank == 0 and world == 1 and w["precision"] == "mixed":
+        line["error_vs_fp64"] = precision_error(R, w)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
