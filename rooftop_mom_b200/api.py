@@ -652,6 +652,27 @@ class Resources:
         return h.value
 
     @staticmethod
+    def check(mesh: Mesh, product="splitFFT", preconditioner=True, method="cg", restart=50, maxIterationCount=1000):
+        """Resources.check (Resources.m:73-141) for device memory: the bytes of a planned run, estimated before
+        anything is built, and rooftopMoM:resources:insufficientMemory if its peak does not fit below the
+        ceiling or into the device's free memory. The assembly's working memory ("chunk") is that of the
+        device assembly: 28 quadrant sums per far-lattice block and 7 moment terms per face pair offset."""
+        est = Resources.estimate(mesh, product, method, preconditioner, restart, maxIterationCount)
+        cx, cy = mesh.count()
+        report = {"generators": est["generators"],
+                  "chunk": 16.0 * (28 * (cx + 1) * (cy + 1) + 7 * cx * cy),
+                  "product": est["product"], "productWorking": est["productWorking"],
+                  "preconditioner": est["preconditioner"] if preconditioner else 0.0,
+                  "preconditionerWorking": est["preconditionerWorking"] if preconditioner else 0.0,
+                  "solver": est["solver"]}
+        # the assembly and the solve do not overlap; within the solve one product runs at a time
+        report["peak"] = max(report["generators"] + report["chunk"],
+                             report["generators"] + report["product"] + report["preconditioner"]
+                             + max(report["productWorking"], report["preconditionerWorking"]) + report["solver"])
+        L.call("rtm_budget_require", float(report["peak"]), identifier="rooftopMoM:resources:insufficientMemory")
+        return report
+
+    @staticmethod
     def estimate(mesh: Mesh, product="splitFFT", method="cg", preconditioner=True, restart=50, maxIterationCount=1000):
         out = (C.c_double * 6)()
         cx, cy = mesh.count()
