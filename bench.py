@@ -37,10 +37,11 @@ WORKLOADS = {
                precision="double"),
     "c2": dict(n=256, density=20, theta=30.0, phi=0.0, pol="TE", method="gmres", tol=1e-6, restart=50,
                pc="blockJacobi", precision="double"),
-    # the inner FP32 FGMRES(30) is right-preconditioned by the FP32 rChan circulant (the reference's default
-    # preconditioner); the error against an FP64 GPU solve of the same plate is reported beside the line
+    # the inner FP32 FGMRES(30) runs without a preconditioner (with the rChan circulant, restarted GMRES
+    # did not reach the tolerance within 20000 iterations on this plate); the error against an FP64 GPU
+    # solve of the same plate is reported beside the line
     "c3": dict(n=1024, density=15, theta=30.0, phi=0.0, pol="TE", method="fgmres", tol=1e-8, restart=30,
-               pc="rChan", precision="mixed"),
+               pc=None, precision="mixed"),
     # 64 plane waves, theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM ~ Bernoulli(1/2), seed 0; COCG
     # preconditioned by the rChan circulant (the reference's default) in FP64 for all right-hand sides at
     # once. FP32 COCG inside FP64 refinement diverges on this plate (its FP32 recurrences break down
@@ -333,13 +334,12 @@ def solve_plate(R, w, rhs_host=None):
 
 def precision_error(R, w):
     """The precision form's error: the mixed solve against an FP64 GPU solve of the same plate (FP64
-    right-preconditioned GMRES with the FP64 rChan circulant to a residual 100 times below the form's)."""
+    GMRES with the same restart to a residual 10 times below the form's)."""
     prob, op, res, rcs = solve_plate(R, w)
     d, p = plane_wave_vectors(w["theta"], w["phi"], w["pol"])
     exc = R.Excitation.planeWave(prob, direction=d, polarization=p, device=True)
-    pc = R.Preconditioner(prob, kernel=w["pc"] or "rChan")
-    ref = R.Solver(method="gmres", tolerance=w["tol"] / 100, restart=w["restart"], maxIterationCount=50000,
-                   side="right").solve(op, exc.vector(), preconditioner=pc)
+    ref = R.Solver(method="gmres", tolerance=w["tol"] / 10, restart=w["restart"], maxIterationCount=40000).solve(
+        op, exc.vector())
     ref._excitation = exc
     x, x64 = res.solution(), ref.solution()
     err = float((x - x64).norm() / x64.norm()) if hasattr(x, "norm") else float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
