@@ -14,6 +14,7 @@
 // consecutive elements). The line buffers are padded (row stride R2 + 1) against bank conflicts.
 #include "grid.h"
 #include "grid_args.cuh"
+#include "pdl.cuh"
 
 namespace rtm {
 namespace {
@@ -139,6 +140,8 @@ __global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_fw
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* sm = reinterpret_cast<T2*>(smem_raw);
+    griddep_wait();
+    griddep_launch_dependents();
     const int c = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
     const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
@@ -178,6 +181,8 @@ __global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_x_mi
     constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* sm = reinterpret_cast<T2*>(smem_raw);
+    griddep_wait();
+    griddep_launch_dependents();
     const int py = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
     const int t = threadIdx.x % R2, gid = threadIdx.x / R2;
@@ -261,6 +266,8 @@ __global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_in
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* sm = reinterpret_cast<T2*>(smem_raw);
+    griddep_wait();
+    griddep_launch_dependents();
     const int c = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
     const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
@@ -319,8 +326,10 @@ template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const
     }
     const int rows_max = a.rows[0] > a.rows[1] ? a.rows[0] : a.rows[1];
     const dim3 grid((rows_max + TI - 1) / TI, 2, nrhs);
-    if (fwd) k_fast_y_fwd<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<const T2*>(x));
-    else k_fast_y_inv<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<T2*>(y));
+    if (fwd)
+        RTM_CUDA(launch_dependent(k_fast_y_fwd<T, NQ>, grid, dim3(Fast<T>::threads), smem, s, a, static_cast<const T2*>(x)));
+    else
+        RTM_CUDA(launch_dependent(k_fast_y_inv<T, NQ>, grid, dim3(Fast<T>::threads), smem, s, a, static_cast<T2*>(y)));
     count_launch();
     return RTM_OK;
 }
@@ -336,7 +345,7 @@ template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaS
         attrs[dev & 63] = true;
     }
     const dim3 grid((a.Q + TEAMS - 1) / TEAMS, 2, nrhs);
-    k_fast_x_mix<T, NP><<<grid, Fast<T>::threads, smem, s>>>(a);
+    RTM_CUDA(launch_dependent(k_fast_x_mix<T, NP>, grid, dim3(Fast<T>::threads), smem, s, a));
     count_launch();
     return RTM_OK;
 }
