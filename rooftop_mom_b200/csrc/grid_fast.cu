@@ -327,7 +327,7 @@ template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const
     const int rows_max = a.rows[0] > a.rows[1] ? a.rows[0] : a.rows[1];
     const dim3 grid((rows_max + TI - 1) / TI, 2, nrhs);
     if (fwd)
-        RTM_CUDA(launch_dependent(k_fast_y_fwd<T, NQ>, grid, dim3(Fast<T>::threads), smem, s, a, static_cast<const T2*>(x)));
+        k_fast_y_fwd<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<const T2*>(x));
     else
         RTM_CUDA(launch_dependent(k_fast_y_inv<T, NQ>, grid, dim3(Fast<T>::threads), smem, s, a, static_cast<T2*>(y)));
     count_launch();

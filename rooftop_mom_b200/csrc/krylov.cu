@@ -23,7 +23,6 @@
 
 #include "fft.cuh"
 #include "krylov.h"
-#include "pdl.cuh"
 
 namespace rtm {
 
@@ -553,8 +552,6 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
     __shared__ double2 coef[kStreamCols];
     __shared__ double2 red[NW][KQ];
     T2* ws = reinterpret_cast<T2*>(smem_raw);  // [chunk]
-    griddep_wait();
-    griddep_launch_dependents();
     const int rhs = blockIdx.y;
     GmState& S = st[rhs];
     if (!S.active) return;
@@ -713,8 +710,8 @@ template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, in
     if (ar.m + 1 <= kStreamCols) {
         int blocks, chunk;
         stream_config(n, &blocks, &chunk);
-        launch_dependent(k_gm_orth_stream<T2>, dim3(blocks, nrhs), dim3(kRT), (size_t)chunk * sizeof(T2), s, V, w, n,
-                         nrhs, st, ar, mode, chunk);
+        k_gm_orth_stream<T2><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar, mode,
+                                                                                        chunk);
         count_launch();
         return;
     }
@@ -731,8 +728,6 @@ template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, in
 template <typename T2>
 __global__ void __launch_bounds__(kRT) k_gm_next(const T2* __restrict__ w, T2* __restrict__ V, int64_t n, int nrhs,
                                                  const GmState* st) {
-    griddep_wait();
-    griddep_launch_dependents();
     const int rhs = blockIdx.y;
     const GmState& S = st[rhs];
     if (!S.active) return;
@@ -1147,8 +1142,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
             launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 0, s);
             launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, s);
             launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 2, s);
-            launch_dependent(k_gm_next<T2>, grid, dim3(kRT), 0, s, (const T2*)w.as<T2>(), Vp, n, nrhs,
-                             (const GmState*)st);
+            k_gm_next<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
             count_launch(1);
         }
         launch_gm_solve(st, ar, nrhs, s);

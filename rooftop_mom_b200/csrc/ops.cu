@@ -12,7 +12,6 @@
 #include "fft.cuh"
 #include "grid.h"
 #include "ops.h"
-#include "pdl.cuh"
 
 namespace rtm {
 
@@ -174,8 +173,6 @@ template <typename T2>
 __global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, const int64_t* __restrict__ index,
                            const T2* __restrict__ inv, const T2* __restrict__ x, T2* __restrict__ y, int64_t n,
                            const int* skip, int stride) {
-    griddep_wait();
-    griddep_launch_dependents();
     const int rhs = blockIdx.y;
     if (skip && skip[(int64_t)rhs * stride]) return;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -199,15 +196,13 @@ struct BlockJacobi : LinearOp {
         const int64_t threads = (int64_t)nblocks * S;
         dim3 g((unsigned)((threads + 255) / 256), nrhs);
         if (precision == RTM_FP64)
-            RTM_CUDA(launch_dependent(k_bj_apply<double2>, g, dim3(256), 0, s, nblocks, S, (const int*)counts.as<int>(),
-                                      (const int64_t*)index.as<int64_t>(), (const double2*)inv.as<double2>(),
-                                      static_cast<const double2*>(x), static_cast<double2*>(y), n,
-                                      (const int*)skip.ptr, skip.stride));
+            k_bj_apply<double2><<<g, 256, 0, s>>>(nblocks, S, counts.as<int>(), index.as<int64_t>(), inv.as<double2>(),
+                                                  static_cast<const double2*>(x), static_cast<double2*>(y), n, skip.ptr,
+                                                  skip.stride);
         else
-            RTM_CUDA(launch_dependent(k_bj_apply<float2>, g, dim3(256), 0, s, nblocks, S, (const int*)counts.as<int>(),
-                                      (const int64_t*)index.as<int64_t>(), (const float2*)inv.as<float2>(),
-                                      static_cast<const float2*>(x), static_cast<float2*>(y), n,
-                                      (const int*)skip.ptr, skip.stride));
+            k_bj_apply<float2><<<g, 256, 0, s>>>(nblocks, S, counts.as<int>(), index.as<int64_t>(), inv.as<float2>(),
+                                                 static_cast<const float2*>(x), static_cast<float2*>(y), n, skip.ptr,
+                                                 skip.stride);
         count_launch();
         RTM_CUDA(cudaGetLastError());
         return RTM_OK;

@@ -1,4 +1,5 @@
-// Programmatic dependent launch (sm_90 and later): a kernel launched with the programmatic
+// Programmatic dependent launch (sm_90 and later), used inside the three kernels of a power-of-two product
+// (the x-mix and the y-inverse are launched as dependents): a kernel launched with the programmatic
 // stream-serialisation attribute may be scheduled while its predecessor on the stream is still running;
 // its CTAs then block in griddep_wait() until the predecessor has completed and its memory is visible.
 // Each kernel launched this way calls griddep_wait() before anything else (so it reads no data of its
