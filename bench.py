@@ -50,7 +50,7 @@ WORKLOADS = {
     "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=30, pc="rChan",
                precision="double", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
-    "c5": dict(n=0, density=0, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi", precision="double",
+    "c5": dict(n=0, density=0, seed=0, method="cg/gmres", tol=1e-6, restart=50, pc="rChan/blockJacobi", precision="double",
                theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
 }
 
@@ -105,7 +105,8 @@ def solve_batch(R, w, b=None):
 def serving_requests(R, count, seed):
     """The c5 request stream: faces Nx (and Ny) log-uniform in [16, 768]; with probability 1/2 a strip one
     face wide fed by a 1 V delta gap at its middle, else a plate under a random plane wave; cell lambda/N
-    with N ~ U[10, 25]; frequency ~ U[0.5, 3] GHz; GMRES(50) with block-Jacobi to 1e-6."""
+    with N ~ U[10, 25]; frequency ~ U[0.5, 3] GHz; to 1e-6 by rChan-preconditioned COCG where the face
+    grid admits the circulant, by block-Jacobi GMRES(50) elsewhere."""
     rng = np.random.default_rng(seed)
     lo, hi = math.log(16), math.log(768)
     out = []
@@ -117,7 +118,15 @@ def serving_requests(R, count, seed):
         f = rng.uniform(0.5e9, 3e9)
         h = SPEED_OF_LIGHT / f / cells
         k = 2 * math.pi * f / SPEED_OF_LIGHT
-        kw = dict(method="gmres", blockJacobi=True, tolerance=1e-6, restart=50, maxIterationCount=20000)
+        # COCG with the rChan circulant where the face grid allows it (no prime factor above the FFT plans'
+        # largest radix), block-Jacobi GMRES(50) elsewhere
+        from rooftop_mom_b200.server import circulant_supported
+
+        if circulant_supported(nx, ny):
+            kw = dict(method="cg", preconditioner="rChan", tolerance=1e-6, maxIterationCount=20000)
+        else:
+            kw = dict(method="gmres", preconditioner="blockJacobi", tolerance=1e-6, restart=50,
+                      maxIterationCount=20000)
         if strip:
             out.append(R.Request.deltaGap(nx, 1, h, h, k, portDirection="x", voltage=1.0, **kw))
         else:
@@ -168,7 +177,8 @@ def run_serving(args):
         "ms_per_step": span / len(reqs) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128" if prec == "double" else "c64/c128", "data": "synthetic request stream, seed 0",
         "config": {"workload": f"c5: {len(reqs)} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
-                               f"cell lambda/U[10,25], f U[0.5,3] GHz, GMRES(50) + block-Jacobi to 1e-6, "
+                               f"cell lambda/U[10,25], f U[0.5,3] GHz, COCG + rChan (or GMRES(50) + block-Jacobi "
+                               f"where the circulant's FFT sizes are not supported) to 1e-6, "
                                f"{args.serving_precision}", "slots": args.slots, "budget_bytes": 150e9,
                    "capacity_solves_per_s": capacity, "arrival_rate": rate},
         "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),

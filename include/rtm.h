@@ -268,7 +268,8 @@ typedef struct rtm_request {
     int port_direction;         /* delta gap: middle port across x (0) or y (1) rooftops */
     double voltage;             /* delta gap: gap voltage */
     int method;                 /* RTM_METHOD_CG or RTM_METHOD_GMRES (right-preconditioned) */
-    int block_jacobi;           /* nonzero: 2 x 2-face block-Jacobi preconditioner */
+    int preconditioner;         /* 0 none, 1 block-Jacobi over 2 x 2 faces, 2 rChan circulant (partwise); the
+                                   circulant needs face counts whose prime factors are at most 61 */
     double tolerance;
     int max_iterations;
     int restart;

@@ -64,7 +64,7 @@ class Request(C.Structure):
     _fields_ = [("count_x", C.c_int), ("count_y", C.c_int), ("size_x", C.c_double), ("size_y", C.c_double),
                 ("wavenumber", C.c_double), ("excitation", C.c_int), ("direction", C.c_double * 3),
                 ("polarization", C.c_double * 3), ("port_direction", C.c_int), ("voltage", C.c_double),
-                ("method", C.c_int), ("block_jacobi", C.c_int), ("tolerance", C.c_double),
+                ("method", C.c_int), ("preconditioner", C.c_int), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int), ("restart", C.c_int), ("keep_current", C.c_int)]
 
 

@@ -8,7 +8,7 @@
 // not hold back small ones behind it.
 //
 // Each slot is a host worker thread. An admitted request runs its whole pipeline on that thread with
-// the handles' own non-blocking streams: assembly, split-FFT product, block-Jacobi preconditioner,
+// the handles' own non-blocking streams: assembly, split-FFT product, preconditioner (block-Jacobi or rChan),
 // excitation on the device, the solve, the RCS or input impedance. Device work of different requests
 // overlaps; no call here synchronises the whole device. Results depend on the request alone, since
 // every launch shape follows from the request's sizes.
@@ -33,6 +33,7 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr int kBlockJacobiUnknowns = 8;  // packed unknowns a 2 x 2-face block of the block-Jacobi inverse (ops.cu)
+constexpr int kPcBlockJacobi = 1, kPcCirculant = 2;  // rtm_request.preconditioner
 
 struct Record {
     uint64_t id = 0;
@@ -55,6 +56,7 @@ int check_request(const rtm_request& q) {
         return fail(RTM_ERR_ARG, "unknown excitation");
     if (q.method != RTM_METHOD_CG && q.method != RTM_METHOD_GMRES) return fail(RTM_ERR_ARG, "unknown method");
     if (!(q.tolerance > 0) || q.max_iterations < 1 || q.restart < 1) return fail(RTM_ERR_ARG, "invalid solver");
+    if (q.preconditioner < 0 || q.preconditioner > kPcCirculant) return fail(RTM_ERR_ARG, "unknown preconditioner");
     return RTM_OK;
 }
 
@@ -62,14 +64,16 @@ int check_request(const rtm_request& q) {
 // solver vectors, excitation and solution), in the server's precision.
 int request_bytes(const rtm_request& q, int precision, double* bytes) {
     double est[6];
-    RTM_TRY(rtm_estimate_bytes(q.count_x, q.count_y, RTM_PRODUCT_SPLIT, q.method, q.block_jacobi != 0, q.restart,
+    RTM_TRY(rtm_estimate_bytes(q.count_x, q.count_y, RTM_PRODUCT_SPLIT, q.method, q.preconditioner != 0, q.restart,
                                q.max_iterations, est));
     const double n = (double)(q.count_x - 1) * q.count_y + (double)q.count_x * (q.count_y - 1);
     const double blocks = (double)((q.count_x + 1) / 2) * ((q.count_y + 1) / 2);
-    const double bj = q.block_jacobi
-                          ? blocks * (kBlockJacobiUnknowns * kBlockJacobiUnknowns * 16.0 + kBlockJacobiUnknowns * 8.0 + 4)
-                          : 0;
-    double total = est[0] + est[1] + est[2] + bj + est[5] + 2 * 16 * n;
+    double pc = 0;
+    if (q.preconditioner == kPcBlockJacobi)
+        pc = blocks * (kBlockJacobiUnknowns * kBlockJacobiUnknowns * 16.0 + kBlockJacobiUnknowns * 8.0 + 4);
+    else if (q.preconditioner == kPcCirculant)
+        pc = est[3] + est[4];
+    double total = est[0] + est[1] + est[2] + pc + est[5] + 2 * 16 * n;
     if (precision == RTM_FP32) total += 0.5 * (est[1] + est[2] + est[5]) + 4 * 16 * n;  // inner FP32 copies
     *bytes = total;
     return RTM_OK;
@@ -161,9 +165,12 @@ struct rtm_server {
         RTM_TRY(rtm_generators_assemble(q.count_x, q.count_y, q.size_x, q.size_y, q.wavenumber, 16, 8, nullptr, &h.g));
         RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP64, 1, &h.op));
         if (mixed) RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP32, 1, &h.op32));
-        if (q.block_jacobi)
+        if (q.preconditioner == kPcBlockJacobi)
             RTM_TRY(rtm_preconditioner_create_block_jacobi(h.g, q.size_x, q.size_y, 2, 2, mixed ? RTM_FP32 : RTM_FP64,
                                                            &h.pc));
+        else if (q.preconditioner == kPcCirculant)
+            RTM_TRY(rtm_preconditioner_create(h.g, q.size_x, q.size_y, RTM_KERNEL_RCHAN, RTM_BUILDER_PARTWISE, nullptr,
+                                              mixed ? RTM_FP32 : RTM_FP64, &h.pc));
         const int64_t n = h.op->op->n;
         r.res.unknowns = n;
         cudaStream_t s = h.op->stream;

@@ -19,11 +19,29 @@ import numpy as np
 from . import _lib as L
 
 
+PRECONDITIONERS = {None: 0, "blockJacobi": 1, "rChan": 2}
+LARGEST_RADIX = 61  # the largest prime factor the FFT plans transform
+
+
+def circulant_supported(countX, countY):
+    """True when the rChan circulant can be built on the face grid: no prime factor of the face counts above
+    the largest radix of the FFT plans (the circulant's period is the face grid itself; it cannot pad)."""
+    def ok(n):
+        p = 2
+        while p * p <= n:
+            while n % p == 0:
+                n //= p
+            p += 1
+        return n <= LARGEST_RADIX
+    return ok(int(countX)) and ok(int(countY))
+
+
 class Request:
-    """One plate solve: grid, frequency, excitation and solver settings (rtm_request)."""
+    """One plate solve: grid, frequency, excitation and solver settings (rtm_request). preconditioner:
+    None, "blockJacobi" (2 x 2 faces) or "rChan" (the reference's default circulant)."""
 
     def __init__(self, countX, countY, sizeX, sizeY, wavenumber, excitation="planeWave", direction=(0, 0, -1),
-                 polarization=(1, 0, 0), portDirection="x", voltage=1.0, method="gmres", blockJacobi=True,
+                 polarization=(1, 0, 0), portDirection="x", voltage=1.0, method="gmres", preconditioner="blockJacobi",
                  tolerance=1e-6, maxIterationCount=10000, restart=50, keepCurrent=False):
         r = L.Request()
         r.count_x, r.count_y = int(countX), int(countY)
@@ -34,7 +52,7 @@ class Request:
         r.port_direction = {"x": 0, "y": 1}[portDirection]
         r.voltage = float(voltage)
         r.method = L.METHODS[method]
-        r.block_jacobi = int(bool(blockJacobi))
+        r.preconditioner = PRECONDITIONERS[preconditioner]
         r.tolerance = float(tolerance)
         r.max_iterations = int(maxIterationCount)
         r.restart = int(restart)

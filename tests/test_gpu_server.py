@@ -32,7 +32,7 @@ def _strip(cx, **kw):
 
 def _mix():
     return [_plate(32, 28), _strip(41), _plate(17, 29, method="cg"), _plate(48, 40), _strip(64, method="cg"),
-            _plate(20, 20, blockJacobi=False), _plate(36, 12)]
+            _plate(20, 20, preconditioner=None), _plate(36, 12)]
 
 
 def _rel(a, b):
@@ -123,3 +123,19 @@ def test_mixed_precision_server_stays_close_to_fp64():
     for a, b in zip(ref, mixed):
         assert b["state"] == "done" and b["converged"] and b["residual"] <= TOL
         assert _rel(b["current"], a["current"]) < 1e-5
+
+
+def test_a_circulant_request_equals_the_direct_cocg_solve():
+    import rooftop_mom_b200 as R
+
+    d, p = (0.5, 0.0, -math.sqrt(0.75)), (0.0, 1.0, 0.0)
+    with R.Server(maxActive=2) as srv:
+        served = srv.wait(srv.submit(_plate(32, 28, d=d, p=p, method="cg", preconditioner="rChan")))
+    prob = R.Problem(R.Mesh(32, 28, LAM / 20, LAM / 20), K)
+    op = R.Operator(prob)
+    pc = R.Preconditioner(prob, kernel="rChan")
+    exc = R.Excitation.planeWave(prob, direction=d, polarization=p)
+    res = R.Solver(method="cg", tolerance=TOL, maxIterationCount=10000).solve(op, exc, preconditioner=pc)
+    assert served["state"] == "done" and served["converged"]
+    assert served["iterations"] == res.iterationCount()
+    assert _rel(served["current"], res.solution()) < 1e-12
