@@ -41,7 +41,7 @@ template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rh
 
 
 // Power-of-two split products with register-resident line transforms (grid_fast.cu). Eligible when
-// both transform sizes are powers of two in [32, 1024] (FP64: [32, 256]) for a product that keeps both
+// both transform sizes are powers of two in [32, 1024] (FP64: [32, 512]) for a product that keeps both
 // y subbands. Returns RTM_OK after launching the three kernels.
 bool fast_split_eligible(int P, int Q, bool fp64);
 template <typename T>

@@ -19,10 +19,14 @@
 namespace rtm {
 namespace {
 
-// CTA size and CTAs per SM: FP32 256 threads x 2 (128 registers a thread), FP64 128 threads x 3 (170).
+// CTA size and CTAs per SM: FP32 256 threads x 2 (128 registers a thread), FP64 128 threads x 3 (170),
+// and for FP64 lines of 512 (32 values a thread) one CTA per SM (up to 255 registers, no spills).
 template <typename T> struct Fast {
     static constexpr int threads = sizeof(T) == 8 ? 128 : 256;
     static constexpr int blocks = sizeof(T) == 8 ? 3 : 2;
+};
+template <typename T, int N> struct FastBlocks {
+    static constexpr int value = (sizeof(T) == 8 && N >= 512) ? 1 : Fast<T>::blocks;
 };
 
 template <int N> struct Shape;
@@ -135,7 +139,7 @@ __device__ __forceinline__ void inv_second(T2 (&v)[Shape<N>::R1], int t, const T
 // l + TI (py + 2 t): consecutive threads take consecutive columns, so rows of TI elements are read
 // and written at once. W[py][c][k][i] = FFT_y(x_c(i, j) mod_y(j)^py).
 template <typename T, int NQ>
-__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) k_fast_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_fw
 // with the subband spectra (the two components of a group pair meet through shared memory), inverse
 // transform, demodulation, the sum over px, scaled by 1 / (PQ), in place in W.
 template <typename T, int NP>
-__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_x_mix(const GridArgs<T> a) {
+__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NP>::value)) k_fast_x_mix(const GridArgs<T> a) {
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, S = R1 / R2;
     constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_x_mi
 // y-inverse: TI columns of one component, a group per (column, y subband); inverse transform along y,
 // demodulation, the sum over py through shared memory, cropped into y.
 template <typename T, int NQ>
-__global__ void __launch_bounds__(Fast<T>::threads, Fast<T>::blocks) k_fast_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) k_fast_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -356,11 +360,9 @@ template <typename T> int dispatch_y(const GridArgs<T>& a, int nrhs, const void*
         case 64: return launch_y<T, 64>(a, nrhs, x, y, fwd, s);
         case 128: return launch_y<T, 128>(a, nrhs, x, y, fwd, s);
         case 256: return launch_y<T, 256>(a, nrhs, x, y, fwd, s);
+        case 512: return launch_y<T, 512>(a, nrhs, x, y, fwd, s);
         default:
-            if constexpr (sizeof(T) == 4) {
-                if (a.Q == 512) return launch_y<T, 512>(a, nrhs, x, y, fwd, s);
-                return launch_y<T, 1024>(a, nrhs, x, y, fwd, s);
-            }
+            if constexpr (sizeof(T) == 4) return launch_y<T, 1024>(a, nrhs, x, y, fwd, s);
             return fail(RTM_ERR_UNSUPPORTED, "transform size");
     }
 }
@@ -371,11 +373,9 @@ template <typename T> int dispatch_x(const GridArgs<T>& a, int nrhs, cudaStream_
         case 64: return launch_x<T, 64>(a, nrhs, s);
         case 128: return launch_x<T, 128>(a, nrhs, s);
         case 256: return launch_x<T, 256>(a, nrhs, s);
+        case 512: return launch_x<T, 512>(a, nrhs, s);
         default:
-            if constexpr (sizeof(T) == 4) {
-                if (a.P == 512) return launch_x<T, 512>(a, nrhs, s);
-                return launch_x<T, 1024>(a, nrhs, s);
-            }
+            if constexpr (sizeof(T) == 4) return launch_x<T, 1024>(a, nrhs, s);
             return fail(RTM_ERR_UNSUPPORTED, "transform size");
     }
 }
@@ -383,7 +383,7 @@ template <typename T> int dispatch_x(const GridArgs<T>& a, int nrhs, cudaStream_
 }  // namespace
 
 bool fast_split_eligible(int P, int Q, bool fp64) {
-    auto ok = [&](int n) { return n >= 32 && n <= (fp64 ? 256 : 1024) && (n & (n - 1)) == 0; };
+    auto ok = [&](int n) { return n >= 32 && n <= (fp64 ? 512 : 1024) && (n & (n - 1)) == 0; };
     return ok(P) && ok(Q);
 }
 
