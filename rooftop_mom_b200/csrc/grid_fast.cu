@@ -26,7 +26,7 @@ template <typename T> struct Fast {
     static constexpr int blocks = sizeof(T) == 8 ? 3 : 2;
 };
 template <typename T, int N> struct FastBlocks {
-    static constexpr int value = (sizeof(T) == 8 && N >= 512) ? 1 : Fast<T>::blocks;
+    static constexpr int value = (sizeof(T) == 8 && N >= 512) || (sizeof(T) == 4 && N >= 1024) ? 1 : Fast<T>::blocks;
 };
 
 template <int N> struct Shape;
