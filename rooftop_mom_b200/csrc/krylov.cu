@@ -568,30 +568,52 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
     double nrm = 0;
     __syncthreads();  // coef
     if (mode) {
-        for (int r = threadIdx.x; r < len; r += kRT) {
+        // two rows a thread at once (r and r + kRT): twice the loads in flight per batch of columns
+        for (int r = threadIdx.x; r < len; r += 2 * kRT) {
+            const int r2 = r + kRT;
+            const bool two = r2 < len;
             double2 v = to_d2(wr[r]);
+            double2 v2 = two ? to_d2(wr[r2]) : make_double2(0, 0);
             int k = 0;
             for (; k + 8 <= cols; k += 8) {
-                T2 t[8];
+                T2 t[8], t2[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) t[u] = Vr[(k + u) * col + r];
+                for (int u = 0; u < 8; ++u) {
+                    t[u] = Vr[(k + u) * col + r];
+                    t2[u] = two ? Vr[(k + u) * col + r2] : from_d2<T2>(make_double2(0, 0));
+                }
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const double2 p = dmul(to_d2(t[u]), coef[k + u]);
                     v.x -= p.x;
                     v.y -= p.y;
+                    const double2 p2 = dmul(to_d2(t2[u]), coef[k + u]);
+                    v2.x -= p2.x;
+                    v2.y -= p2.y;
                 }
             }
             for (; k < cols; ++k) {
                 const double2 p = dmul(to_d2(Vr[k * col + r]), coef[k]);
                 v.x -= p.x;
                 v.y -= p.y;
+                if (two) {
+                    const double2 p2 = dmul(to_d2(Vr[k * col + r2]), coef[k]);
+                    v2.x -= p2.x;
+                    v2.y -= p2.y;
+                }
             }
             const T2 vs = from_d2<T2>(v);
             wr[r] = vs;
             if (mode == 1) ws[r] = vs;
             const double2 vd = to_d2(vs);
             nrm += vd.x * vd.x + vd.y * vd.y;
+            if (two) {
+                const T2 vs2 = from_d2<T2>(v2);
+                wr[r2] = vs2;
+                if (mode == 1) ws[r2] = vs2;
+                const double2 vd2 = to_d2(vs2);
+                nrm += vd2.x * vd2.x + vd2.y * vd2.y;
+            }
         }
     } else {
         for (int r = threadIdx.x; r < len; r += kRT) ws[r] = wr[r];
