@@ -491,6 +491,8 @@ def main():
                     help="one untimed solve of the workload, no JSON line (the command profiler captures run)")
     ap.add_argument("--matvec", action="store_true",
                     help="only the product of the workload, applied --steps times (the command profiler captures run)")
+    ap.add_argument("--assembly", action="store_true",
+                    help="time the generator assembly of the workload's plate (FP64 GFLOP/s of the far lattice)")
     ap.add_argument("--requests", type=int, default=100, help="c5: requests in the stream (2000 in the full form)")
     ap.add_argument("--slots", type=int, default=8, help="c5: requests on the device at once")
     ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
@@ -528,6 +530,24 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.assembly:
+        n = w["n"]
+        h = 1.0 / w["density"]
+        times = []
+        for k in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            R.Problem(R.Mesh(n, n, h, h), 2 * math.pi).generators()
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        t = float(np.median(times))
+        # 120 FP64 flops per far-lattice kernel value (the 4 x 7 moment multiply-adds and the distance and
+        # phase), order_far^2 values per lattice block, (n + 1)^2 blocks
+        values = 8 * 8 * (n + 1) ** 2
+        print(f"assembly {n}x{n}: {t * 1e3:.2f} ms, {values / 1e6:.1f} M far-lattice values, "
+              f"{120 * values / t / 1e9:.0f} GFLOP/s FP64 (algorithmic)")
+        return
     if args.matvec:
         rf = roofline_matvec(R, w, args.steps, torch.cuda.current_stream().cuda_stream)
         print(f"product {rf['precision']} {rf['P']}x{rf['Q']}: {rf['seconds'] * 1e6:.1f} us, "
