@@ -149,7 +149,8 @@ def run_serving(args):
         warm = serving_requests(R, 4, 1)
         for r in [srv.submit(q) for q in warm]:
             srv.wait(r, release=True)
-        burst = reqs[: min(len(reqs), args.slots * 4)]
+        # capacity from a closed-loop burst of a tenth of the stream (at least four requests a slot)
+        burst = reqs[: min(len(reqs), max(args.slots * 4, len(reqs) // 10))]
         ids = [srv.submit(q) for q in burst]
         res = [srv.wait(r, release=True) for r in ids]
         span = max(x["finished"] for x in res) - min(x["submitted"] for x in res)
