@@ -534,6 +534,33 @@ class Result:
                C.byref(out))
         return out.value
 
+    def bistaticRadarCrossSection(self, directions, polarizations):
+        """Bistatic RCS (m^2) of the current for observation directions r (unit vectors from the plate to the
+        observer) and receive polarisations p (perpendicular to r): (k Z0)^2 |e_r^T J|^2 / (4 pi I^2), with
+        e_r the unit plane wave travelling along -r with polarisation p and I the incident intensity.
+        At r = -d, p = the incident polarisation it is the monostatic radarCrossSection
+        (computeRadarCrossSection.m:18-19); the reference's current code has no bistatic form (its
+        obsolete v1 had a far-field pattern), so this one rests on that identity and on reciprocity."""
+        p_inc = self._parameters("planeWave")
+        prob = self._excitation.problem()
+        dirs = np.atleast_2d(np.asarray(directions, dtype=np.float64))
+        pols = np.atleast_2d(np.asarray(polarizations, dtype=np.float64))
+        if dirs.shape != pols.shape or dirs.shape[1] != 3:
+            raise _err("rooftopMoM:result:invalidDirections", "Directions and polarizations are matching 3-vectors.")
+        device = _is_device(self._x)
+        xp, where, keep = _vec_in(self._x, prob.rooftopCount())
+        # intensity' = sqrt(I): the ABI divides by intensity'^4 = I^2 for a unit receive wave
+        scale = math.sqrt(p_inc["intensity"])
+        out = np.empty(len(dirs))
+        for i, (r, p) in enumerate(zip(dirs, pols)):
+            e = Excitation.planeWave(prob, direction=-r, polarization=p, device=device).vector()
+            ep, _, keep_e = _vec_in(e, prob.rooftopCount())
+            v = C.c_double()
+            L.call("rtm_radar_cross_section", prob.wavenumber(), ep, xp, prob.rooftopCount(), scale, where,
+                   C.byref(v))
+            out[i] = v.value
+        return out
+
     def normalizedRadarCrossSection(self):
         wavelength = 2 * math.pi / self._excitation.problem().wavenumber()
         return self.radarCrossSection() / wavelength**2

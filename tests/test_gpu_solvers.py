@@ -196,3 +196,45 @@ def test_mixed_cocg_with_a_circulant_solves_several_right_hand_sides():
         assert r.converged() and r.residualNorm() <= 1e-6
         single = R.Solver(method="cg", tolerance=1e-10, maxIterationCount=5000).solve(op64, b[k * n:(k + 1) * n])
         assert rel(r.solution(), single.solution()) < 1e-4
+
+
+def _wave(theta, phi):
+    t, p = np.radians(theta), np.radians(phi)
+    d = np.array([np.sin(t) * np.cos(p), np.sin(t) * np.sin(p), -np.cos(t)])
+    return d, np.array([-np.sin(p), np.cos(p), 0.0])  # TE
+
+
+def test_bistatic_rcs_at_backscatter_is_the_monostatic_one_and_matches_its_definition():
+    import rooftop_mom_b200 as R
+    from oracle import excitation as EX, geometry as G
+
+    prob = R.Problem(R.Mesh(24, 20, 1 / 20, 1 / 20), 2 * np.pi)
+    d, p = _wave(30, 40)
+    exc = R.Excitation.planeWave(prob, direction=d, polarization=p)
+    res = R.Solver(method="gmres", tolerance=1e-10, restart=50, maxIterationCount=3000).solve(R.Operator(prob), exc)
+    mono = res.radarCrossSection()
+    assert res.bistaticRadarCrossSection([-d], [p])[0] == pytest.approx(mono, rel=1e-12)
+    # another observation direction against the formula on the oracle's receive wave
+    r, q = _wave(60, 200)
+    r = -r  # observe towards the source side of that wave
+    rt = G.Rooftops(24, 20, 1 / 20, 1 / 20, 8)
+    er = EX.plane_wave(rt, 2 * np.pi, -r, q, 1.0)
+    kz = 2 * np.pi * 376.730313668
+    want = kz**2 * abs(er @ res.solution()) ** 2 / (4 * np.pi)
+    assert res.bistaticRadarCrossSection([r], [q])[0] == pytest.approx(want, rel=1e-10)
+
+
+def test_bistatic_rcs_is_reciprocal():
+    """Swapping incidence and observation (same polarisations) leaves the bistatic RCS unchanged: the
+    Green's matrix is complex symmetric, e_B^T Z^-1 e_A = e_A^T Z^-1 e_B."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(24, 20, 1 / 20, 1 / 20), 2 * np.pi)
+    op = R.Operator(prob)
+    (dA, pA), (dB, pB) = _wave(20, 10), _wave(55, 130)
+    solver = R.Solver(method="gmres", tolerance=1e-11, restart=60, maxIterationCount=4000)
+    rA = solver.solve(op, R.Excitation.planeWave(prob, direction=dA, polarization=pA))
+    rB = solver.solve(op, R.Excitation.planeWave(prob, direction=dB, polarization=pB))
+    sAB = rA.bistaticRadarCrossSection([-dB], [pB])[0]
+    sBA = rB.bistaticRadarCrossSection([-dA], [pA])[0]
+    assert sAB == pytest.approx(sBA, rel=1e-8)
