@@ -630,11 +630,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
 }
 
 static int run_gen(GenArgs& a, cudaStream_t s) {
-    static bool attrs = false;
-    if (!attrs) {
-        cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attrs = true;
+    static bool attrs[64] = {};  // per device: the attribute belongs to the device's context
+    int dev = 0;
+    RTM_CUDA(cudaGetDevice(&dev));
+    if (!attrs[dev & 63]) {
+        RTM_CUDA(cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        RTM_CUDA(cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attrs[dev & 63] = true;
     }
     if (a.nitems == 0) return RTM_OK;
     a.ti = 4;
@@ -1075,11 +1077,13 @@ struct TwoSidedSpectra {
 };
 
 static int line_conv(const TwoSidedSpectra& t, int dim, const double2* K, double2* v, cudaStream_t s) {
-    static bool attrs = false;
-    if (!attrs) {
-        cudaFuncSetAttribute(k_line_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(k_line_conv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attrs = true;
+    static bool attrs[64] = {};  // per device
+    int dev = 0;
+    RTM_CUDA(cudaGetDevice(&dev));
+    if (!attrs[dev & 63]) {
+        RTM_CUDA(cudaFuncSetAttribute(k_line_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        RTM_CUDA(cudaFuncSetAttribute(k_line_conv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attrs[dev & 63] = true;
     }
     if (dim == 0) {
         const size_t smem = (size_t)(sk(t.P - 1) + 1) * sizeof(double2);
