@@ -184,6 +184,8 @@ __global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, c
     const T2* col = inv + (int64_t)blk * S * S + r;
     const T2* xr = x + rhs * n;
     T2 acc = czero<T2>();
+    // unrolled so that the loads of all columns are in flight together (the order of the sum is unchanged)
+#pragma unroll 8
     for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
     y[rhs * n + idx[r]] = acc;
 }
