@@ -14,6 +14,8 @@
  *   - `where` says whether a pointer is host (RTM_HOST) or device (RTM_DEVICE) memory. Host
  *     arguments are copied in and out inside the call.
  *   - `stream` is a cudaStream_t passed as void*; NULL means the library's own stream of the handle.
+ *   - `nrhs`, the vectors of one batched call, is 1 to 65535 (RTM_ERR_ARG below, RTM_ERR_SIZE above):
+ *     the batched kernels span the vectors in one grid dimension.
  *   - Every call returns an rtm_status; rtm_last_error() gives the message of the last failure on
  *     the calling thread. Nothing here aborts the process or falls back to the CPU.
  */

@@ -55,6 +55,14 @@ int check_where(int where) {
     return RTM_OK;
 }
 
+// Right-hand sides of one call: the batched launches span them in a grid's y or z dimension.
+constexpr int kMaxRhs = 65535;
+int check_rhs(int nrhs) {
+    if (nrhs < 1) return fail(RTM_ERR_ARG, "nrhs must be positive");
+    if (nrhs > kMaxRhs) return fail(RTM_ERR_SIZE, "at most 65535 right-hand sides in one call");
+    return RTM_OK;
+}
+
 // Input vectors of an operator call as device pointers in the operator's precision.
 // Staging blocks go back to the allocator's cache when these leave scope, so any copy or kernel
 // still using them on the call's stream is waited for first.
@@ -328,7 +336,7 @@ int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int 
     if (!op || !x || !y) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
     if (n != op->op->n) return fail(RTM_ERR_SIZE, "The input must be a numeric " + std::to_string(op->op->n) + "x1 vector.");
-    if (nrhs < 1) return fail(RTM_ERR_ARG, "nrhs must be positive");
+    RTM_TRY(check_rhs(nrhs));
     cudaStream_t s = pick(stream, op->stream);
     RTM_TRY(op->op->reserve(nrhs));
     Staged in;
@@ -347,6 +355,7 @@ int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void* x, void
     if (!op || !x || !y) return fail(RTM_ERR_ARG, "null argument");
     if (!op->grid) return fail(RTM_ERR_UNSUPPORTED, "the fixed scratch serves FFT products only");
     if (n != op->op->n) return fail(RTM_ERR_SIZE, "The input must be a numeric " + std::to_string(op->op->n) + "x1 vector.");
+    RTM_TRY(check_rhs(nrhs));
     cudaStream_t s = pick(stream, op->stream);
     RTM_TRY(apply_fixed_scratch(*op->grid, x, y, nrhs, s));
     if (!stream) RTM_CUDA(cudaStreamSynchronize(s));
@@ -433,6 +442,7 @@ int rtm_preconditioner_apply(rtm_preconditioner* pc, const void* x, void* y, int
     if (!pc || !x || !y) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
     if (n != pc->op->n) return fail(RTM_ERR_SIZE, "The input must be a numeric " + std::to_string(pc->op->n) + "x1 vector.");
+    RTM_TRY(check_rhs(nrhs));
     cudaStream_t s = pick(stream, pc->stream);
     RTM_TRY(pc->op->reserve(nrhs));
     Staged in;
@@ -478,7 +488,7 @@ int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_config* 
     if (!op || !b || !x) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_config(config));
     RTM_TRY(check_where(where));
-    if (nrhs < 1) return fail(RTM_ERR_ARG, "nrhs must be positive");
+    RTM_TRY(check_rhs(nrhs));
     if (n != op->op->n) return fail(RTM_ERR_SIZE, "The operator does not match the " + std::to_string(n) +
                                                       " unknowns of the right-hand side.");
     if (pc && pc->op->n != n) return fail(RTM_ERR_SIZE, "The preconditioner does not match the " + std::to_string(n) +
@@ -531,6 +541,7 @@ int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner
     if (!op || !inner_op || !b || !x) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_config(config));
     RTM_TRY(check_where(where));
+    RTM_TRY(check_rhs(nrhs));
     if (op->op->precision != RTM_FP64 || inner_op->op->precision != RTM_FP32)
         return fail(RTM_ERR_ARG, "the outer operator is FP64 and the inner one FP32");
     if (inner_pc && inner_pc->op->precision != RTM_FP32) return fail(RTM_ERR_ARG, "the inner preconditioner is FP32");
@@ -572,7 +583,8 @@ int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner
 int rtm_plane_wave(int count_x, int count_y, double size_x, double size_y, int order, double wavenumber,
                    const double* directions, const double* polarizations, const double* intensities, int nrhs,
                    void* out, int where, void* stream) {
-    if (!directions || !polarizations || !intensities || !out || nrhs < 1) return fail(RTM_ERR_ARG, "null argument");
+    if (!directions || !polarizations || !intensities || !out) return fail(RTM_ERR_ARG, "null argument");
+    RTM_TRY(check_rhs(nrhs));
     RTM_TRY(check_where(where));
     if (count_x < 1 || count_y < 1 || order < 1) return fail(RTM_ERR_ARG, "invalid grid or order");
     CallStream own;

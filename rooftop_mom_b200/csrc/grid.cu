@@ -285,21 +285,20 @@ __global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_strip(c
 }
 
 // --------------------------------------------------------------------------------------------
-template <typename T, bool POW2> static void set_attrs_one() {
-    cudaFuncSetAttribute(k_grid_y_fwd<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_grid_x_mix<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_grid_y_inv<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_strip<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+template <typename T, bool POW2> static int set_attrs_one() {
+    RTM_CUDA(cudaFuncSetAttribute(k_grid_y_fwd<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RTM_CUDA(cudaFuncSetAttribute(k_grid_x_mix<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RTM_CUDA(cudaFuncSetAttribute(k_grid_y_inv<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RTM_CUDA(cudaFuncSetAttribute(k_strip<T, POW2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    return RTM_OK;
 }
 
-template <typename T> static void set_smem_attrs() {
-    static bool done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (done[dev & 63]) return;
-    set_attrs_one<T, true>();
-    set_attrs_one<T, false>();
-    done[dev & 63] = true;
+template <typename T> static int set_smem_attrs() {
+    static DeviceOnce once;
+    return once([]() -> int {
+        RTM_TRY((set_attrs_one<T, true>()));
+        return set_attrs_one<T, false>();
+    });
 }
 
 // Shared stride of the lines of a CTA that transforms `lines` lines of length n in place: room for
@@ -325,7 +324,7 @@ template <typename T>
 static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip,
                    void* work) {
     using T2 = typename Cx<T>::T2;
-    set_smem_attrs<T>();
+    RTM_TRY(set_smem_attrs<T>());
     const T2* x = static_cast<const T2*>(xv);
     T2* y = static_cast<T2*>(yv);
     GridArgs<T> a{};
@@ -425,7 +424,7 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
 
 int GridApplicator::reserve(int nrhs) {
     // kernel attributes are set here, outside of any stream capture
-    if (precision == RTM_FP64) set_smem_attrs<double>(); else set_smem_attrs<float>();
+    RTM_TRY(precision == RTM_FP64 ? set_smem_attrs<double>() : set_smem_attrs<float>());
     if (nrhs <= max_rhs && (mode == kStrip || work.bytes >= work_bytes_per_rhs() * (size_t)nrhs)) return RTM_OK;
     if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
     max_rhs = std::max(max_rhs, nrhs);
@@ -630,14 +629,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) k_gen_x(const GenArgs a) {
 }
 
 static int run_gen(GenArgs& a, cudaStream_t s) {
-    static bool attrs[64] = {};  // per device: the attribute belongs to the device's context
-    int dev = 0;
-    RTM_CUDA(cudaGetDevice(&dev));
-    if (!attrs[dev & 63]) {
+    static DeviceOnce once;
+    RTM_TRY(once([]() -> int {
         RTM_CUDA(cudaFuncSetAttribute(k_gen_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         RTM_CUDA(cudaFuncSetAttribute(k_gen_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attrs[dev & 63] = true;
-    }
+        return RTM_OK;
+    }));
     if (a.nitems == 0) return RTM_OK;
     a.ti = 4;
     while (a.ti > 1 && ((size_t)a.ti * (sk(a.Q - 1) + 1) * sizeof(double2) > (size_t)kSmemBudget ||
@@ -1077,14 +1074,12 @@ struct TwoSidedSpectra {
 };
 
 static int line_conv(const TwoSidedSpectra& t, int dim, const double2* K, double2* v, cudaStream_t s) {
-    static bool attrs[64] = {};  // per device
-    int dev = 0;
-    RTM_CUDA(cudaGetDevice(&dev));
-    if (!attrs[dev & 63]) {
+    static DeviceOnce once;
+    RTM_TRY(once([]() -> int {
         RTM_CUDA(cudaFuncSetAttribute(k_line_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         RTM_CUDA(cudaFuncSetAttribute(k_line_conv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attrs[dev & 63] = true;
-    }
+        return RTM_OK;
+    }));
     if (dim == 0) {
         const size_t smem = (size_t)(sk(t.P - 1) + 1) * sizeof(double2);
         const int thr = fft_threads(1, t.tP->plan);

@@ -320,14 +320,12 @@ template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const
     using T2 = typename Cx<T>::T2;
     constexpr int TI = Fast<T>::threads / (2 * Shape<NQ>::R2);
     const size_t smem = y_smem<T, NQ>();
-    static bool attrs[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!attrs[dev & 63]) {
+    static DeviceOnce once;
+    RTM_TRY(once([smem]() -> int {
         RTM_CUDA(cudaFuncSetAttribute(k_fast_y_fwd<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         RTM_CUDA(cudaFuncSetAttribute(k_fast_y_inv<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attrs[dev & 63] = true;
-    }
+        return RTM_OK;
+    }));
     const int rows_max = a.rows[0] > a.rows[1] ? a.rows[0] : a.rows[1];
     const dim3 grid((rows_max + TI - 1) / TI, 2, nrhs);
     if (fwd)
@@ -341,13 +339,11 @@ template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const
 template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
     constexpr int TEAMS = Fast<T>::threads / (4 * Shape<NP>::R2);
     const size_t smem = x_smem<T, NP>();
-    static bool attrs[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!attrs[dev & 63]) {
+    static DeviceOnce once;
+    RTM_TRY(once([smem]() -> int {
         RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attrs[dev & 63] = true;
-    }
+        return RTM_OK;
+    }));
     const dim3 grid((a.Q + TEAMS - 1) / TEAMS, 2, nrhs);
     RTM_CUDA(launch_dependent(k_fast_x_mix<T, NP>, grid, dim3(Fast<T>::threads), smem, s, a));
     count_launch();

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,7 @@ namespace rtm {
 void set_error(const std::string& msg);
 int fail(int status, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+inline int check_cuda(cudaError_t e, const char* what) { return e == cudaSuccess ? RTM_OK : cuda_fail(e, what); }
 
 #define RTM_CUDA(call)                                        \
     do {                                                      \
@@ -31,6 +33,23 @@ int cuda_fail(cudaError_t e, const char* what);
 
 extern int64_t g_launches;  // launches of this library's kernels (incremented by the launchers)
 inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (int64_t)n, __ATOMIC_RELAXED); }
+
+// One-time set-up per device, such as kernel attributes, which belong to the device's context. Host
+// threads that reach the same device's set-up together may both run it, so the set-up must be
+// idempotent; the flags are atomic, so that race is well defined. The flag is set only when the
+// set-up succeeds. Ordinals above 63 run the set-up on every call.
+struct DeviceOnce {
+    std::atomic<bool> done[64] = {};
+    template <typename F> int operator()(F&& setup) {
+        int dev = 0;
+        RTM_CUDA(cudaGetDevice(&dev));
+        const bool tracked = dev >= 0 && dev < 64;
+        if (tracked && done[dev].load(std::memory_order_acquire)) return RTM_OK;
+        RTM_TRY(setup());
+        if (tracked) done[dev].store(true, std::memory_order_release);
+        return RTM_OK;
+    }
+};
 
 // ---------------------------------------------------------------------------------------------
 // Budget ledger of device bytes (Budget.m). Thread-safe.

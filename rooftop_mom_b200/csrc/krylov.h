@@ -1,6 +1,7 @@
 // Iterative solvers on the device (krylov.cu, mixed.cu).
 #pragma once
 
+#include <atomic>
 #include <vector>
 
 #include "ops.h"
@@ -16,7 +17,7 @@ struct SolveConfig {
     double inner_tolerance = 1e-4;
     int max_refinements = 20;
     int right_preconditioned = 0;  // GMRES: 0 left (the reference's form), 1 right (flexible)
-    const volatile int* cancel = nullptr;  // nonzero: stop at the next host check (unconverged result)
+    const std::atomic<int>* cancel = nullptr;  // nonzero: stop at the next host check (unconverged result)
 };
 
 struct SolveResult {

@@ -244,16 +244,22 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
     if ((*status = index16.alloc(nb * kMaxBlockUnknowns * sizeof(int64_t))) != RTM_OK) return nullptr;
     if ((*status = inv64.alloc(nb * kMaxBlockUnknowns * kMaxBlockUnknowns * sizeof(double2))) != RTM_OK) return nullptr;
     if ((*status = flag.alloc(sizeof(int))) != RTM_OK) return nullptr;
-    cudaMemsetAsync(flag.ptr, 0, sizeof(int), s);
+    if ((*status = check_cuda(cudaMemsetAsync(flag.ptr, 0, sizeof(int), s), "block-Jacobi flag")) != RTM_OK)
+        return nullptr;
     g.counts = op->counts.as<int>();
     g.index = index16.as<int64_t>();
     g.inv = inv64.as<double2>();
     g.singular = flag.as<int>();
-    cudaFuncSetAttribute(k_bj_build, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    // a preference only: a device that declines it runs the build all the same
+    if (cudaFuncSetAttribute(k_bj_build, cudaFuncAttributePreferredSharedMemoryCarveout, 0) != cudaSuccess)
+        (void)cudaGetLastError();
     k_bj_build<<<(unsigned)((nb + 63) / 64), 64, 0, s>>>(g);
     count_launch();
+    if ((*status = check_cuda(cudaGetLastError(), "block-Jacobi build launch")) != RTM_OK) return nullptr;
     int bad = 0;
-    cudaMemcpyAsync(&bad, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if ((*status = check_cuda(cudaMemcpyAsync(&bad, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s),
+                              "block-Jacobi flag")) != RTM_OK)
+        return nullptr;
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         *status = cuda_fail(e, "block-Jacobi build");
@@ -277,7 +283,8 @@ std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double 
         k_bj_pack<float2><<<pb, 256, 0, s>>>(op->nblocks, S, inv64.as<double2>(), index16.as<int64_t>(),
                                              op->inv.as<float2>(), op->index.as<int64_t>());
     count_launch();
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
         *status = cuda_fail(e, "block-Jacobi packing");
         return nullptr;
     }

@@ -12,6 +12,7 @@
 // excitation on the device, the solve, the RCS or input impedance. Device work of different requests
 // overlaps; no call here synchronises the whole device. Results depend on the request alone, since
 // every launch shape follows from the request's sizes.
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -40,7 +41,23 @@ struct Record {
     rtm_request req{};
     rtm_request_result res{};
     std::vector<double> current;  // interleaved complex
-    volatile int cancel = 0;
+    std::atomic<int> cancel{0};  // set by rtm_server_cancel / destroy, read by the worker and the solver
+};
+
+// What a request's pipeline produces: the result fields it fills and the current it keeps.
+struct Outcome {
+    rtm_request_result res{};
+    std::vector<double> current;
+    void commit(rtm_request_result& to) const {
+        to.unknowns = res.unknowns;
+        to.solve_s = res.solve_s;
+        to.converged = res.converged;
+        to.iteration_count = res.iteration_count;
+        to.residual_norm = res.residual_norm;
+        to.rcs = res.rcs;
+        to.impedance[0] = res.impedance[0];
+        to.impedance[1] = res.impedance[1];
+    }
 };
 
 double seconds_since(Clock::time_point t0) {
@@ -129,10 +146,13 @@ struct rtm_server {
                 }
             }
             int st = RTM_OK;
-            if (r->res.state == RTM_REQUEST_RUNNING) st = run(*r);
+            Outcome out;
+            if (r->res.state == RTM_REQUEST_RUNNING) st = run(*r, out);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 if (r->res.state == RTM_REQUEST_RUNNING) {
+                    out.commit(r->res);
+                    r->current = std::move(out.current);
                     r->res.finished_s = seconds_since(epoch);
                     r->res.status = st;
                     r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
@@ -146,8 +166,9 @@ struct rtm_server {
         }
     }
 
-    // The whole pipeline of one request on this thread.
-    int run(Record& r) {
+    // The whole pipeline of one request on this thread. Its results go to `out`, which the worker
+    // copies into the record under the lock, so a concurrent poll never sees them half written.
+    int run(const Record& r, Outcome& out) {
         const rtm_request& q = r.req;
         struct Handles {
             rtm_generators* g = nullptr;
@@ -172,7 +193,7 @@ struct rtm_server {
             RTM_TRY(rtm_preconditioner_create(h.g, q.size_x, q.size_y, RTM_KERNEL_RCHAN, RTM_BUILDER_PARTWISE, nullptr,
                                               mixed ? RTM_FP32 : RTM_FP64, &h.pc));
         const int64_t n = h.op->op->n;
-        r.res.unknowns = n;
+        out.res.unknowns = n;
         cudaStream_t s = h.op->stream;
         DeviceBuffer b, x;
         StreamSyncGuard guard(s);
@@ -215,20 +236,20 @@ struct rtm_server {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (st != RTM_OK) return st;
-        r.res.solve_s = ms * 1e-3;
+        out.res.solve_s = ms * 1e-3;
         if (!res.stats.empty()) {
-            r.res.converged = res.stats[0].converged;
-            r.res.iteration_count = res.stats[0].iteration_count;
-            r.res.residual_norm = res.stats[0].residual_norm;
+            out.res.converged = res.stats[0].converged;
+            out.res.iteration_count = res.stats[0].iteration_count;
+            out.res.residual_norm = res.stats[0].residual_norm;
         }
         if (q.excitation == RTM_EXCITE_PLANE_WAVE)
-            RTM_TRY(rtm_radar_cross_section(q.wavenumber, b.ptr, x.ptr, n, 1.0, RTM_DEVICE, &r.res.rcs));
+            RTM_TRY(rtm_radar_cross_section(q.wavenumber, b.ptr, x.ptr, n, 1.0, RTM_DEVICE, &out.res.rcs));
         else
             RTM_TRY(rtm_input_impedance(q.count_x, q.count_y, q.size_x, q.size_y, x.ptr, port.data(), (int)port.size(),
-                                        q.voltage, RTM_DEVICE, r.res.impedance));
+                                        q.voltage, RTM_DEVICE, out.res.impedance));
         if (q.keep_current) {
-            r.current.resize((size_t)2 * n);
-            RTM_CUDA(cudaMemcpyAsync(r.current.data(), x.ptr, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+            out.current.resize((size_t)2 * n);
+            RTM_CUDA(cudaMemcpyAsync(out.current.data(), x.ptr, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, s));
             RTM_CUDA(cudaStreamSynchronize(s));
         }
         return RTM_OK;

@@ -57,6 +57,22 @@ def test_version_and_errors_without_a_gpu(library):
     assert "invalid grid" in _lib.last_error()
 
 
+def test_batched_calls_bound_the_vector_count(library):
+    """A batched call takes 1 to 65535 vectors; the count is checked before any device work."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    dummy = (C.c_double * 3)(0.0, 0.0, -1.0)
+    sink = (C.c_double * 2)()
+    args = (8, 8, 0.05, 0.05, 8, 6.283185307179586, dummy, dummy, dummy)
+    assert lib.rtm_plane_wave(*args, 65536, sink, _lib.HOST, None) == _lib.ERR_SIZE
+    assert "65535" in _lib.last_error()
+    assert lib.rtm_plane_wave(*args, 0, sink, _lib.HOST, None) == _lib.ERR_ARG
+    assert "positive" in _lib.last_error()
+
+
 def test_byte_models_match_the_oracle(library):
     import ctypes as C
 
