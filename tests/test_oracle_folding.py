@@ -1,9 +1,10 @@
 """The oracle's circulant building blocks against their definitions, restating the reference's unit tests
 tests/+unit/+assembler/+preconditioner/+utils/FoldGeneratorTest.m:5-45, ExtendEvenlyTest.m:5-15,
-GeneratePartSpectraTest.m:9-28 and GenerateOptimalOfProductTest.m:9-24: folding puts the windowed
-offset p of a count-n direction at p mod n, the even extension mirrors both offsets, the four part
-spectra sum to the two-level Toeplitz matrix, and the optimal circulant of a product keeps the
-diagonal of the product in the Fourier basis."""
+GeneratePartSpectraTest.m:9-28, GenerateOptimalOfProductTest.m:9-24 and
++kernels/KernelsTest.m:36-104: folding puts the windowed offset p of a count-n direction at p mod n, the
+even extension mirrors both offsets, the four part spectra sum to the two-level Toeplitz matrix, the
+optimal circulant of a product keeps the diagonal of the product in the Fourier basis, and each kernel
+places and weights the offsets as its window says."""
 from __future__ import annotations
 
 import numpy as np
@@ -105,3 +106,57 @@ def test_optimal_of_a_product_keeps_the_fourier_diagonal(grid):
     product = _toeplitz(ga) @ _toeplitz(gb).conj().T
     want = np.diag(F @ product @ F.conj().T).reshape(grid, order="F")
     np.testing.assert_allclose(got, want, atol=1e-12 * np.abs(want).max())
+
+
+# The kernels (tests/+unit/+assembler/+preconditioner/+kernels/KernelsTest.m:36-104), on the even extension
+# of one-sided generators with integer entries, so every sum is exact.
+def _one_sided(rows, cols):
+    return np.arange(1.0, rows * cols + 1).reshape(rows, cols, order="F")
+
+
+@pytest.mark.parametrize("kernel", [PC.t_chan, PC.r_chan])
+@pytest.mark.parametrize("grid", [(5, 4), (1, 6), (7, 1)])
+def test_t_chan_and_r_chan_fold_an_even_generator_one_sided(kernel, grid):
+    g = np.random.default_rng(1)
+    gen = g.standard_normal(grid) + 1j * g.standard_normal(grid)
+    np.testing.assert_allclose(kernel(gen, even=True), kernel(PC.extend_evenly(gen)), atol=1e-14)
+    assert kernel(None, even=True) is None
+
+
+def test_strang_copies_the_central_offsets():
+    g = _one_sided(5, 4)
+    c = PC.strang(PC.extend_evenly(g))
+    np.testing.assert_array_equal(c[:3, :3], g[:3, :3])
+    np.testing.assert_array_equal(c[3:5, 0], g[[2, 1], 0])  # offsets -2 and -1 wrap to 3 and 4
+    assert c[0, 3] == g[0, 1]  # along a count of 4, offset -1 wraps to 3
+
+
+def test_r_chan_adds_the_reflection_in_every_direction():
+    g = _one_sided(4, 3)
+    c = PC.r_chan(PC.extend_evenly(g))
+    assert c[0, 0] == g[0, 0]
+    assert c[1, 0] == g[1, 0] + g[3, 0]
+    assert c[0, 1] == g[0, 1] + g[0, 2]
+    assert c[1, 1] == g[1, 1] + g[3, 1] + g[1, 2] + g[3, 2]
+
+
+def test_huckle_with_unit_bandwidths_keeps_the_zero_offset():
+    g = _one_sided(5, 4)
+    want = np.zeros((5, 4))
+    want[0, 0] = g[0, 0]
+    np.testing.assert_array_equal(PC.huckle(PC.extend_evenly(g), 1, 1), want)
+
+
+def test_huckle_damps_and_wraps():
+    g = _one_sided(5, 4)
+    c = PC.huckle(PC.extend_evenly(g), 2, 1)
+    np.testing.assert_array_equal(c[[1, 4], 0], [0.5 * g[1, 0]] * 2)  # offset 1 damped by 1 - 1/2, at 1 and 4
+    np.testing.assert_array_equal(c[[2, 3], 0], [0, 0])
+
+
+def test_empty_generators_give_empty_circulants():
+    assert PC.strang(None) is None
+    assert PC.t_chan(None) is None
+    assert PC.r_chan(None) is None
+    assert PC.huckle(None, 2, 2) is None
+    assert PC.superoptimal(None) is None
