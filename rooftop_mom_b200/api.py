@@ -161,10 +161,12 @@ class Problem:
             wavenumber = electricalSize / mesh.radius()
         if not (math.isfinite(wavenumber) and wavenumber > 0):
             raise _err("rooftopMoM:problem:invalidWavenumber", "The wavenumber must be positive and finite.")
-        orders = np.atleast_1d(np.asarray(quadratureOrder))
+        orders = np.atleast_1d(np.asarray(quadratureOrder, dtype=np.float64))
         if orders.size not in (1, 2):
             raise _err("rooftopMoM:problem:invalidQuadratureOrder",
                        "The quadrature order is one order or a pair [near, far].")
+        if not np.all((orders >= 1) & (orders == np.floor(orders))):
+            raise _err("rooftopMoM:problem:invalidQuadratureOrder", "The quadrature orders are positive integers.")
         self._mesh = mesh
         self._k = float(wavenumber)
         self._orders = (int(orders[0]), int(orders[-1]))
@@ -173,6 +175,9 @@ class Problem:
     @staticmethod
     def fromElectricalSize(electricalSize, density=10, aspect=1, quadratureOrder=(16, 8), chunkSize=None):
         """Problem.m:159-206: the fewest faces reaching the density, rounded up to 7-smooth counts, k = 2 pi."""
+        for v, name in ((electricalSize, "electricalSize"), (density, "density"), (aspect, "aspect")):
+            if not (math.isfinite(v) and v > 0):
+                raise _err("rooftopMoM:problem:invalidArgument", f"The {name} must be positive and finite.")
         sides = np.array([aspect, 1.0]) * (electricalSize / math.pi) / math.hypot(aspect, 1.0)
         counts = np.maximum(1, np.ceil((1 - 4 * np.finfo(float).eps) * sides * density)).astype(int)
         counts = [fast_fft_size(c) for c in counts]

@@ -1,0 +1,110 @@
+"""The host side of the Python mirror of the MATLAB API, which needs no GPU until generators are assembled:
+Mesh and Problem as the reference's tests/+unit/MeshTest.m:5-29 and ProblemTest.m:5-16, :18-29 and
+:64-140 hold them. MATLAB's argument validators (MATLAB:validators:*) have no Python counterpart; the
+mirror raises RtmError with a rooftopMoM:* identifier for the same inputs."""
+from __future__ import annotations
+
+import math
+
+import pytest
+
+from rooftop_mom_b200 import Mesh, Problem, RtmError
+
+
+def test_mesh_getters():
+    mesh = Mesh(4, 3, 0.1, 0.2)
+    assert (*mesh.count(), *mesh.faceSize()) == (4, 3, 0.1, 0.2)
+
+
+def test_mesh_radius_is_half_the_diagonal():
+    assert Mesh(4, 3, 0.1, 0.2).radius() == pytest.approx(math.hypot(0.4, 0.6) / 2, rel=1e-15)
+
+
+@pytest.mark.parametrize("args", [(0, 3, 0.1, 0.1), (2.5, 3, 0.1, 0.1), (4, 3, -0.1, 0.1), (4, 3, 0.1, math.inf)])
+def test_invalid_meshes_raise(args):
+    with pytest.raises(RtmError):
+        Mesh(*args)
+
+
+def test_a_single_face_has_no_rooftop():
+    with pytest.raises(RtmError) as e:
+        Mesh(1, 1, 0.1, 0.1)
+    assert e.value.identifier == "rooftopMoM:mesh:noRooftops"
+
+
+def test_problem_getters():
+    mesh = Mesh(4, 3, 0.1, 0.1)
+    problem = Problem(mesh, 2 * math.pi, quadratureOrder=3)
+    assert problem.mesh() is mesh
+    assert problem.wavenumber() == 2 * math.pi
+    assert problem.rooftopCount() == 17
+    assert problem.quadratureOrder() == (3, 3)
+
+
+def test_quadrature_orders_of_the_near_and_the_far_pairs():
+    mesh = Mesh(4, 3, 0.1, 0.1)
+    assert Problem(mesh, 2 * math.pi).quadratureOrder() == (16, 8)
+    assert Problem(mesh, 2 * math.pi, quadratureOrder=(12, 6)).quadratureOrder() == (12, 6)
+
+
+def test_electrical_size_sets_the_wavenumber():
+    mesh = Mesh(4, 3, 0.1, 0.2)
+    problem = Problem(mesh, electricalSize=0.5, quadratureOrder=3)
+    assert problem.wavenumber() == pytest.approx(0.5 / mesh.radius(), rel=1e-15)
+    assert problem.electricalSize() == pytest.approx(0.5, rel=1e-15)
+
+
+def test_density_counts_the_longer_face_side():
+    # faces of 0.08 m along y: 12.5 per wavelength of 1 m
+    assert Problem(Mesh(4, 3, 0.05, 0.08), 2 * math.pi, quadratureOrder=3).density() == pytest.approx(12.5, rel=1e-15)
+
+
+def test_from_electrical_size_meshes_the_plate():
+    # ka = 4 at 1 m: the diagonal is 4 / pi, the sides 1.139 and 0.569 m, 13.7 and 6.8 faces at 12 a wavelength
+    problem = Problem.fromElectricalSize(4, density=12, aspect=2, quadratureOrder=3)
+    (cx, cy), (sx, sy) = problem.mesh().count(), problem.mesh().faceSize()
+    assert (cx, cy) == (14, 7)
+    assert cx * sx / (cy * sy) == pytest.approx(2, rel=1e-14)
+    assert problem.wavenumber() == 2 * math.pi
+    assert problem.electricalSize() == pytest.approx(4, rel=1e-14)
+    assert problem.density() >= 12
+
+
+def test_from_electrical_size_rounds_the_counts_to_fast_fft_sizes():
+    # ka = 4.6 needs 10.35 faces a side at 10 a wavelength; the 11 that reach it round up to 12
+    problem = Problem.fromElectricalSize(4.6, density=10, quadratureOrder=3)
+    assert problem.mesh().count() == (12, 12)
+    assert problem.density() >= 10
+
+
+def test_from_electrical_size_meshes_a_strip_one_face_across():
+    problem = Problem.fromElectricalSize(math.pi / 2, density=20, aspect=250, quadratureOrder=3)
+    assert problem.mesh().count() == (10, 1)
+
+
+def test_from_electrical_size_refuses_a_single_face():
+    with pytest.raises(RtmError) as e:
+        Problem.fromElectricalSize(0.1)
+    assert e.value.identifier == "rooftopMoM:problem:singleFace"
+
+
+def test_invalid_problems_raise():
+    mesh = Mesh(4, 3, 0.1, 0.1)
+    with pytest.raises(RtmError):
+        Problem(mesh, 0)
+    with pytest.raises(RtmError) as e:
+        Problem(mesh, 2 * math.pi, quadratureOrder=2.5)
+    assert e.value.identifier == "rooftopMoM:problem:invalidQuadratureOrder"
+    with pytest.raises(RtmError) as e:
+        Problem(mesh, 2 * math.pi, quadratureOrder=(16, 8, 4))
+    assert e.value.identifier == "rooftopMoM:problem:invalidQuadratureOrder"
+    with pytest.raises(TypeError):
+        Problem(mesh, 2 * math.pi, order=3)
+    for kwargs in ({}, {"wavenumber": 2 * math.pi, "electricalSize": 2}):
+        with pytest.raises(RtmError) as e:
+            Problem(mesh, **kwargs)
+        assert e.value.identifier == "rooftopMoM:problem:invalidWavenumber"
+    with pytest.raises(RtmError):
+        Problem(mesh, electricalSize=-1)
+    with pytest.raises(RtmError):
+        Problem.fromElectricalSize(4, density=0)
