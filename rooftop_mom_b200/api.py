@@ -409,9 +409,9 @@ class Excitation:
         return v / np.linalg.norm(v)
 
     @classmethod
-    def planeWave(cls, problem: Problem, direction=(0, 0, -1), polarization=(1, 0, 0), intensity=1.0,
-                  device=False):
-        """device=True keeps the vector on the GPU (a complex128 CUDA tensor)."""
+    def planeWaveVectors(cls, direction, polarization):
+        """The unit direction and polarization of a plane wave (Excitation.m:52-62): both normalised, and
+        perpendicular to within the rounding of a rotated frame."""
         d = cls._normalize(direction, "direction")
         p = cls._normalize(polarization, "polarization")
         dot = float(d @ p)
@@ -419,6 +419,13 @@ class Excitation:
             raise _err("rooftopMoM:excitation:notPerpendicular",
                        f"The polarization must be perpendicular to the direction of propagation, their dot product "
                        f"is {dot:.1e}.")
+        return d, p
+
+    @classmethod
+    def planeWave(cls, problem: Problem, direction=(0, 0, -1), polarization=(1, 0, 0), intensity=1.0,
+                  device=False):
+        """device=True keeps the vector on the GPU (a complex128 CUDA tensor)."""
+        d, p = cls.planeWaveVectors(direction, polarization)
         cx, cy = problem.mesh().count()
         a, b = problem.mesh().faceSize()
         n = problem.rooftopCount()
@@ -609,9 +616,18 @@ class Solver:
             b = rightHandSide.vector()
         else:
             b = rightHandSide
-            if not _is_device(b) and not np.all(np.isfinite(np.asarray(b))):
-                raise _err("rooftopMoM:solver:invalidRightHandSide",
-                           "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+            if not _is_device(b):
+                try:
+                    a = np.asarray(b)
+                    finite = a.dtype.kind in "biufc" and bool(np.all(np.isfinite(a)))
+                except (TypeError, ValueError):
+                    finite = False
+                if not finite:
+                    raise _err("rooftopMoM:solver:invalidRightHandSide",
+                               "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+        if not isinstance(operator, (np.ndarray, _Product)):
+            raise _err("rooftopMoM:solver:invalidOperator",
+                       "The operator is a rooftopMoM.Operator, a DenseOperator or a numeric matrix.")
         if isinstance(operator, np.ndarray):
             operator = DenseOperator(operator)
         if isinstance(preconditioner, np.ndarray):

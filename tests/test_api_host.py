@@ -1,11 +1,13 @@
 """The host side of the Python mirror of the MATLAB API, which needs no GPU until generators are assembled:
 Mesh and Problem as the reference's tests/+unit/MeshTest.m:5-29 and ProblemTest.m:5-16, :18-29 and
-:64-140 hold them. MATLAB's argument validators (MATLAB:validators:*) have no Python counterpart; the
-mirror raises RtmError with a rooftopMoM:* identifier for the same inputs."""
+:64-140 hold them, and the argument checks of Excitation and Solver. MATLAB's argument validators
+(MATLAB:validators:*) have no Python counterpart; the mirror raises RtmError with a rooftopMoM:*
+identifier for the same inputs."""
 from __future__ import annotations
 
 import math
 
+import numpy as np
 import pytest
 
 from rooftop_mom_b200 import Mesh, Problem, RtmError
@@ -108,3 +110,80 @@ def test_invalid_problems_raise():
         Problem(mesh, electricalSize=-1)
     with pytest.raises(RtmError):
         Problem.fromElectricalSize(4, density=0)
+
+
+# Excitation and Solver arguments (tests/+unit/ExcitationTest.m:5-59, SolverTest.m:46-67): every check
+# below runs before any device work, and the delta gap of host memory is built on the host.
+def test_plane_wave_normalizes_its_vectors():
+    from rooftop_mom_b200 import Excitation
+
+    d, p = Excitation.planeWaveVectors([0, 0, -2], [0, 3, 0])
+    np.testing.assert_array_equal(d, [0, 0, -1])
+    np.testing.assert_array_equal(p, [0, 1, 0])
+
+
+def test_plane_wave_needs_perpendicular_nonzero_vectors():
+    from rooftop_mom_b200 import Excitation
+
+    with pytest.raises(RtmError) as e:
+        Excitation.planeWaveVectors([1, 0, 0], [1, 1, 0])
+    assert e.value.identifier == "rooftopMoM:excitation:notPerpendicular"
+    with pytest.raises(RtmError) as e:
+        Excitation.planeWaveVectors([0, 0, -1], [0, 0, 0])
+    assert e.value.identifier == "rooftopMoM:excitation:zeroVector"
+
+
+def test_plane_wave_accepts_a_rotated_frame():
+    from rooftop_mom_b200 import Excitation
+
+    a = (0.3, 1.1, 2.5)
+    rx = np.array([[1, 0, 0], [0, math.cos(a[0]), -math.sin(a[0])], [0, math.sin(a[0]), math.cos(a[0])]])
+    ry = np.array([[math.cos(a[1]), 0, math.sin(a[1])], [0, 1, 0], [-math.sin(a[1]), 0, math.cos(a[1])]])
+    rz = np.array([[math.cos(a[2]), -math.sin(a[2]), 0], [math.sin(a[2]), math.cos(a[2]), 0], [0, 0, 1]])
+    frame = rz @ ry @ rx
+    Excitation.planeWaveVectors(frame[:, 2], frame[:, 0])
+
+
+def test_delta_gap_defaults_to_the_middle_port():
+    from oracle import excitation as EX
+    from oracle.geometry import Rooftops
+    from rooftop_mom_b200 import Excitation
+
+    problem = Problem(Mesh(6, 1, 0.1, 0.1), 2 * math.pi, quadratureOrder=3)
+    e = Excitation.deltaGap(problem, voltage=2)
+    assert e.type() == "deltaGap"
+    np.testing.assert_array_equal(e.parameters()["port"], [2])
+    assert e.parameters()["voltage"] == 2
+    np.testing.assert_array_equal(e.vector(), EX.delta_gap(Rooftops(6, 1, 0.1, 0.1, 3), [2], 2))
+
+
+def test_delta_gap_checks_the_port():
+    from rooftop_mom_b200 import Excitation
+
+    problem = Problem(Mesh(6, 1, 0.1, 0.1), 2 * math.pi, quadratureOrder=3)
+    for port in ([1, 1], [5]):
+        with pytest.raises(RtmError) as e:
+            Excitation.deltaGap(problem, port=port)
+        assert e.value.identifier == "rooftopMoM:excitation:invalidPort"
+    with pytest.raises(RtmError) as e:
+        Excitation.deltaGap(problem, direction="y")
+    assert e.value.identifier == "rooftopMoM:excitation:noRooftops"
+
+
+def test_invalid_solvers_and_solver_inputs_raise():
+    from rooftop_mom_b200 import Solver
+
+    for kwargs in ({"method": "bicg"}, {"tolerance": 2}):
+        with pytest.raises(RtmError):
+            Solver(**kwargs)
+    with pytest.raises(RtmError) as e:
+        Solver(restart=2.5)
+    assert e.value.identifier == "rooftopMoM:solver:invalidRestart"
+    solver = Solver()
+    with pytest.raises(RtmError) as e:
+        solver.solve("matrix", np.ones(3))
+    assert e.value.identifier == "rooftopMoM:solver:invalidOperator"
+    for rhs in (np.array([1, np.nan, 3]), ["a", "b", "c"]):
+        with pytest.raises(RtmError) as e:
+            solver.solve(np.eye(3), rhs)
+        assert e.value.identifier == "rooftopMoM:solver:invalidRightHandSide"
