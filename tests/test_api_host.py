@@ -187,3 +187,20 @@ def test_invalid_solvers_and_solver_inputs_raise():
         with pytest.raises(RtmError) as e:
             solver.solve(np.eye(3), rhs)
         assert e.value.identifier == "rooftopMoM:solver:invalidRightHandSide"
+
+
+def test_result_quantities_need_their_excitation():
+    # tests/+unit/ResultTest.m:13-14, :24, :43: the checks come before any device work
+    from rooftop_mom_b200 import Excitation, Result
+    from rooftop_mom_b200 import _lib as L
+
+    problem = Problem(Mesh(6, 1, 0.1, 0.1), 2 * math.pi, quadratureOrder=3)
+    gap = Result(np.zeros(5, complex), L.SolveStats(), np.array([1.0]), Excitation.deltaGap(problem))
+    for quantity in (gap.radarCrossSection, gap.normalizedRadarCrossSection):
+        with pytest.raises(RtmError) as e:
+            quantity()
+        assert e.value.identifier == "rooftopMoM:result:wrongExcitation"
+    plain = Result(np.zeros(3, complex), L.SolveStats(), np.array([1.0]), None)
+    with pytest.raises(RtmError) as e:
+        plain.inputImpedance()
+    assert e.value.identifier == "rooftopMoM:result:wrongExcitation"
