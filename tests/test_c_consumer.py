@@ -1,0 +1,68 @@
+"""include/rtm.h compiles as strict C99 (gcc -std=c99 -pedantic -Wall -Werror), as a MEX gateway includes
+it, and a C program linked against librtm.so calls the entry points that need no GPU: the version, the byte
+models (against the oracle), the size of the fixed scratch array, a delta gap built in host memory (against
+the oracle) and the status and message of two rejected calls."""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+@pytest.fixture(scope="module")
+def consumer(tmp_path_factory):
+    from rooftop_mom_b200 import build
+
+    lib = build.build()
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    exe = str(tmp_path_factory.mktemp("c") / "abi_consumer")
+    libdir = os.path.dirname(lib)
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "abi_consumer.c"), "-o", exe, "-L", libdir, "-l:librtm.so",
+                    f"-Wl,-rpath,{libdir}"], check=True, capture_output=True, text=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
+    return {line.split()[0]: line.split()[1:] for line in out.splitlines()}
+
+
+def test_version(consumer):
+    assert consumer["version"] == ["0", "3.5.0"]
+
+
+def test_byte_models(consumer):
+    from oracle import excitation as EX
+    from oracle.geometry import Rooftops
+
+    rt = Rooftops(256, 256, 0.1, 0.1)
+    stored, working = EX.estimate_product(rt, "splitFFT")
+    pc_stored, pc_working = EX.estimate_preconditioner(rt)
+    want = [EX.estimate_generators(rt), stored, working, pc_stored, pc_working,
+            EX.estimate_solver(rt.count, "gmres", True, 50, 1000)]
+    assert consumer["estimate"][0] == "0"
+    assert [float(v) for v in consumer["estimate"][1:]] == want
+
+
+def test_fixed_scratch_size(consumer):
+    assert consumer["scratch"] == ["0", str(32 << 20)]
+
+
+def test_delta_gap_in_host_memory(consumer):
+    from oracle import excitation as EX
+    from oracle.geometry import Rooftops
+
+    assert consumer["gap"][0] == "0"
+    want = EX.delta_gap(Rooftops(4, 3, 0.1, 0.2), [1, 4, 10], 3.0)
+    assert [float(v) for v in consumer["gap"][1:]] == list(want)
+
+
+def test_rejected_calls_report_status_and_message(consumer):
+    from rooftop_mom_b200 import _lib as L
+
+    assert consumer["null"][0] == str(L.ERR_ARG)
+    assert " ".join(consumer["null"][1:]) == "null output"
+    assert consumer["rhs"][0] == str(L.ERR_SIZE)
+    assert "65535" in " ".join(consumer["rhs"][1:])
