@@ -445,7 +445,9 @@ def run_reference(args, w):
     t = float(np.median(times))
     value = 1.0 / t
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
+        # n_gpus is the N of the launch this line is compared with; the arm itself runs on host cores only
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "device": "host CPU cores (no GPU used)",
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": config_of(args, w),

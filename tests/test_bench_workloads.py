@@ -59,3 +59,21 @@ def test_the_request_stream_is_seeded_and_chooses_a_preconditioner_per_grid():
         assert sa.preconditioner == expect
         lam = 2 * math.pi / sa.wavenumber
         assert 10 - 1e-9 <= lam / sa.size_x <= 25 + 1e-9
+
+
+def test_the_reference_arm_prints_its_line_on_the_host():
+    """bench.py --impl reference runs the oracle's CPU path (no GPU) and prints the contract's line: the
+    launch's N, the metric and unit of our arm, a cpu_baseline and an e2e object."""
+    import json
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "0"], check=True, capture_output=True, text=True,
+                         timeout=600, cwd=root).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["unit"] == "solves/s" and line["higher_is_better"] is True and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
