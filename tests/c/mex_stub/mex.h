@@ -20,6 +20,9 @@ typedef enum { mxDOUBLE_CLASS = 6, mxUINT64_CLASS = 15 } mxClassID;
 int mxGetString(const mxArray* a, char* buf, mwSize len);
 double mxGetScalar(const mxArray* a);
 bool mxIsEmpty(const mxArray* a);
+bool mxIsComplex(const mxArray* a);
+size_t mxGetM(const mxArray* a);
+size_t mxGetN(const mxArray* a);
 size_t mxGetNumberOfElements(const mxArray* a);
 void* mxGetData(const mxArray* a);
 mxDouble* mxGetDoubles(const mxArray* a);
