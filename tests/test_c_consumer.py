@@ -80,5 +80,6 @@ def test_the_mex_gateway_of_the_integration_notes_compiles_against_the_header(tm
     assert "mexFunction" in source
     path = tmp_path / "rtm_mex.c"
     path.write_text(source)
-    subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-Wall", "-Werror", "-I", os.path.join(ROOT, "tests", "c", "mex_stub"),
-                    "-I", os.path.join(ROOT, "include"), str(path)], check=True, capture_output=True, text=True)
+    subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-Wall", "-Wextra", "-Werror",
+                    "-I", os.path.join(ROOT, "tests", "c", "mex_stub"), "-I", os.path.join(ROOT, "include"), str(path)],
+                   check=True, capture_output=True, text=True)
