@@ -185,10 +185,11 @@ def test_size_mismatch_raises_the_reference_error():
 
 
 @pytest.mark.parametrize("precision", ["double", "single"])
-@pytest.mark.parametrize("count", [(32, 32), (64, 64), (64, 128), (256, 256), (512, 512), (1024, 1024)])
+@pytest.mark.parametrize("count", [(32, 32), (64, 64), (64, 128), (128, 64), (256, 256), (512, 512), (1024, 1024)])
 def test_power_of_two_products_match_the_oracle(count, precision):
     """The power-of-two fast path (transform sizes 32..1024; FP64 up to 512, the generic engine above)
-    against the oracle's split product (applyBothDirections_.m:14-85) of the same generators."""
+    against the oracle's split product (applyBothDirections_.m:14-85) of the same generators. Every line
+    length runs in both directions: 64 x 128 and 128 x 64 exchange the x-mix and the y transforms."""
     import rooftop_mom_b200 as R
     from oracle import assembly as A, geometry as G, spectra as S
 
