@@ -56,6 +56,8 @@ def _rel(a, b):
         ((40, 36), "leanSplitFFT", "double", 2),
         ((33, 28), "fft", "double", 1),
         ((64, 48), "splitFFT", "single", 3),
+        ((64, 64), "splitFFT", "double", 2),  # power-of-two grids: the register-resident fast path
+        ((64, 32), "splitFFT", "single", 3),
     ],
 )
 def test_fixed_scratch_matches_the_allocating_product(count, product, precision, nrhs):
