@@ -216,7 +216,8 @@ RTM_API int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_precon
 /* Excitation and results (src/+rooftopMoM/+operator) ------------------------------------------ */
 
 /* generatePlaneWave.m:18-42 on the device, for nrhs waves: direction and polarization are 3*nrhs
- * unit vectors, intensity nrhs values. order is the far quadrature order of the rooftops. */
+ * unit vectors, each pair perpendicular (RTM_ERR_ARG unless within 1e-9 of that), intensity nrhs values.
+ * order is the far quadrature order of the rooftops. */
 RTM_API int rtm_plane_wave(int count_x, int count_y, double size_x, double size_y, int order, double wavenumber,
                    const double* directions, const double* polarizations, const double* intensities, int nrhs,
                    void* out, int where, void* stream);
@@ -266,7 +267,8 @@ typedef struct rtm_request {
     double wavenumber;          /* k = 2 pi f / c */
     int excitation;             /* rtm_excitation */
     double direction[3];        /* plane wave: unit propagation direction */
-    double polarization[3];     /* plane wave: unit polarisation (intensity 1) */
+    double polarization[3];     /* plane wave: unit polarisation perpendicular to it (intensity 1); submit
+                                   rejects the pair unless both hold to within 1e-9 */
     int port_direction;         /* delta gap: middle port across x (0) or y (1) rooftops */
     double voltage;             /* delta gap: gap voltage */
     int method;                 /* RTM_METHOD_CG or RTM_METHOD_GMRES (right-preconditioned) */

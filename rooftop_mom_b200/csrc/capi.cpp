@@ -28,6 +28,19 @@ int middle_port(int count_x, int count_y, int direction, std::vector<int64_t>& p
     }
     return RTM_OK;
 }
+
+int check_plane_wave(const double* d, const double* p) {
+    double dd = 0, pp = 0, dp = 0;
+    for (int i = 0; i < 3; ++i) {
+        dd += d[i] * d[i];
+        pp += p[i] * p[i];
+        dp += d[i] * p[i];
+    }
+    constexpr double kTol = 1e-9;
+    if (!(std::fabs(std::sqrt(dd) - 1) <= kTol) || !(std::fabs(std::sqrt(pp) - 1) <= kTol) || !(std::fabs(dp) <= kTol))
+        return fail(RTM_ERR_ARG, "The direction and polarization of a plane wave must be perpendicular unit vectors.");
+    return RTM_OK;
+}
 }  // namespace rtm
 
 namespace {
@@ -586,6 +599,7 @@ int rtm_plane_wave(int count_x, int count_y, double size_x, double size_y, int o
     if (!directions || !polarizations || !intensities || !out) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_rhs(nrhs));
     RTM_TRY(check_where(where));
+    for (int k = 0; k < nrhs; ++k) RTM_TRY(check_plane_wave(directions + 3 * k, polarizations + 3 * k));
     if (count_x < 1 || count_y < 1 || order < 1) return fail(RTM_ERR_ARG, "invalid grid or order");
     CallStream own;
     RTM_TRY(make_stream(&own.s));

@@ -47,4 +47,8 @@ struct rtm_preconditioner {
 namespace rtm {
 // The rooftops of the middle port of a grid in direction 0 (x) or 1 (y), generateMiddlePort.m:14-28.
 int middle_port(int count_x, int count_y, int direction, std::vector<int64_t>& port);
+// RTM_OK when the direction and polarization of a plane wave are perpendicular unit vectors (to 1e-9), the
+// form generatePlaneWave.m:18-42 takes them in (Excitation.planeWave normalises and checks them,
+// Excitation.m:52-62); RTM_ERR_ARG otherwise.
+int check_plane_wave(const double* direction, const double* polarization);
 }  // namespace rtm

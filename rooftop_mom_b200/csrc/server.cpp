@@ -71,6 +71,7 @@ int check_request(const rtm_request& q) {
     if (!(q.size_x > 0) || !(q.size_y > 0) || !(q.wavenumber > 0)) return fail(RTM_ERR_ARG, "invalid sizes");
     if (q.excitation != RTM_EXCITE_PLANE_WAVE && q.excitation != RTM_EXCITE_DELTA_GAP)
         return fail(RTM_ERR_ARG, "unknown excitation");
+    if (q.excitation == RTM_EXCITE_PLANE_WAVE) RTM_TRY(check_plane_wave(q.direction, q.polarization));
     if (q.method != RTM_METHOD_CG && q.method != RTM_METHOD_GMRES) return fail(RTM_ERR_ARG, "unknown method");
     if (!(q.tolerance > 0) || q.max_iterations < 1 || q.restart < 1) return fail(RTM_ERR_ARG, "invalid solver");
     if (q.preconditioner < 0 || q.preconditioner > kPcCirculant) return fail(RTM_ERR_ARG, "unknown preconditioner");

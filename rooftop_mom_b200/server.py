@@ -43,6 +43,12 @@ class Request:
     def __init__(self, countX, countY, sizeX, sizeY, wavenumber, excitation="planeWave", direction=(0, 0, -1),
                  polarization=(1, 0, 0), portDirection="x", voltage=1.0, method="gmres", preconditioner="blockJacobi",
                  tolerance=1e-6, maxIterationCount=10000, restart=50, keepCurrent=False):
+        if excitation == "planeWave":
+            from .api import Excitation
+
+            # normalised and checked as Excitation.planeWave does, so a request and a direct solve of the same
+            # wave see the same vectors
+            direction, polarization = Excitation.planeWaveVectors(direction, polarization)
         r = L.Request()
         r.count_x, r.count_y = int(countX), int(countY)
         r.size_x, r.size_y, r.wavenumber = float(sizeX), float(sizeY), float(wavenumber)

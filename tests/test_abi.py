@@ -73,6 +73,23 @@ def test_batched_calls_bound_the_vector_count(library):
     assert "positive" in _lib.last_error()
 
 
+def test_plane_waves_take_perpendicular_unit_vectors(library):
+    """generatePlaneWave.m takes a unit direction and a unit polarization perpendicular to it; the ABI checks
+    both before any device work."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    one = (C.c_double * 1)(1.0)
+    sink = (C.c_double * 2)()
+    for d, p in (((0, 0, -2), (1, 0, 0)), ((0, 0, -1), (1, 0, 0.1)), ((1, 0, 0), (1, 0, 0))):
+        dv, pv = (C.c_double * 3)(*d), (C.c_double * 3)(*p)
+        assert lib.rtm_plane_wave(8, 8, 0.05, 0.05, 8, 6.283185307179586, dv, pv, one, 1, sink, _lib.HOST,
+                                  None) == _lib.ERR_ARG
+        assert "perpendicular unit vectors" in _lib.last_error()
+
+
 def test_byte_models_match_the_oracle(library):
     import ctypes as C
 

@@ -61,3 +61,24 @@ def test_server_configuration_is_checked():
     h = C.c_void_p()
     with pytest.raises(L.RtmError):
         L.call("rtm_server_create", C.byref(cfg), C.byref(h))
+
+
+def test_plane_wave_requests_take_perpendicular_unit_vectors():
+    """Request normalises the vectors as Excitation.planeWave does; the ABI rejects a request whose vectors are
+    not perpendicular unit vectors, before any device work."""
+    import ctypes as C
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    req = R.Request.planeWave(40, 32, 0.05, 0.05, 2 * math.pi, direction=(0, 0, -2), polarization=(0, 3, 0))
+    assert list(req.struct.direction) == [0, 0, -1] and list(req.struct.polarization) == [0, 1, 0]
+    with pytest.raises(L.RtmError) as e:
+        R.Request.planeWave(40, 32, 0.05, 0.05, 2 * math.pi, direction=(1, 0, 0), polarization=(1, 1, 0))
+    assert e.value.identifier == "rooftopMoM:excitation:notPerpendicular"
+    with R.Server(budgetBytes=1e9, maxActive=1) as srv:
+        raw = _request().struct
+        raw.direction[:] = [0.0, 0.0, -2.0]
+        rid = C.c_uint64()
+        assert L.load().rtm_server_submit(srv._h, C.byref(raw), C.byref(rid)) == L.ERR_ARG
+        assert "perpendicular unit vectors" in L.last_error()
