@@ -182,7 +182,9 @@ typedef struct rtm_solve_config {
     int method;            /* RTM_METHOD_CG (COCG), RTM_METHOD_GMRES, RTM_METHOD_FGMRES_IR */
     double tolerance;      /* relative residual to stop at (Solver.m:29, default 1e-6) */
     int max_iterations;    /* Solver.m:30, default 1000 */
-    int restart;           /* GMRES cycle length (Solver.m:31, default 50); FGMRES inner cycle */
+    int restart;           /* GMRES cycle length (Solver.m:31, default 50); FGMRES inner cycle. At most 344
+                              in FP64 and 638 in FP32 (RTM_ERR_UNSUPPORTED above): longer bases do not fit
+                              the orthogonalisation's shared-memory tile */
     double inner_tolerance;/* FGMRES_IR: relative residual of one FP32 inner solve */
     int max_refinements;   /* FGMRES_IR: bound on the FP64 outer refinement steps */
     int check_every;       /* iterations between host convergence checks (0: library default) */

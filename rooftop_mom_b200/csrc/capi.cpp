@@ -657,7 +657,12 @@ int rtm_input_impedance(int count_x, int count_y, double size_x, double size_y, 
                         const int64_t* port, int port_count, double voltage, int where, double* out) {
     if (!current || !port || port_count < 1 || !out) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
+    if (count_x < 1 || count_y < 1) return fail(RTM_ERR_ARG, "invalid grid");
     const int64_t n = (int64_t)(count_x - 1) * count_y + (int64_t)count_x * (count_y - 1);
+    // the port's currents are gathered on the device: every index must name a rooftop
+    for (int i = 0; i < port_count; ++i)
+        if (port[i] < 0 || port[i] >= n)
+            return fail(RTM_ERR_ARG, "The port must hold rooftop indices below " + std::to_string(n) + ".");
     CallStream own;
     RTM_TRY(make_stream(&own.s));
     cudaStream_t s = own.s;

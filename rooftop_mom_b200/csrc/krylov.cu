@@ -523,6 +523,8 @@ __global__ void __launch_bounds__(kRT) k_gm_orth(const T2* __restrict__ V, T2* _
     }
 }
 
+constexpr int kOrthSmemMax = 200 * 1024;  // dynamic shared memory k_gm_orth may take
+
 // Rows per tile and shared bytes of k_gm_orth (two buffers) for a basis of up to m + 1 columns.
 template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
     const size_t fixed = (size_t)(2 * (m + 1) + std::max(kRT, m + 1)) * sizeof(double2);
@@ -1067,6 +1069,15 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     const T2* x0 = static_cast<const T2*>(x0v);
     T2* x = static_cast<T2*>(xv);
     const int m = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)cfg.restart, n, (int64_t)cfg.max_iterations}));
+    if (m + 1 > kStreamCols) {
+        // bases above kStreamCols columns run k_gm_orth, whose tile of the basis sits in shared memory
+        int TR;
+        size_t smem;
+        orth_config<T2>(m, &TR, &smem);
+        if (smem > (size_t)kOrthSmemMax)
+            return fail(RTM_ERR_UNSUPPORTED, "a GMRES restart of " + std::to_string(m) +
+                                                 " is longer than this build's orthogonalisation holds in shared memory");
+    }
     const int nb = reduce_blocks(n);
     const size_t vec = (size_t)n * nrhs * sizeof(T2);
     // Right (flexible) preconditioning keeps z_j = M v_j and solves A M u = b, x = Z y: the monitored
@@ -1133,7 +1144,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     k_gm_norm<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), n, st, ar, 1, 1);
     count_launch();
     // function attributes are set before the capture
-    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kOrthSmemMax));
     {
         int sb, sc;
         stream_config(n, &sb, &sc);
