@@ -109,3 +109,20 @@ def test_byte_models_match_the_oracle(library):
                 ps, pw = EX.estimate_preconditioner(rt)
                 assert out[3] == ps and out[4] == pw
                 assert out[5] == EX.estimate_solver(rt.count, method, True, 50, 1000)
+
+
+def test_input_impedance_rejects_ports_outside_the_rooftops(library):
+    """The port's currents are gathered on the device, so every index must name a rooftop: the ABI checks
+    them before any device work."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    n = 3 * 3 + 4 * 2  # a 4 x 3 plate
+    current = (C.c_double * (2 * n))()
+    out = (C.c_double * 2)()
+    for bad in (n, -1):
+        port = (C.c_int64 * 2)(1, bad)
+        assert lib.rtm_input_impedance(4, 3, 0.1, 0.2, current, port, 2, 1.0, _lib.HOST, out) == _lib.ERR_ARG
+        assert "rooftop indices below 17" in _lib.last_error()
