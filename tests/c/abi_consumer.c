@@ -40,5 +40,40 @@ int main(void) {
     print_error("null", status);
     status = rtm_plane_wave(8, 8, 0.05, 0.05, 8, 6.283185307179586, dir, pol, &one, 70000, sink, RTM_HOST, NULL);
     print_error("rhs", status);
+
+    /* the serving loop: a request above the whole budget fails at submission, before any device work */
+    {
+        rtm_server_config cfg;
+        rtm_server* srv = NULL;
+        rtm_request req;
+        rtm_request_result res;
+        uint64_t id = 0;
+        memset(&cfg, 0, sizeof cfg);
+        cfg.budget_bytes = 1e6;
+        cfg.max_active = 2;
+        cfg.precision = RTM_FP64;
+        memset(&req, 0, sizeof req);
+        req.count_x = 40;
+        req.count_y = 32;
+        req.size_x = req.size_y = 0.05;
+        req.wavenumber = 6.283185307179586;
+        req.excitation = RTM_EXCITE_PLANE_WAVE;
+        req.direction[2] = -1;
+        req.polarization[0] = 1;
+        req.method = RTM_METHOD_GMRES;
+        req.preconditioner = 1;
+        req.tolerance = 1e-6;
+        req.max_iterations = 1000;
+        req.restart = 50;
+        status = rtm_server_create(&cfg, &srv);
+        printf("server_create %d\n", status);
+        status = rtm_server_submit(srv, &req, &id);
+        printf("server_submit %d %llu\n", status, (unsigned long long)id);
+        memset(&res, 0, sizeof res);
+        status = rtm_server_poll(srv, id, 0, &res, NULL, 0, 1);
+        printf("server_poll %d %d %d %.17g\n", status, res.state, res.status, res.bytes);
+        status = rtm_server_destroy(srv);
+        printf("server_destroy %d\n", status);
+    }
     return 0;
 }

@@ -1,8 +1,9 @@
 """include/rtm.h compiles as strict C99 (gcc -std=c99 -pedantic -Wall -Werror), as a MEX gateway includes
 it, and a C program linked against librtm.so calls the entry points that need no GPU: the version, the byte
 models (against the oracle), the size of the fixed scratch array, a delta gap built in host memory (against
-the oracle) and the status and message of two rejected calls. The MEX gateway of INTEGRATION.md compiles
-against the header."""
+the oracle), the status and message of two rejected calls, and the serving loop's create / submit / poll /
+destroy with a request that fails at submission. The MEX gateway of INTEGRATION.md compiles against the
+header."""
 from __future__ import annotations
 
 import os
@@ -58,6 +59,18 @@ def test_delta_gap_in_host_memory(consumer):
     assert consumer["gap"][0] == "0"
     want = EX.delta_gap(Rooftops(4, 3, 0.1, 0.2), [1, 4, 10], 3.0)
     assert [float(v) for v in consumer["gap"][1:]] == list(want)
+
+
+def test_the_serving_loop_from_c(consumer):
+    """rtm_server_* from C: create, a submission that fails at once on the budget, poll, destroy."""
+    from rooftop_mom_b200 import _lib as L
+
+    assert consumer["server_create"] == ["0"]
+    assert consumer["server_submit"] == ["0", "1"]
+    status, state, failure, nbytes = consumer["server_poll"]
+    assert (status, L.STATES[int(state)], int(failure)) == ("0", "failed", L.ERR_OOM_BUDGET)
+    assert float(nbytes) > 1e6
+    assert consumer["server_destroy"] == ["0"]
 
 
 def test_rejected_calls_report_status_and_message(consumer):
