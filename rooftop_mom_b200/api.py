@@ -351,10 +351,13 @@ class Preconditioner(_Product):
             raise _err("rooftopMoM:preconditioner:invalidBuilder", "The builder is 'partwise', 'blockwise' or 'hybrid'.")
         bw = None
         if bandwidth is not None:
-            if np.size(bandwidth) != 2:
+            bw_values = np.asarray(bandwidth, dtype=np.float64).ravel()
+            if bw_values.size != 2:
                 raise _err("rooftopMoM:preconditioner:invalidBandwidth",
                            "The bandwidth is a pair [bandwidthX, bandwidthY].")
-            bw = (C.c_int * 2)(int(bandwidth[0]), int(bandwidth[1]))
+            if not np.all((bw_values >= 1) & (bw_values == np.floor(bw_values))):
+                raise _err("rooftopMoM:preconditioner:invalidBandwidth", "The bandwidths are positive integers.")
+            bw = (C.c_int * 2)(int(bw_values[0]), int(bw_values[1]))
         gen = problem.generators()
         if modifier is not None:
             gen = gen.modify(modifier)

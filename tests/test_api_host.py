@@ -204,3 +204,17 @@ def test_result_quantities_need_their_excitation():
     with pytest.raises(RtmError) as e:
         plain.inputImpedance()
     assert e.value.identifier == "rooftopMoM:result:wrongExcitation"
+
+
+def test_invalid_preconditioners_raise_before_any_device_work():
+    # tests/+unit/PreconditionerTest.m:62-71
+    from rooftop_mom_b200 import Preconditioner
+
+    problem = Problem(Mesh(8, 8, 0.05, 0.05), 2 * math.pi, quadratureOrder=3)
+    with pytest.raises(RtmError) as e:
+        Preconditioner(problem, kernel="jacobi")
+    assert e.value.identifier == "rooftopMoM:preconditioner:invalidKernel"
+    for bandwidth in ([1, 2, 3], [0, 2], [1.5, 2]):
+        with pytest.raises(RtmError) as e:
+            Preconditioner(problem, kernel="huckle", bandwidth=bandwidth)
+        assert e.value.identifier == "rooftopMoM:preconditioner:invalidBandwidth"
