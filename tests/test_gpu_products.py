@@ -99,6 +99,25 @@ def test_products_match_the_dense_matrix(name, product):
     assert rel(R.Operator(prob, product=product).apply(v), dense @ v) < 1e-12
 
 
+@pytest.mark.parametrize("name", ["plate", "stripX", "stripY"])
+@pytest.mark.parametrize("modifier", ["real", "imag"])
+@pytest.mark.parametrize("product", PRODUCTS)
+def test_the_modifier_selects_a_part_of_the_matrix(product, modifier, name):
+    """+unit/OperatorTest.m:18-25: the operator of the real or imaginary part of the generators
+    (Generators.modify, rtm_generators_modify) is that part of the dense matrix, rel 1e-12."""
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, excitation as EX, geometry as G
+
+    cx, cy, a, b = GRIDS[name]
+    prob = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, a, b, 3)
+    part = np.real if modifier == "real" else np.imag
+    dense = part(EX.dense_matrix(A.Generators(xx, yy, e, rt.content), rt))
+    v = random_vector(rt.count, seed=2)
+    assert rel(R.Operator(prob, product=product, modifier=modifier).apply(v), dense @ v) < 1e-12
+
+
 @pytest.mark.parametrize("name", ["plate", "oddPlate", "stripX", "stripY", "square32"])
 def test_spectra_match_the_oracle(name):
     import rooftop_mom_b200 as R
