@@ -52,6 +52,8 @@ def test_version_and_errors_without_a_gpu(library):
     assert (a.value, b.value, c.value) == (3, 5, 0)
     # argument errors are reported without touching a device
     assert lib.rtm_generators_destroy(None) == 0
+    v = C.c_int()
+    assert lib.rtm_generators_info(None, C.byref(v), C.byref(v), C.byref(v)) == _lib.ERR_ARG
     out = (C.c_double * 6)()
     assert lib.rtm_estimate_bytes(0, 4, 1, 0, 0, 50, 1000, out) == _lib.ERR_ARG
     assert "invalid grid" in _lib.last_error()

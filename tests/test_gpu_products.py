@@ -99,6 +99,22 @@ def test_products_match_the_dense_matrix(name, product):
     assert rel(R.Operator(prob, product=product).apply(v), dense @ v) < 1e-12
 
 
+@pytest.mark.parametrize("name,content", [("plate", 3), ("stripX", 1), ("stripY", 2)])
+def test_generators_info_reports_the_grid_and_content(name, content):
+    """rtm_generators_info: the face counts and the rooftop content (RTM_BOTH, RTM_XONLY, RTM_YONLY) of
+    assembled generators (Generators.content, Generators.m)."""
+    import ctypes as C
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    cx, cy, a, b = GRIDS[name]
+    gen = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3).generators()
+    got = [C.c_int(), C.c_int(), C.c_int()]
+    L.call("rtm_generators_info", gen.handle, *[C.byref(v) for v in got])
+    assert [v.value for v in got] == [cx, cy, content]
+
+
 @pytest.mark.parametrize("name", ["plate", "stripX", "stripY"])
 @pytest.mark.parametrize("modifier", ["real", "imag"])
 @pytest.mark.parametrize("product", PRODUCTS)
