@@ -82,3 +82,26 @@ def test_plane_wave_requests_take_perpendicular_unit_vectors():
         rid = C.c_uint64()
         assert L.load().rtm_server_submit(srv._h, C.byref(raw), C.byref(rid)) == L.ERR_ARG
         assert "perpendicular unit vectors" in L.last_error()
+
+
+def test_requests_that_fail_on_the_device_release_their_slot_and_bytes():
+    """Admission, the workers and the release of a request's bytes on its failure path: without a GPU
+    every admitted request fails at its first device call, and the queue must still drain through the
+    slots and the budget (which admits two of these requests at a time) with every request reported."""
+    import torch
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    if torch.cuda.is_available():
+        pytest.skip("on a GPU these requests run; this test follows the failure path")
+    with R.Server(budgetBytes=1.0, maxActive=1) as probe:
+        one = probe.poll(probe.submit(_request()))["bytes"]
+    with R.Server(budgetBytes=2.5 * one, maxActive=3) as srv:
+        ids = [srv.submit(_request()) for _ in range(7)]
+        results = [srv.poll(rid, wait=60.0) for rid in ids]
+        assert [r["state"] for r in results] == ["failed"] * 7
+        assert all(r["status"] == L.ERR_CUDA for r in results)
+        assert all(r["finished"] >= r["started"] >= r["submitted"] for r in results)
+        # the released bytes admit a later request too
+        assert srv.poll(srv.submit(_request()), wait=60.0)["state"] == "failed"
