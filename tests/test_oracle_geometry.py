@@ -1,6 +1,6 @@
-"""The oracle's rooftops and quadrature rules, restating the reference's unit tests
-tests/+unit/+basisFunctions/UniformRooftopsTest.m:5-58, +utils/GenerateGaussLegendre1DTest.m:5-34 and
-GaussLegendre2RectQuadratureTest.m:5-30."""
+"""The oracle's rooftops, quadrature rules and constants, restating the reference's unit tests
+tests/+unit/+basisFunctions/UniformRooftopsTest.m:5-58, +utils/GenerateGaussLegendre1DTest.m:5-34,
+GaussLegendre2RectQuadratureTest.m:5-30 and tests/+unit/+assembler/ConstantsTest.m:5-20."""
 from __future__ import annotations
 
 import math
@@ -81,3 +81,16 @@ def test_the_u_coordinate_runs_fastest():
     np.testing.assert_array_equal(pu[:2], pu[2:4])
     assert pv[0] == pv[1]
     assert pu[0] < pu[1]
+
+
+def test_constants_are_those_of_the_reference():
+    # src/+rooftopMoM/+assembler/Constants.m:8-17 and tests/+unit/+assembler/ConstantsTest.m:5-20: c exact,
+    # Z0 given, mu0 and epsilon0 derived from them and within CODATA 2018's uncertainty
+    import rooftop_mom_b200.api as api
+
+    assert G.SPEED_OF_LIGHT == api.SPEED_OF_LIGHT == 299792458.0
+    assert G.Z0 == api.Z0 == 376.730313668
+    assert G.SPEED_OF_LIGHT**2 * G.MU0 * G.EPSILON0 == pytest.approx(1.0, rel=4 * np.finfo(float).eps)
+    assert math.sqrt(G.MU0 / G.EPSILON0) == pytest.approx(G.Z0, rel=4 * np.finfo(float).eps)
+    assert G.MU0 == pytest.approx(1.25663706212e-6, rel=1.5e-10)
+    assert G.EPSILON0 == pytest.approx(8.8541878128e-12, rel=1.5e-10)

@@ -2,8 +2,10 @@
 restating the reference's unit tests
 tests/+unit/+assembler/+greensMatrix/+utils/IntegrateMomentsTest.m:5-54,
 tests/+unit/+assembler/+singularIntegrals/GeneratePowerMomentsTest.m:48-66,
-tests/+unit/+assembler/+singularIntegrals/EvaluateRemainderTest.m:5-21 and
-tests/+unit/+assembler/+greensMatrix/+utils/AccumulateMomentsTest.m:5-59."""
+tests/+unit/+assembler/+singularIntegrals/EvaluateRemainderTest.m:5-21,
+tests/+unit/+assembler/+greensMatrix/+utils/AccumulateMomentsTest.m:5-59,
+tests/+unit/+assembler/+singularIntegrals/+utils/IntegrateMonomialTest.m:9-52 and
+tests/+unit/+assembler/+singularIntegrals/GenerateExtractedMomentsTest.m:5-18."""
 from __future__ import annotations
 
 import numpy as np
@@ -152,3 +154,51 @@ def test_a_missing_direction_is_skipped():
                                  (1, 1))
     assert parts.magnetic_yy is None
     np.testing.assert_array_equal(parts.electric, np.ones((6, 1)))
+
+
+# tests/+unit/+assembler/+singularIntegrals/+utils/IntegrateMonomialTest.m:9-52: G(a, b), the integral of
+# u^m v^n R^p over [0, a] x [0, b], of which the moments are corner differences.
+@pytest.mark.parametrize("power", [-1, 1, 3])
+def test_monomial_integrals_vanish_on_the_axes(power):
+    for m in range(4):
+        for n in range(2):
+            np.testing.assert_array_equal(SI.integrate_monomial(power, m, n, [0, 0.7, 0], [0.4, 0, 0]), [0, 0, 0])
+
+
+@pytest.mark.parametrize("power", [-1, 1, 3])
+def test_corner_differences_of_monomial_integrals_are_the_integrals(power):
+    from scipy import integrate
+
+    for a0, a1, b0, b1 in ((0.0, 0.6, 0.0, 0.25), (0.3, 0.8, 0.1, 0.9)):  # a corner at the singular point, and not
+        for m in range(4):
+            for n in range(2):
+                def G(a, b):
+                    return float(SI.integrate_monomial(power, m, n, a, b))
+
+                want = integrate.dblquad(lambda v, u: u**m * v**n * (u * u + v * v) ** (power / 2), a0, a1, b0, b1,
+                                         epsabs=0, epsrel=1e-13)[0]
+                got = G(a1, b1) - G(a0, b1) - G(a1, b0) + G(a0, b0)
+                assert got == pytest.approx(want, rel=1e-11)
+
+
+@pytest.mark.parametrize("power", [-1, 1, 3])
+def test_monomial_integrals_are_homogeneous(power):
+    for m in range(4):
+        for n in range(2):
+            G = lambda a, b: float(SI.integrate_monomial(power, m, n, a, b))  # noqa: E731
+            assert G(0.9, 2.4) == pytest.approx(3.0 ** (m + n + power + 2) * G(0.3, 0.8), rel=1e-14)
+
+
+@pytest.mark.parametrize("power", [-1, 1, 3])
+def test_monomial_integrals_exchange_their_arguments(power):
+    G = lambda m, n, a, b: float(SI.integrate_monomial(power, m, n, a, b))  # noqa: E731
+    assert G(0, 1, 0.3, 0.7) == pytest.approx(G(1, 0, 0.7, 0.3), rel=1e-14)
+    assert G(1, 1, 0.3, 0.7) == pytest.approx(G(1, 1, 0.7, 0.3), rel=1e-14)
+
+
+def test_extracted_moments_combine_the_power_moments():
+    # tests/+unit/+assembler/+singularIntegrals/GenerateExtractedMomentsTest.m:5-18
+    a, b = 0.1, 0.15
+    want = SI.power_moments(a, b, -1) - K**2 / 2 * SI.power_moments(a, b, 1) + K**4 / 24 * SI.power_moments(a, b, 3)
+    np.testing.assert_allclose(SI.extracted_moments(a, b, K), want, rtol=1e-15)
+    np.testing.assert_array_equal(SI.extracted_moments(a, b, 0.0), SI.power_moments(a, b, -1))
