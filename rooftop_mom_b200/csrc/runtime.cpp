@@ -38,12 +38,17 @@ static std::mutex g_budget_mu;
 static double g_ceiling = 0.0;  // <= 0: none
 static double g_held = 0.0;
 
+// A byte count as the reference's messages write it (src/+rooftopMoM/+resources/+utils/formatBytes.m):
+// whole bytes below 1 kB, else one decimal in kB, MB, GB or TB (powers of 1024); an infinite count (no
+// ceiling) reads "unlimited", an unknown one "unknown".
 static std::string format_bytes(double b) {
-    const char* units[] = {"B", "KB", "MB", "GB", "TB"};
-    int u = 0;
-    while (b >= 1024.0 && u < 4) { b /= 1024.0; ++u; }
+    if (std::isinf(b)) return "unlimited";
+    if (std::isnan(b)) return "unknown";
+    const char* units[] = {"B", "kB", "MB", "GB", "TB"};
+    const int e = std::min(std::max((int)std::floor(std::log2(std::max(b, 1.0)) / 10), 0), 4);
     char buf[64];
-    snprintf(buf, sizeof buf, "%.1f %s", b, units[u]);
+    if (e == 0) snprintf(buf, sizeof buf, "%.0f B", std::round(b));
+    else snprintf(buf, sizeof buf, "%.1f %s", b / std::pow(1024.0, e), units[e]);
     return buf;
 }
 

@@ -128,3 +128,22 @@ def test_input_impedance_rejects_ports_outside_the_rooftops(library):
         port = (C.c_int64 * 2)(1, bad)
         assert lib.rtm_input_impedance(4, 3, 0.1, 0.2, current, port, 2, 1.0, _lib.HOST, out) == _lib.ERR_ARG
         assert "rooftop indices below 17" in _lib.last_error()
+
+
+def test_memory_messages_format_bytes_as_the_reference():
+    """The ceiling message of Budget.require (Budget.m:93-97) with byte counts written as formatBytes.m and
+    its tests (tests/+unit/+resources/+utils/FormatBytesTest.m:5-11) write them: whole bytes, then one
+    decimal in kB, MB, GB, TB. The ceiling check comes before any device query; nothing is held here."""
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    cases = [(512.0, 1536.0, "1.5 kB", "512 B"), (3 * 2 ** 30, 4 * 2 ** 30, "4.0 GB", "3.0 GB"),
+             (2 ** 20, 1.5 * 2 ** 20, "1.5 MB", "1.0 MB")]
+    try:
+        for ceiling, need, need_text, ceiling_text in cases:
+            assert lib.rtm_budget_configure(ceiling) == 0
+            assert lib.rtm_budget_require(need) == _lib.ERR_OOM_BUDGET
+            assert _lib.last_error() == (f"The request needs {need_text}, but only {ceiling_text} of the memory "
+                                         f"ceiling of {ceiling_text} are left.")
+    finally:
+        lib.rtm_budget_configure(0.0)
