@@ -38,6 +38,24 @@ def _vec_in(x, n: int, dtype=np.complex128):
     return a.ctypes.data_as(C.c_void_p), L.HOST, a
 
 
+def format_bytes(count: float) -> str:
+    """A byte count as the reference's messages write it (src/+rooftopMoM/+resources/+utils/formatBytes.m)."""
+    if math.isinf(count):
+        return "unlimited"
+    if math.isnan(count):
+        return "unknown"
+    units = ("B", "kB", "MB", "GB", "TB")
+    e = min(max(math.floor(math.log2(max(count, 1.0)) / 10), 0), len(units) - 1)
+    return f"{round(count)} B" if e == 0 else f"{count / 1024 ** e:.1f} {units[e]}"
+
+
+def assembly_bytes(countX: int, countY: int):
+    """(generators, working) device bytes of an assembly: the three generators (estimateGenerators.m:11) and
+    the 28 lattice-block sums and 7 moment terms of each of the (countX + 1)(countY + 1) blocks."""
+    rooftops = (countX - 1) * countY + countX * (countY - 1)
+    return 16.0 * (rooftops + countX * countY), 16.0 * 35 * (countX + 1) * (countY + 1)
+
+
 def fast_fft_size(count: int) -> int:
     """generateFastFFTSize.m:11-15."""
     n = int(count)
@@ -86,6 +104,15 @@ class Mesh:
         return a * b + c * d
 
 
+def _modifier_key(modifier):
+    """'real' or 'imag' for a modifier given by name or as np.real / np.imag (Generators.m:25-37)."""
+    if modifier is np.real or modifier == "real":
+        return "real"
+    if modifier is np.imag or modifier == "imag":
+        return "imag"
+    raise _err("rooftopMoM:operator:invalidModifier", "The modifier is 'real', 'imag' or None.")
+
+
 class Generators:
     """Generators.m: the three Toeplitz generators, held on the device."""
 
@@ -107,9 +134,7 @@ class Generators:
 
     def modify(self, modifier):
         """Generators.modify with 'real' / 'imag' (or np.real / np.imag)."""
-        key = {np.real: "real", np.imag: "imag"}.get(modifier, modifier)
-        if key not in L.MODIFIERS:
-            raise _err("rooftopMoM:operator:invalidModifier", "The modifier is 'real', 'imag' or None.")
+        key = _modifier_key(modifier)
         out = C.c_void_p()
         L.call("rtm_generators_modify", self._h, L.MODIFIERS[key], C.byref(out))
         return Generators(out, self._mesh)
@@ -171,6 +196,20 @@ class Problem:
         self._k = float(wavenumber)
         self._orders = (int(orders[0]), int(orders[-1]))
         self._generators = None
+        self._require_assembly()
+
+    def _require_assembly(self):
+        """Problem.m:77 and :210-219: the generators and the assembly's working arrays must fit below the
+        memory ceiling already when the problem is made (the assembly checks the device's free memory too)."""
+        ceiling, held = C.c_double(), C.c_double()
+        L.call("rtm_budget_query", C.byref(ceiling), C.byref(held))
+        gen, work = assembly_bytes(*self._mesh.count())
+        if ceiling.value > 0 and held.value + gen + work > ceiling.value:
+            raise RtmError(L.ERR_OOM_BUDGET,
+                           f"The assembly of {self.rooftopCount()} rooftops (generators {format_bytes(gen)}, chunk "
+                           f"{format_bytes(work)}) needs {format_bytes(gen + work)}, but only "
+                           f"{format_bytes(max(0.0, ceiling.value - held.value))} of the memory ceiling of "
+                           f"{format_bytes(ceiling.value)} are left.", "rooftopMoM:resources:insufficientMemory")
 
     @staticmethod
     def fromElectricalSize(electricalSize, density=10, aspect=1, quadratureOrder=(16, 8), chunkSize=None):
@@ -277,6 +316,8 @@ class Operator(_Product):
             raise _err("rooftopMoM:operator:invalidProduct", "The product is 'fft', 'splitFFT' or 'leanSplitFFT'.")
         if precision not in L.PRECISIONS:
             raise _err("rooftopMoM:operator:invalidPrecision", "The precision is 'double' or 'single'.")
+        if modifier is not None:
+            _modifier_key(modifier)
         gen = problem.generators()
         if modifier is not None:
             gen = gen.modify(modifier)
@@ -358,6 +399,8 @@ class Preconditioner(_Product):
             if not np.all((bw_values >= 1) & (bw_values == np.floor(bw_values))):
                 raise _err("rooftopMoM:preconditioner:invalidBandwidth", "The bandwidths are positive integers.")
             bw = (C.c_int * 2)(int(bw_values[0]), int(bw_values[1]))
+        if modifier is not None:
+            _modifier_key(modifier)
         gen = problem.generators()
         if modifier is not None:
             gen = gen.modify(modifier)

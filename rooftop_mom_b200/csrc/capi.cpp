@@ -229,12 +229,18 @@ int rtm_generators_assemble(int count_x, int count_y, double size_x, double size
                             int far_order, void* stream, rtm_generators** out) {
     if (!out) return fail(RTM_ERR_ARG, "null output handle");
     *out = nullptr;
+    if (count_x < 1 || count_y < 1) return fail(RTM_ERR_ARG, "invalid grid");
+    // Problem.m:210-219 (requireAssembly_): the generators and the assembly's working arrays, here the 28
+    // lattice-block sums and the 7 moment terms of every block, must fit before anything is built
+    const double rooftops = (double)(count_x - 1) * count_y + (double)count_x * (count_y - 1);
+    const double gen_bytes = 16.0 * (rooftops + (double)count_x * count_y);
+    const double work_bytes = 16.0 * 35 * (count_x + 1.0) * (count_y + 1.0);
+    const std::string subject = "The assembly of " + std::to_string((long long)rooftops) + " rooftops (generators " +
+                                format_bytes(gen_bytes) + ", chunk " + format_bytes(work_bytes) + ")";
+    RTM_TRY(budget_require(gen_bytes + work_bytes, subject.c_str()));
     auto h = std::make_unique<rtm_generators>();
     RTM_CUDA(cudaGetDevice(&h->device));
     RTM_TRY(make_stream(&h->stream));
-    const double gen_bytes = 16.0 * ((double)(count_x - 1) * count_y + (double)count_x * (count_y - 1) +
-                                     (double)count_x * count_y);
-    RTM_TRY(budget_require(gen_bytes + 16.0 * 35 * (count_x + 1.0) * (count_y + 1.0), "The assembly"));
     RTM_TRY(assemble_generators(count_x, count_y, size_x, size_y, wavenumber, near_order, far_order, h->g,
                                 pick(stream, h->stream)));
     if (stream) RTM_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));

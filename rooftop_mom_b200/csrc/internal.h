@@ -54,6 +54,8 @@ struct DeviceOnce {
 // ---------------------------------------------------------------------------------------------
 // Budget ledger of device bytes (Budget.m). Thread-safe.
 int budget_require(double bytes, const char* what);
+// A byte count as the reference's messages write it (formatBytes.m): "512 B", "1.5 kB", "3.0 GB".
+std::string format_bytes(double bytes);
 void budget_hold(double bytes);
 void budget_release(double bytes);
 // Returns the cached idle blocks of the current device to the driver.

@@ -41,7 +41,7 @@ static double g_held = 0.0;
 // A byte count as the reference's messages write it (src/+rooftopMoM/+resources/+utils/formatBytes.m):
 // whole bytes below 1 kB, else one decimal in kB, MB, GB or TB (powers of 1024); an infinite count (no
 // ceiling) reads "unlimited", an unknown one "unknown".
-static std::string format_bytes(double b) {
+std::string format_bytes(double b) {
     if (std::isinf(b)) return "unlimited";
     if (std::isnan(b)) return "unknown";
     const char* units[] = {"B", "kB", "MB", "GB", "TB"};
