@@ -263,3 +263,19 @@ def test_batched_product_equals_single_products():
     ys = op.apply(np.concatenate(vs), nrhs=4)
     for k in range(4):
         assert rel(ys[k * n:(k + 1) * n], op.apply(vs[k])) < 1e-15 + 1e-14
+
+
+@pytest.mark.parametrize("kernel", ["rChan", "tChan"])
+def test_a_singular_circulant_raises(kernel):
+    """+unit/PreconditionerTest.m:57-60: generators that vanish make every block spectrum zero, so the
+    circulant cannot be inverted (rooftopMoM:preconditioner:singular)."""
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    mesh = R.Mesh(5, 4, 0.1, 0.15)
+    prob = R.Problem(mesh, 2 * np.pi, quadratureOrder=3)
+    prob.setGenerators(R.Generators.fromArrays(mesh, np.zeros((4, 4), complex), np.zeros((5, 3), complex),
+                                               np.zeros((5, 4), complex)))
+    with pytest.raises(L.RtmError) as e:
+        R.Preconditioner(prob, kernel=kernel)
+    assert e.value.identifier == "rooftopMoM:preconditioner:singular"
