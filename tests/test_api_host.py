@@ -218,3 +218,17 @@ def test_invalid_preconditioners_raise_before_any_device_work():
         with pytest.raises(RtmError) as e:
             Preconditioner(problem, kernel="huckle", bandwidth=bandwidth)
         assert e.value.identifier == "rooftopMoM:preconditioner:invalidBandwidth"
+
+
+def test_invalid_operators_raise_before_any_device_work():
+    # tests/+unit/OperatorTest.m:35-38, and the modifier of Operator.m / Generators.modify
+    from rooftop_mom_b200 import Operator
+
+    problem = Problem(Mesh(8, 8, 0.05, 0.05), 2 * math.pi, quadratureOrder=3)
+    for kwargs, identifier in (({"product": "dense"}, "rooftopMoM:operator:invalidProduct"),
+                               ({"precision": "half"}, "rooftopMoM:operator:invalidPrecision"),
+                               ({"modifier": "abs"}, "rooftopMoM:operator:invalidModifier"),
+                               ({"modifier": np.abs}, "rooftopMoM:operator:invalidModifier")):
+        with pytest.raises(RtmError) as e:
+            Operator(problem, **kwargs)
+        assert e.value.identifier == identifier
