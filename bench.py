@@ -406,9 +406,22 @@ def peaks():
 
 # ---------------------------------------------------------------------------------------------
 # CPU leg: the oracle (numpy/scipy restatement of the reference's MATLAB path) on the host cores.
+def cpu_matvec_ms(apply, v):
+    """The oracle's product timed as benchmarks/measureThreadScaling.m:58-74 times it: one warm-up, then the
+    median of 5 (milliseconds)."""
+    apply(v)
+    times = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        apply(v)
+        times.append(time.perf_counter() - t0)
+    return float(np.median(times)) * 1e3
+
+
 def cpu_sample(w, iterations_gpu, sample_iterations=25):
-    """Times the oracle's setup (assembly, spectra, block-Jacobi, plane wave) and a bounded number of
-    its GMRES iterations; a full solve is setup + iterations_gpu x per-iteration time."""
+    """Times the oracle's setup (assembly, spectra, block-Jacobi, plane wave), its product and a bounded
+    number of its GMRES iterations; a full solve is setup + iterations_gpu x per-iteration time. Returns
+    (setup s, iteration s, product ms)."""
     from oracle import assembly as A, blockjacobi as BJ, excitation as EX, geometry as G, solvers as OS, spectra as S
 
     n, h, k = w["n"], 1.0 / w["density"], 2 * math.pi
@@ -430,11 +443,11 @@ def cpu_sample(w, iterations_gpu, sample_iterations=25):
         Ar = (lambda v: apply(pc(v))) if pc else apply
         OS.gmres_iterate(Ar, b, None, 1e-300, m, w["restart"])
     t_iter = (time.perf_counter() - t0) / m
-    return t_setup, t_iter
+    return t_setup, t_iter, cpu_matvec_ms(apply, b)
 
 
 def cpu_full_solve(w):
-    """A whole oracle solve of a small plate, to its tolerance: (seconds, iterations)."""
+    """A whole oracle solve of a small plate, to its tolerance: (seconds, iterations, product ms)."""
     from oracle import assembly as A, blockjacobi as BJ, excitation as EX, geometry as G, solvers as OS, spectra as S
 
     n, h, k = w["n"], 1.0 / w["density"], 2 * math.pi
@@ -445,9 +458,11 @@ def cpu_full_solve(w):
     pc = BJ.BlockJacobi(gen, rt, 2, 2).apply if w["pc"] == "blockJacobi" else None
     d, p = plane_wave_vectors(w["theta"], w["phi"], w["pol"])
     b = EX.plane_wave(rt, k, d, p, 1.0)
-    out = OS.solve("cg" if w["method"] == "cg" else "gmres", lambda v: S.split_apply(rt, sub, rt.content, v), b,
-                   tol=w["tol"], maxit=20000, restart=w["restart"], precond=pc)
-    return time.perf_counter() - t0, out.iteration_count
+    apply = lambda v: S.split_apply(rt, sub, rt.content, v)  # noqa: E731
+    out = OS.solve("cg" if w["method"] == "cg" else "gmres", apply, b, tol=w["tol"], maxit=20000,
+                   restart=w["restart"], precond=pc)
+    t_solve = time.perf_counter() - t0
+    return t_solve, out.iteration_count, cpu_matvec_ms(apply, b)
 
 
 # Plates small enough for the CPU legs to run whole solves instead of extrapolating a sample.
@@ -463,9 +478,9 @@ def run_reference(args, w):
     times = []
     for step in range(args.warmup + args.steps):
         if full:
-            t_step, iters = cpu_full_solve(w)
+            t_step, iters, mv_ms = cpu_full_solve(w)
         else:
-            t_setup, t_iter = cpu_sample(w, iters, sample_iterations=10)
+            t_setup, t_iter, mv_ms = cpu_sample(w, iters, sample_iterations=10)
             t_step = t_setup + iters * t_iter
         if step >= args.warmup:
             times.append(t_step)
@@ -486,7 +501,8 @@ def run_reference(args, w):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": config_of(args, w),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
+                         "matvec_ms": mv_ms},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -685,16 +701,16 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         if w["n"] <= FULL_SOLVE_MAX_FACES:
-            t_cpu, cpu_its = cpu_full_solve(w)
+            t_cpu, cpu_its, mv_ms = cpu_full_solve(w)
             sample = f"one whole oracle solve: assembly, spectra, plane wave and {cpu_its} iterations (measured)"
         else:
-            t_setup, t_iter = cpu_sample(w, its[0], sample_iterations=20)
+            t_setup, t_iter, mv_ms = cpu_sample(w, its[0], sample_iterations=20)
             t_cpu = t_setup + its[0] * t_iter
             sample = (f"oracle setup (assembly, spectra, preconditioner, plane wave) timed once, plus 20 iterations "
                       f"timed and scaled to the GPU solve's {its[0]} iterations: {t_setup:.2f} s + "
                       f"{its[0]} x {t_iter * 1e3:.1f} ms (extrapolated)")
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-                                "sample": sample}
+                                "sample": sample, "matvec_ms": mv_ms}
     if rank == 0 and world == 1 and w["precision"] == "mixed":
         line["error_vs_fp64"] = precision_error(R, w)
     if dist:
