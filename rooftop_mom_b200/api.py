@@ -254,6 +254,12 @@ class Problem:
             self._generators = Generators(out, self._mesh)
         return self._generators
 
+    def memory(self):
+        """Problem.m:147-155: the bytes of the generators, zero before they are assembled."""
+        if self._generators is None:
+            return 0.0
+        return assembly_bytes(*self._mesh.count())[0]
+
     def setGenerators(self, generators: Generators):
         """Uses given generators instead of assembling them (e.g. the reference's stored ones)."""
         self._generators = generators

@@ -232,3 +232,9 @@ def test_invalid_operators_raise_before_any_device_work():
         with pytest.raises(RtmError) as e:
             Operator(problem, **kwargs)
         assert e.value.identifier == identifier
+
+
+def test_problem_memory_is_zero_before_the_assembly():
+    # Problem.m:147-155: the bytes of the generators once assembled, zero before
+    problem = Problem(Mesh(4, 3, 0.1, 0.1), 2 * math.pi, quadratureOrder=3)
+    assert problem.memory() == 0.0
