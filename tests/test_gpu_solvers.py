@@ -238,3 +238,20 @@ def test_bistatic_rcs_is_reciprocal():
     sAB = rA.bistaticRadarCrossSection([-dB], [pB])[0]
     sBA = rB.bistaticRadarCrossSection([-dA], [pA])[0]
     assert sAB == pytest.approx(sBA, rel=1e-8)
+
+
+@pytest.mark.parametrize("method", ["cg", "gmres"])
+def test_a_non_finite_right_hand_side_on_the_device_is_not_converged(method):
+    """A right-hand side with a NaN, passed as a device tensor (which the API does not read back to check), ends
+    the solve unconverged within its iteration limit: COCG stops on the non-finite residual
+    (ConjugateGradient.m:55-58), GMRES runs out its iterations; neither raises."""
+    import torch
+
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(8, 8, 0.05, 0.05), 2 * np.pi, quadratureOrder=3)
+    b = torch.ones(prob.rooftopCount(), dtype=torch.complex128, device="cuda")
+    b[3] = float("nan")
+    res = R.Solver(method=method, tolerance=1e-6, maxIterationCount=20, restart=10).solve(R.Operator(prob), b)
+    assert not res.converged()
+    assert res.iterationCount() <= 20
