@@ -677,6 +677,16 @@ class Solver:
                 if not finite:
                     raise _err("rooftopMoM:solver:invalidRightHandSide",
                                "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+        if initialGuess is not None and not _is_device(initialGuess):
+            # Solver.m:62: the initial guess is numeric and finite
+            try:
+                g = np.asarray(initialGuess)
+                finite = g.dtype.kind in "biufc" and bool(np.all(np.isfinite(g)))
+            except (TypeError, ValueError):
+                finite = False
+            if not finite:
+                raise _err("rooftopMoM:solver:invalidInitialGuess", "The initial guess is a numeric vector of finite "
+                                                                     "values.")
         if not isinstance(operator, (np.ndarray, _Product)):
             raise _err("rooftopMoM:solver:invalidOperator",
                        "The operator is a rooftopMoM.Operator, a DenseOperator or a numeric matrix.")

@@ -187,6 +187,10 @@ def test_invalid_solvers_and_solver_inputs_raise():
         with pytest.raises(RtmError) as e:
             solver.solve(np.eye(3), rhs)
         assert e.value.identifier == "rooftopMoM:solver:invalidRightHandSide"
+    for guess in (np.array([1, np.inf, 1]), ["a", "b", "c"]):
+        with pytest.raises(RtmError) as e:
+            solver.solve(np.eye(3), np.ones(3), initialGuess=guess)
+        assert e.value.identifier == "rooftopMoM:solver:invalidInitialGuess"
 
 
 def test_result_quantities_need_their_excitation():
