@@ -1,7 +1,7 @@
 /*
  * rtm.h - C ABI of librtm.so, the B200 (sm_100a) solve path of rooftop-mom.
  *
- * A thin MEX gateway binds these entry points under the unchanged MATLAB
+ * A thin MEX gateway (mex/rtm_mex.c) binds these entry points under the unchanged MATLAB
  * +rooftopMoM call signatures; the tests bind them through Python ctypes.
  *
  * Conventions
@@ -138,9 +138,12 @@ RTM_API int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t
  * (rtm_fixed_scratch_bytes, 32 MiB) instead of the operator's own buffer. No counterpart in the
  * reference: it exists for callers whose device memory belongs to another allocator or ledger and
  * that must not allocate per call. FFT products only; RTM_ERR_SIZE when the working grids of nrhs
- * vectors exceed the array. The first call on a device looks the array up (make it before any stream
- * capture). All calls on a device share the array: calls that can overlap in time race, so the
- * caller serialises them. A null stream runs on the operator's stream and waits for the result. */
+ * vectors exceed the array. The array takes 32 MiB of device memory on each device where it is first
+ * looked up (the first call there; under CUDA_MODULE_LOADING=EAGER, every context of the process) and
+ * keeps it until the process exits, outside the budget ledger. Every call looks the array's address up
+ * again; the first call on a device loads it, so make that call before any stream capture. All calls
+ * on a device share the array: calls that can overlap in time race, so the caller serialises them. A
+ * null stream runs on the operator's stream and waits for the result. */
 RTM_API int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void* x, void* y, int64_t n, int nrhs,
                                              void* stream);
 /* Size of the fixed scratch array in bytes. */

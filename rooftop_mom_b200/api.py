@@ -671,17 +671,18 @@ class Solver:
             if not _is_device(b):
                 try:
                     a = np.asarray(b)
-                    finite = a.dtype.kind in "biufc" and bool(np.all(np.isfinite(a)))
+                    # Solver.m:162-168: isnumeric, which logical arrays are not
+                    finite = a.dtype.kind in "iufc" and bool(np.all(np.isfinite(a)))
                 except (TypeError, ValueError):
                     finite = False
                 if not finite:
                     raise _err("rooftopMoM:solver:invalidRightHandSide",
                                "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
         if initialGuess is not None and not _is_device(initialGuess):
-            # Solver.m:62: the initial guess is numeric and finite
+            # Solver.m:62: mustBeNumeric (which rejects logical arrays) and mustBeFinite
             try:
                 g = np.asarray(initialGuess)
-                finite = g.dtype.kind in "biufc" and bool(np.all(np.isfinite(g)))
+                finite = g.dtype.kind in "iufc" and bool(np.all(np.isfinite(g)))
             except (TypeError, ValueError):
                 finite = False
             if not finite:

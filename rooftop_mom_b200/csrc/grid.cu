@@ -438,46 +438,22 @@ int GridApplicator::apply(const void* x, void* y, int nrhs, cudaStream_t s, Skip
 }
 
 // ---------------------------------------------------------------------------------------------
-// Fixed scratch: a working grid W in a file-scope device array, for callers that must not allocate
-// device memory per call. Such callers are the ones whose device memory is owned by someone else: a
-// MATLAB MEX gateway whose gpuArray memory pool already holds the device, or a serving process
-// whose admission ledger has handed out all of HBM and cannot let a call take more behind its back.
-// Every call on a device shares the one array, so calls that may overlap in time (other streams,
-// other host threads) race on it: the caller serialises them. Nothing in it has to start at zero:
-// the y-forward pass writes every entry of W that the later passes read.
-constexpr size_t kFixedScratchBytes = size_t(32) << 20;  // 32 MiB
-static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
-
-// The array's address per device, looked up on the first call with that device current (the lookup
-// may load the module on the device, so make that first call before any stream capture).
-static int fixed_scratch(void** out) {
-    static std::mutex mu;
-    static void* addr[64] = {};
-    int dev = 0;
-    RTM_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return fail(RTM_ERR_UNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_fixed_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fixed_scratch)");
-        addr[dev] = p;
-    }
-    *out = addr[dev];
-    return RTM_OK;
-}
-
-size_t fixed_scratch_bytes() { return kFixedScratchBytes; }
+// Fixed scratch: the working grid W in the library's fixed device array (fixed_scratch.cu) instead of
+// the product's own buffer. Every call on a device shares the one array, so calls that may overlap in
+// time (other streams, other host threads) race on it: the caller serialises them. Nothing in it has
+// to start at zero: the y-forward pass writes every entry of W that the later passes read.
+int fixed_scratch_address(void** out);
 
 int apply_fixed_scratch(const GridApplicator& g, const void* x, void* y, int nrhs, cudaStream_t s) {
     if (nrhs < 1) return fail(RTM_ERR_ARG, "nrhs must be positive");
     const size_t need = g.work_bytes_per_rhs() * (size_t)nrhs;
-    if (need > kFixedScratchBytes)
+    const size_t cap = fixed_scratch_bytes();
+    if (need > cap)
         return fail(RTM_ERR_SIZE, "the working grid of " + std::to_string(nrhs) + " right-hand sides needs " +
                                       std::to_string(need) + " bytes, above the fixed scratch of " +
-                                      std::to_string(kFixedScratchBytes) + " bytes");
+                                      std::to_string(cap) + " bytes");
     void* work = nullptr;
-    if (g.mode != kStrip) RTM_TRY(fixed_scratch(&work));
+    if (g.mode != kStrip) RTM_TRY(fixed_scratch_address(&work));
     return g.precision == RTM_FP64 ? apply_t<double>(g, x, y, nrhs, s, SkipFlags{}, work)
                                    : apply_t<float>(g, x, y, nrhs, s, SkipFlags{}, work);
 }

@@ -139,28 +139,34 @@ struct rtm_server {
                 r = records.at(ready.front()).get();
                 ready.pop_front();
                 if (r->cancel) {
+                    // Cancelled while admitted: give its bytes and slot back in this same critical
+                    // section. Once the state reads CANCELLED a poll with release may erase the
+                    // record, so nothing touches r after the lock is dropped.
                     r->res.state = RTM_REQUEST_CANCELLED;
                     r->res.finished_s = seconds_since(epoch);
-                } else {
-                    r->res.state = RTM_REQUEST_RUNNING;
-                    r->res.started_s = seconds_since(epoch);
+                    held -= r->res.bytes;
+                    --admitted;
+                    admit_locked();
+                    lk.unlock();
+                    done_cv.notify_all();
+                    continue;
                 }
+                r->res.state = RTM_REQUEST_RUNNING;
+                r->res.started_s = seconds_since(epoch);
             }
-            int st = RTM_OK;
+            // RUNNING is not a finished state, so no poll releases the record while it runs.
             Outcome out;
-            if (r->res.state == RTM_REQUEST_RUNNING) st = run(*r, out);
+            const int st = run(*r, out);
             {
                 std::lock_guard<std::mutex> lk(mu);
-                if (r->res.state == RTM_REQUEST_RUNNING) {
-                    out.commit(r->res);
-                    r->current = std::move(out.current);
-                    r->res.finished_s = seconds_since(epoch);
-                    r->res.status = st;
-                    r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
-                                             : (st == RTM_OK ? RTM_REQUEST_DONE : RTM_REQUEST_FAILED);
-                }
+                out.commit(r->res);
+                r->current = std::move(out.current);
+                r->res.finished_s = seconds_since(epoch);
+                r->res.status = st;
                 held -= r->res.bytes;
                 --admitted;
+                r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
+                                         : (st == RTM_OK ? RTM_REQUEST_DONE : RTM_REQUEST_FAILED);
                 admit_locked();
             }
             done_cv.notify_all();

@@ -1,5 +1,5 @@
 /* Declarations of the parts of MATLAB's documented C API (matrix.h / mex.h, interleaved complex, R2018a+)
- * that the MEX gateway in INTEGRATION.md uses, so that tests/test_c_consumer.py can compile the gateway
+ * that the MEX gateway mex/rtm_mex.c uses, so that tests/test_c_consumer.py can compile the gateway
  * for a syntax and type check where MATLAB is not installed. A stand-in for checking only: a real build
  * uses MATLAB's own mex.h through `mex -R2018a`. */
 #ifndef RTM_TEST_MEX_STUB_H

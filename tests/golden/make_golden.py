@@ -11,7 +11,7 @@ T. Chan preconditioned vectors, a plane wave, and for the first grid the dense i
 R^-1, R, R^3 over five cells at the four touching offsets to 30 digits
 (tests/data/generateExactMoments.py of the reference).
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>
 """
 from __future__ import annotations
 
@@ -56,4 +56,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference_root>")
+    main(sys.argv[1])

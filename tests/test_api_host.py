@@ -183,11 +183,11 @@ def test_invalid_solvers_and_solver_inputs_raise():
     with pytest.raises(RtmError) as e:
         solver.solve("matrix", np.ones(3))
     assert e.value.identifier == "rooftopMoM:solver:invalidOperator"
-    for rhs in (np.array([1, np.nan, 3]), ["a", "b", "c"]):
+    for rhs in (np.array([1, np.nan, 3]), ["a", "b", "c"], np.array([True, False, True])):
         with pytest.raises(RtmError) as e:
             solver.solve(np.eye(3), rhs)
         assert e.value.identifier == "rooftopMoM:solver:invalidRightHandSide"
-    for guess in (np.array([1, np.inf, 1]), ["a", "b", "c"]):
+    for guess in (np.array([1, np.inf, 1]), ["a", "b", "c"], np.array([True, False, True])):
         with pytest.raises(RtmError) as e:
             solver.solve(np.eye(3), np.ones(3), initialGuess=guess)
         assert e.value.identifier == "rooftopMoM:solver:invalidInitialGuess"

@@ -2,7 +2,7 @@
 it, and a C program linked against librtm.so calls the entry points that need no GPU: the version, the byte
 models (against the oracle), the size of the fixed scratch array, a delta gap built in host memory (against
 the oracle), the status and message of two rejected calls, and the serving loop's create / submit / poll /
-destroy with a request that fails at submission. The MEX gateway of INTEGRATION.md compiles against the
+destroy with a request that fails at submission. The MEX gateway mex/rtm_mex.c compiles against the
 header."""
 from __future__ import annotations
 
@@ -82,17 +82,13 @@ def test_rejected_calls_report_status_and_message(consumer):
     assert "65535" in " ".join(consumer["rhs"][1:])
 
 
-def test_the_mex_gateway_of_the_integration_notes_compiles_against_the_header(tmp_path):
-    """The C gateway written out in INTEGRATION.md, compiled for syntax and types against include/rtm.h and a
-    stand-in for MATLAB's mex.h: a signature that drifts from the header fails here."""
+def test_the_mex_gateway_compiles_against_the_header():
+    """The C gateway mex/rtm_mex.c, compiled for syntax and types against include/rtm.h and a stand-in for
+    MATLAB's mex.h: a signature that drifts from the header fails here."""
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    section = text.split("## MEX gateway", 1)[1]
-    source = section.split("```c\n", 1)[1].split("```", 1)[0]
-    assert "mexFunction" in source
-    path = tmp_path / "rtm_mex.c"
-    path.write_text(source)
+    path = os.path.join(ROOT, "mex", "rtm_mex.c")
+    assert "mexFunction" in open(path).read()
     subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-Wall", "-Wextra", "-Werror",
-                    "-I", os.path.join(ROOT, "tests", "c", "mex_stub"), "-I", os.path.join(ROOT, "include"), str(path)],
+                    "-I", os.path.join(ROOT, "tests", "c", "mex_stub"), "-I", os.path.join(ROOT, "include"), path],
                    check=True, capture_output=True, text=True)

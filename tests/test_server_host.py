@@ -105,3 +105,53 @@ def test_requests_that_fail_on_the_device_release_their_slot_and_bytes():
         assert all(r["finished"] >= r["started"] >= r["submitted"] for r in results)
         # the released bytes admit a later request too
         assert srv.poll(srv.submit(_request()), wait=60.0)["state"] == "failed"
+
+
+def test_cancelled_admitted_requests_release_their_bytes_under_concurrent_polls():
+    """A request cancelled after admission, before a worker starts it, gives its slot and bytes back in the
+    same step that marks it cancelled, so a poll that releases the finished record in the meantime cannot
+    race the ledger. Many requests are submitted and cancelled at once while a second thread polls each
+    with release in a loop; afterwards the whole budget must be free again: a request that needs nearly all
+    of it is admitted and reaches a finished state."""
+    import threading
+
+    import torch
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    if torch.cuda.is_available():
+        pytest.skip("on a GPU these requests run; this test follows the host path of cancelled requests")
+    with R.Server(budgetBytes=1.0, maxActive=1) as probe:
+        one = probe.poll(probe.submit(_request()))["bytes"]
+    with R.Server(budgetBytes=4.5 * one, maxActive=4) as srv:
+        for _ in range(5):
+            ids = [srv.submit(_request()) for _ in range(24)]
+            seen = {}
+
+            def poller():
+                pending = list(ids)
+                while pending:
+                    rest = []
+                    for rid in pending:
+                        res = srv.poll(rid, release=True)
+                        if res["state"] in ("done", "failed", "cancelled"):
+                            seen[rid] = res["state"]
+                        else:
+                            rest.append(rid)
+                    pending = rest
+
+            t = threading.Thread(target=poller)
+            t.start()
+            for rid in ids:
+                try:
+                    srv.cancel(rid)
+                except L.RtmError as e:  # the poller already released this finished request
+                    assert "unknown request" in str(e)
+            t.join(timeout=120)
+            assert not t.is_alive()
+            assert sorted(seen) == sorted(ids)
+            assert set(seen.values()) <= {"failed", "cancelled"}
+        # every released byte is back: four requests' worth fits again
+        big = [srv.submit(_request()) for _ in range(4)]
+        assert all(srv.poll(rid, wait=60.0)["state"] in ("failed", "cancelled") for rid in big)
