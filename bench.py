@@ -50,7 +50,7 @@ WORKLOADS = {
     "c4": dict(n=512, density=20, rhs=64, seed=0, method="cg", tol=1e-6, restart=30, pc="rChan",
                precision="double", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
-    "c5": dict(n=0, density=0, seed=0, method="cg/gmres", tol=1e-6, restart=50, pc="rChan/blockJacobi", precision="double",
+    "c5": dict(n=0, density=0, seed=0, method="cg", tol=1e-6, restart=50, pc="rChan", precision="double",
                theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
 }
 
@@ -105,8 +105,7 @@ def solve_batch(R, w, b=None):
 def serving_requests(R, count, seed):
     """The c5 request stream: faces Nx (and Ny) log-uniform in [16, 768]; with probability 1/2 a strip one
     face wide fed by a 1 V delta gap at its middle, else a plate under a random plane wave; cell lambda/N
-    with N ~ U[10, 25]; frequency ~ U[0.5, 3] GHz; to 1e-6 by rChan-preconditioned COCG where the face
-    grid admits the circulant, by block-Jacobi GMRES(50) elsewhere."""
+    with N ~ U[10, 25]; frequency ~ U[0.5, 3] GHz; to 1e-6 by rChan-preconditioned COCG."""
     rng = np.random.default_rng(seed)
     lo, hi = math.log(16), math.log(768)
     out = []
@@ -118,15 +117,9 @@ def serving_requests(R, count, seed):
         f = rng.uniform(0.5e9, 3e9)
         h = SPEED_OF_LIGHT / f / cells
         k = 2 * math.pi * f / SPEED_OF_LIGHT
-        # COCG with the rChan circulant where the face grid allows it (no prime factor above the FFT plans'
-        # largest radix), block-Jacobi GMRES(50) elsewhere
-        from rooftop_mom_b200.server import circulant_supported
-
-        if circulant_supported(nx, ny):
-            kw = dict(method="cg", preconditioner="rChan", tolerance=1e-6, maxIterationCount=20000)
-        else:
-            kw = dict(method="gmres", preconditioner="blockJacobi", tolerance=1e-6, restart=50,
-                      maxIterationCount=20000)
+        # COCG with the rChan circulant, the reference's default preconditioner (face counts with a large
+        # prime factor transform by Bluestein convolutions)
+        kw = dict(method="cg", preconditioner="rChan", tolerance=1e-6, maxIterationCount=20000)
         if strip:
             out.append(R.Request.deltaGap(nx, 1, h, h, k, portDirection="x", voltage=1.0, **kw))
         else:
@@ -178,8 +171,7 @@ def run_serving(args):
         "ms_per_step": span / len(reqs) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128" if prec == "double" else "c64/c128", "data": "synthetic request stream, seed 0",
         "config": {"workload": f"c5: {len(reqs)} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
-                               f"cell lambda/U[10,25], f U[0.5,3] GHz, COCG + rChan (or GMRES(50) + block-Jacobi "
-                               f"where the circulant's FFT sizes are not supported) to 1e-6, "
+                               f"cell lambda/U[10,25], f U[0.5,3] GHz, COCG + rChan to 1e-6, "
                                f"{args.serving_precision}", "slots": args.slots, "budget_bytes": 150e9,
                    "capacity_solves_per_s": capacity, "arrival_rate": rate},
         "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
@@ -343,6 +335,109 @@ def solve_plate(R, w, rhs_host=None):
     return prob, op, res, rcs
 
 
+# The precision form's inner solves aim no lower than this relative residual (an FP32 solve reaches it
+# safely); each refinement step's inner solve otherwise stops once the outer tolerance will be met.
+INNER_FLOOR = 1e-5
+# Right-hand sides of the batched arms: the workload's own wave and the rest drawn as the batching form
+# draws its waves (theta ~ U[0, 80] deg, phi ~ U[0, 360), TE / TM ~ Bernoulli(1/2), seed 0).
+BATCH_RHS = 16
+
+
+def batch_waves(w, count):
+    d, p = plane_wave_vectors(w["theta"], w["phi"], w["pol"])
+    dirs, pols = random_waves(count - 1, np.random.default_rng(0))
+    return np.vstack([d[None], dirs]), np.vstack([p[None], pols])
+
+
+def rcs_of(R, prob, b, x, k, n):
+    """Monostatic RCS of right-hand side k of a batched device solve (computeRadarCrossSection.m:18-19)."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib as L
+
+    out = C.c_double()
+    L.call("rtm_radar_cross_section", prob.wavenumber(), C.c_void_p(b[k * n:(k + 1) * n].data_ptr()),
+           C.c_void_p(x[k * n:(k + 1) * n].data_ptr()), n, 1.0, L.DEVICE, C.byref(out))
+    return out.value
+
+
+def solve_arm(R, w, mixed, dirs, pols):
+    """One step of an arm on the workload's plate: assembly, spectra, block-Jacobi (2 x 2 faces), the plane
+    waves on the device, the solve of all right-hand sides at once to the workload's FP64 true residual, and
+    the RCS of each. mixed: FP32 flexible GMRES(restart) with an FP32 product and FP32 block-Jacobi inside
+    FP64 iterative refinement; else FP64 right-preconditioned GMRES(restart). Returns (solutions as one
+    device tensor, results, RCS values)."""
+    import torch
+
+    prob = build_plate(R, w)
+    nrhs, n = len(dirs), prob.rooftopCount()
+    op = R.Operator(prob, maxRhs=nrhs)
+    b = batch_rhs(R, prob, dirs, pols)
+    if mixed:
+        inner = R.Operator(prob, precision="single", maxRhs=nrhs)
+        pc = R.Preconditioner.blockJacobi(prob, (2, 2), precision="single")
+        res = R.Solver(method="fgmres", tolerance=w["tol"], restart=w["restart"], innerTolerance=INNER_FLOOR,
+                       maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc, nrhs=nrhs)
+    else:
+        pc = R.Preconditioner.blockJacobi(prob, (2, 2))
+        res = R.Solver(method="gmres", tolerance=w["tol"], restart=w["restart"], maxIterationCount=20000,
+                       side="right").solve(op, b, preconditioner=pc, nrhs=nrhs)
+    res = res if isinstance(res, list) else [res]
+    x = torch.cat([r.solution().reshape(-1) for r in res]) if nrhs > 1 else res[0].solution().reshape(-1)
+    rcs = [rcs_of(R, prob, b, x, k, n) for k in range(nrhs)]
+    return x, res, rcs
+
+
+def time_arm(R, w, mixed, dirs, pols, steps, warmup):
+    """Solves/s of an arm (right-hand sides solved per second), CUDA events around `steps` steps."""
+    import torch
+
+    for _ in range(warmup):
+        solve_arm(R, w, mixed, dirs, pols)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = []
+    for _ in range(steps):
+        out.append(solve_arm(R, w, mixed, dirs, pols))
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    x, res, rcs = out[-1]
+    return {"value": len(dirs) * steps / t, "unit": "solves/s", "rhs": len(dirs), "steps": steps,
+            "ms_per_step": t / steps * 1e3,
+            "iterations": max(r.iterationCount() for r in res),
+            "refinements": max(r.refinements() for r in res) if mixed else 0,
+            "true_residual": max(r.residualNorm() for r in res),
+            "all_converged_to_tolerance": all(r.converged() and r.residualNorm() <= w["tol"] for r in res)}, x, rcs
+
+
+def precision_arms(R, w, steps, warmup):
+    """The metric's "mixed vs FP64" on the workload's plate: FP64 and mixed, one right-hand side and a batch
+    of BATCH_RHS, each to the FP64 true residual of the workload. Errors of the currents and RCS are taken
+    against an FP64 solve of the same right-hand sides driven to 1e-10."""
+    import torch
+
+    d1, p1 = batch_waves(w, 1)
+    dB, pB = batch_waves(w, BATCH_RHS)
+    arms = {}
+    sols = {}
+    for name, mixed, (dd, pp) in (("fp64", False, (d1, p1)), ("mixed", True, (d1, p1)),
+                                  ("fp64_batched", False, (dB, pB)), ("mixed_batched", True, (dB, pB))):
+        arms[name], x, rcs = time_arm(R, w, mixed, dd, pp, steps, warmup)
+        sols[name] = (x, rcs)
+    ref_w = dict(w, tol=1e-10)
+    xr, _, rcs_r = solve_arm(R, ref_w, False, dB, pB)
+    n = xr.numel() // BATCH_RHS
+    for name, (x, rcs) in sols.items():
+        cur = max(float((x[k * n:(k + 1) * n] - xr[k * n:(k + 1) * n]).norm() / xr[k * n:(k + 1) * n].norm())
+                  for k in range(len(rcs)))
+        rc = max(abs(a - b) / abs(b) for a, b in zip(rcs, rcs_r))
+        arms[name]["error_vs_fp64_1e-10"] = {"current_rel": cur, "rcs_rel": rc}
+    torch.cuda.synchronize()
+    return arms
+
+
 def precision_error(R, w):
     """The precision form's error: the mixed solve against an FP64 GPU solve of the same plate (FP64
     GMRES with the same restart to a residual 10 times below the form's)."""
@@ -418,10 +513,11 @@ def cpu_matvec_ms(apply, v):
     return float(np.median(times)) * 1e3
 
 
-def cpu_sample(w, iterations_gpu, sample_iterations=25):
-    """Times the oracle's setup (assembly, spectra, block-Jacobi, plane wave), its product and a bounded
-    number of its GMRES iterations; a full solve is setup + iterations_gpu x per-iteration time. Returns
-    (setup s, iteration s, product ms)."""
+def cpu_sample(w):
+    """Times the oracle's setup (assembly, spectra, block-Jacobi, plane wave) and one whole restart cycle of
+    its solver (GMRES: `restart` iterations, so the cost of the Gram-Schmidt passes, which grows with the
+    step within a cycle, is averaged over a full cycle; COCG: 50 iterations). Returns (setup s, s per
+    iteration, product ms)."""
     from oracle import assembly as A, blockjacobi as BJ, excitation as EX, geometry as G, solvers as OS, spectra as S
 
     n, h, k = w["n"], 1.0 / w["density"], 2 * math.pi
@@ -433,15 +529,16 @@ def cpu_sample(w, iterations_gpu, sample_iterations=25):
     d, p = plane_wave_vectors(w["theta"], w["phi"], w["pol"])
     b = EX.plane_wave(rt, k, d, p, 1.0)
     t_setup = time.perf_counter() - t0
-    apply = lambda v: S.split_apply(rt, sub, rt.content, v)
-    m = max(1, sample_iterations)
+    apply = lambda v: S.split_apply(rt, sub, rt.content, v)  # noqa: E731
     t0 = time.perf_counter()
     if w["method"] == "cg":
+        m = 50
         OS.cocg_iterate(apply, b, None, 1e-300, m, pc)
     else:
         # right preconditioning as the GPU solve: A M u = b
+        m = w["restart"]
         Ar = (lambda v: apply(pc(v))) if pc else apply
-        OS.gmres_iterate(Ar, b, None, 1e-300, m, w["restart"])
+        OS.gmres_iterate(Ar, b, None, 1e-300, m, m)
     t_iter = (time.perf_counter() - t0) / m
     return t_setup, t_iter, cpu_matvec_ms(apply, b)
 
@@ -470,37 +567,42 @@ FULL_SOLVE_MAX_FACES = 64
 
 
 def run_reference(args, w):
-    """--impl reference: the oracle's CPU path, all host threads; a whole solve for small plates, else a
-    bounded sample per step scaled to the solve's iteration count."""
+    """--impl reference: the oracle's CPU path (the reference's MATLAB restated) on all host threads. Small
+    plates run whole solves per step. Larger ones time, per step, the setup and one whole restart cycle,
+    and give solves/s for a solve of the oracle's own iteration count (ORACLE_ITERATIONS, from one whole
+    oracle solve of the workload); ms_per_step is the wall time of the step actually run."""
     cores = os.cpu_count() or 1
     full = w["n"] <= FULL_SOLVE_MAX_FACES
-    iters = REFERENCE_ITERATIONS.get(args.workload)
-    times = []
+    iters = ORACLE_ITERATIONS.get(args.workload)
+    solve_times, walls = [], []
     for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         if full:
-            t_step, iters, mv_ms = cpu_full_solve(w)
+            t_solve, iters, mv_ms = cpu_full_solve(w)
         else:
-            t_setup, t_iter, mv_ms = cpu_sample(w, iters, sample_iterations=10)
-            t_step = t_setup + iters * t_iter
+            t_setup, t_iter, mv_ms = cpu_sample(w)
+            t_solve = t_setup + iters * t_iter
         if step >= args.warmup:
-            times.append(t_step)
-    t = float(np.median(times))
+            solve_times.append(t_solve)
+            walls.append(time.perf_counter() - t0)
+    t = float(np.median(solve_times))
     value = 1.0 / t
     if full:
         sample = (f"numpy/scipy oracle (the reference's MATLAB path restated), per step one whole solve: assembly, "
                   f"spectra, plane wave and {iters} iterations to the tolerance (measured, not extrapolated)")
     else:
         sample = (f"numpy/scipy oracle (the reference's MATLAB path restated), per step: assembly + spectra + "
-                  f"preconditioner + plane wave timed, plus 10 GMRES/COCG iterations timed and scaled to the "
-                  f"{iters} iterations {REFERENCE_ITERATION_SOURCE.get(args.workload, 'of the same solve')} "
-                  f"(extrapolated)")
+                  f"preconditioner + plane wave timed, plus one whole restart cycle of the solver timed; solves/s "
+                  f"is for setup + {iters} iterations at that per-iteration time, {iters} being "
+                  f"{ORACLE_ITERATION_SOURCE[args.workload]} (extrapolated: a whole solve takes "
+                  f"{t:.0f} s)")
     line = {
         # n_gpus is the N of the launch this line is compared with; the arm itself runs on host cores only
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "device": "host CPU cores (no GPU used)",
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": config_of(args, w),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(walls)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": config_of(args, w), "seconds_per_solve": t, "extrapolated": not full,
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
                          "matvec_ms": mv_ms},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -508,15 +610,27 @@ def run_reference(args, w):
     print(json.dumps(line))
 
 
-# Iteration counts of the default solves (FP64 GPU, same algorithm as the oracle), used to scale the
-# CPU leg's bounded sample to a full solve (c1 runs whole solves instead).
-REFERENCE_ITERATIONS = {"c2": 2511, "c3": 9220}
-REFERENCE_ITERATION_SOURCE = {
-    "c2": "of the same solve on the GPU (FP64, same algorithm)",
-    # the reference has no precision form; its path for this plate is FP64 GMRES(30)
-    "c3": "of an FP64 GMRES(30) solve of this plate on the GPU, measured to 1e-9 (the count to the workload's "
-          "1e-8 is lower, so the extrapolated CPU time is an upper bound)",
+# Iteration counts of whole oracle solves of the workloads (the oracle's own; c1 runs whole solves per
+# step instead). c2: oracle/solvers.gmres_iterate with the block-Jacobi oracle on the right, to 1e-6, as
+# `python bench.py --impl reference --workload c2 --full-solve` runs it.
+ORACLE_ITERATIONS = {"c2": 2511, "c3": 9220}
+ORACLE_ITERATION_SOURCE = {
+    "c2": "the count of one whole oracle solve of this plate (block-Jacobi GMRES(50) to 1e-6)",
+    # the reference has no precision form; its path for this plate is FP64 GMRES(30), which the oracle
+    # cannot run to the end within hours on the host
+    "c3": "the count of an FP64 GMRES(30) solve of this plate on the GPU to 1e-9 (a whole oracle solve of "
+          "2.1 M unknowns takes hours; the count to the workload's 1e-8 is lower, so the CPU time is an upper "
+          "bound)",
 }
+
+
+def run_reference_full(args, w):
+    """One whole oracle solve of the workload, to the workload's tolerance: its iteration count is the
+    ORACLE_ITERATIONS entry of the workload."""
+    t, its, mv = cpu_full_solve(w)
+    print(json.dumps({"impl": "reference", "workload": args.workload, "seconds": t, "iterations": its,
+                      "matvec_ms": mv, "cores": os.cpu_count()}))
+
 
 METRIC = "solves/s at rel. residual 1e-6, mixed vs FP64 GPU; matvec HBM GB/s; p99 ms"
 
@@ -544,6 +658,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-arms", action="store_true", help="skip the mixed / batched arms of c2")
+    ap.add_argument("--full-solve", action="store_true",
+                    help="with --impl reference: one whole oracle solve of the workload (its iteration count)")
     ap.add_argument("--once", action="store_true",
                     help="one untimed solve of the workload, no JSON line (the command profiler captures run)")
     ap.add_argument("--matvec", action="store_true",
@@ -568,7 +685,7 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args, w)
+            run_reference_full(args, w) if args.full_solve else run_reference(args, w)
         return
 
     import torch
@@ -704,15 +821,23 @@ def main():
             t_cpu, cpu_its, mv_ms = cpu_full_solve(w)
             sample = f"one whole oracle solve: assembly, spectra, plane wave and {cpu_its} iterations (measured)"
         else:
-            t_setup, t_iter, mv_ms = cpu_sample(w, its[0], sample_iterations=20)
-            t_cpu = t_setup + its[0] * t_iter
-            sample = (f"oracle setup (assembly, spectra, preconditioner, plane wave) timed once, plus 20 iterations "
-                      f"timed and scaled to the GPU solve's {its[0]} iterations: {t_setup:.2f} s + "
-                      f"{its[0]} x {t_iter * 1e3:.1f} ms (extrapolated)")
+            iters = ORACLE_ITERATIONS[args.workload]
+            t_setup, t_iter, mv_ms = cpu_sample(w)
+            t_cpu = t_setup + iters * t_iter
+            sample = (f"oracle setup (assembly, spectra, preconditioner, plane wave) timed once, plus one whole "
+                      f"restart cycle timed, for a solve of {iters} iterations "
+                      f"({ORACLE_ITERATION_SOURCE[args.workload]}): {t_setup:.2f} s + {iters} x "
+                      f"{t_iter * 1e3:.1f} ms (extrapolated)")
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                                 "sample": sample, "matvec_ms": mv_ms}
     if rank == 0 and world == 1 and w["precision"] == "mixed":
         line["error_vs_fp64"] = precision_error(R, w)
+    if args.workload == "c2" and not args.no_arms:
+        # the metric's "mixed vs FP64": both precisions, single and batched, on the same plate
+        arms = precision_arms(R, w, min(args.steps, 5), min(args.warmup, 2))
+        line["arms"] = arms
+        line["mixed_over_fp64"] = arms["mixed_batched"]["value"] / arms["fp64"]["value"]
+        line["mixed_over_fp64_single_rhs"] = arms["mixed"]["value"] / arms["fp64"]["value"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -188,11 +188,14 @@ typedef struct rtm_solve_config {
     int restart;           /* GMRES cycle length (Solver.m:31, default 50); FGMRES inner cycle. At most 344
                               in FP64 and 638 in FP32 (RTM_ERR_UNSUPPORTED above): longer bases do not fit
                               the orthogonalisation's shared-memory tile */
-    double inner_tolerance;/* FGMRES_IR: relative residual of one FP32 inner solve */
+    double inner_tolerance;/* FGMRES_IR: the tightest relative residual one FP32 inner solve aims at. Each inner
+                              solve stops as soon as its right-hand side's outer tolerance is met in this
+                              refinement step (at 0.5 tolerance ||b|| / ||r||), but not below this floor */
     int max_refinements;   /* FGMRES_IR: bound on the FP64 outer refinement steps */
     int check_every;       /* iterations between host convergence checks (0: library default) */
     int right_preconditioned; /* GMRES: 0 left preconditioning (GeneralizedMinimumResidual.m:2-5), 1 right
-                                 (flexible GMRES: the monitored residual is that of op * x = b) */
+                                 (x = x0 + M V y at the end of each cycle: the monitored residual is that
+                                 of op * x = b) */
 } rtm_solve_config;
 
 typedef struct rtm_solve_stats {
@@ -277,8 +280,7 @@ typedef struct rtm_request {
     int port_direction;         /* delta gap: middle port across x (0) or y (1) rooftops */
     double voltage;             /* delta gap: gap voltage */
     int method;                 /* RTM_METHOD_CG or RTM_METHOD_GMRES (right-preconditioned) */
-    int preconditioner;         /* 0 none, 1 block-Jacobi over 2 x 2 faces, 2 rChan circulant (partwise); the
-                                   circulant needs face counts whose prime factors are at most 61 */
+    int preconditioner;         /* 0 none, 1 block-Jacobi over 2 x 2 faces, 2 rChan circulant (partwise) */
     double tolerance;
     int max_iterations;
     int restart;

@@ -93,7 +93,8 @@ def gmres_iterate(apply, b, x0, tol, maxit, restart, precond=None):
     norms = [rn / ref]
     converged = norms[0] < tol
     it = 0
-    V = np.zeros((n, m + 1), dtype=np.complex128)
+    # column-major as MATLAB's V, so that V(:, 1:step) is one contiguous block for BLAS
+    V = np.zeros((n, m + 1), dtype=np.complex128, order="F")
     H = np.zeros((m + 1, m), dtype=np.complex128)
     cs = np.zeros(m, dtype=np.complex128)
     sn = np.zeros(m, dtype=np.complex128)
@@ -107,10 +108,12 @@ def gmres_iterate(apply, b, x0, tol, maxit, restart, precond=None):
             it += 1
             w = P(apply(V[:, step - 1]))
             # orthogonalize_.m:15-23: classical Gram-Schmidt twice against the first `step` columns
-            h = V[:, :step].conj().T @ w
-            w = w - V[:, :step] @ h
-            c = V[:, :step].conj().T @ w
-            w = w - V[:, :step] @ c
+            # V' * w as conj(V.' * conj(w)): the same products without a conjugated copy of the basis
+            Vs = V[:, :step]
+            h = (Vs.T @ w.conj()).conj()
+            w = w - Vs @ h
+            c = (Vs.T @ w.conj()).conj()
+            w = w - Vs @ c
             h = h + c
             H[:step, step - 1] = h
             H[step, step - 1] = np.linalg.norm(w)

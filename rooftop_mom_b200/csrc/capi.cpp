@@ -365,7 +365,7 @@ int rtm_operator_apply(rtm_operator* op, const void* x, void* y, int64_t n, int 
     RTM_TRY(out_prepare(y, n * nrhs, prec, where, o, s));
     RTM_TRY(op->op->apply(in.ptr, o.ptr, nrhs, s, SkipFlags{}));
     RTM_TRY(out_finish(y, n * nrhs, prec, where, o, s));
-    if (where == RTM_DEVICE && !stream) RTM_CUDA(cudaStreamSynchronize(s));
+    if (where == RTM_HOST || !stream) RTM_TRY(device_fault_check(s));
     return RTM_OK;
 }
 
@@ -377,7 +377,7 @@ int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void* x, void
     RTM_TRY(check_rhs(nrhs));
     cudaStream_t s = pick(stream, op->stream);
     RTM_TRY(apply_fixed_scratch(*op->grid, x, y, nrhs, s));
-    if (!stream) RTM_CUDA(cudaStreamSynchronize(s));
+    if (!stream) RTM_TRY(device_fault_check(s));
     return RTM_OK;
 }
 
@@ -471,7 +471,7 @@ int rtm_preconditioner_apply(rtm_preconditioner* pc, const void* x, void* y, int
     RTM_TRY(out_prepare(y, n * nrhs, prec, where, o, s));
     RTM_TRY(pc->op->apply(in.ptr, o.ptr, nrhs, s, SkipFlags{}));
     RTM_TRY(out_finish(y, n * nrhs, prec, where, o, s));
-    if (where == RTM_DEVICE && !stream) RTM_CUDA(cudaStreamSynchronize(s));
+    if (where == RTM_HOST || !stream) RTM_TRY(device_fault_check(s));
     return RTM_OK;
 }
 

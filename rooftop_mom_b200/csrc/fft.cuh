@@ -161,13 +161,17 @@ __host__ __device__ constexpr int fft_ipt(int r) {
     return r == 2 ? 8 : r == 3 ? 6 : r == 4 ? 4 : r == 5 ? 4 : r == 7 ? 3 : r == 8 ? 2 : 1;
 }
 
+// Elements a line buffer of plan p spans in shared memory (positions sk(e), e < p.m; p.m == p.n except
+// for Bluestein plans, whose lines hold the convolution of length p.m).
+__host__ __device__ inline int fft_span(const FftPlan& p) { return sk(p.m - 1) + 1; }
+
 // Threads a CTA needs to transform `lines` lines of plan p in place (a multiple of 32).
 __host__ __device__ inline int fft_threads(int lines, const FftPlan& p) {
     int t = 32;
     for (int s = 0; s < p.nstages; ++s) {
         const int r = p.radix[s];
         const int per = fft_ipt(r);
-        const int need = (lines * (p.n / r) + per - 1) / per;
+        const int need = (lines * (p.m / r) + per - 1) / per;
         t = need > t ? need : t;
     }
     return (t + 31) / 32 * 32;
@@ -260,40 +264,96 @@ __device__ __noinline__ void pass_ip_generic(T2* buf, int n, int R, int Ns, int 
     __syncthreads();
 }
 
-// Transforms, in place, the `lines` lines of length p.n in buf (element e of line l at
-// buf[l * ls + sk(e) * es]); tw (global or shared) holds the p.n roots. Needs blockDim.x >=
-// fft_threads(lines, p); call it after a __syncthreads() that makes buf visible; it returns after
-// one. POW2 instantiates radices 16, 8, 4 and 2 inline (lengths that are powers of two); otherwise
-// every radix runs as a separate function.
+// The Stockham stages of plan p over transforms of length n (p.n, or p.m inside a Bluestein plan).
 template <bool INV, bool POW2, typename T2>
-__device__ __forceinline__ void fft_inplace(T2* buf, int lines, int ls, int es, const FftPlan& p, const T2* tw) {
+__device__ __forceinline__ void fft_stages(T2* buf, int lines, int ls, int es, const FftPlan& p, int n, const T2* tw) {
     int Ns = 1;
     for (int s = 0; s < p.nstages; ++s) {
         const int r = p.radix[s];
         if constexpr (POW2) {
             switch (r) {
-                case 2: pass_ip_body<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 4: pass_ip_body<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 8: pass_ip_body<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                default: pass_ip_body<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
+                case 2: pass_ip_body<2, 8, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 4: pass_ip_body<4, 4, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 8: pass_ip_body<8, 2, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                default: pass_ip_body<16, 1, INV>(buf, n, Ns, lines, ls, es, tw); break;
             }
         } else {
             switch (r) {
-                case 2: pass_ip<2, 8, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 3: pass_ip<3, 6, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 4: pass_ip<4, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 5: pass_ip<5, 4, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 7: pass_ip<7, 3, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 8: pass_ip<8, 2, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                case 16: pass_ip<16, 1, INV>(buf, p.n, Ns, lines, ls, es, tw); break;
-                default: pass_ip_generic<INV>(buf, p.n, r, Ns, lines, ls, es, tw); break;
+                case 2: pass_ip<2, 8, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 3: pass_ip<3, 6, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 4: pass_ip<4, 4, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 5: pass_ip<5, 4, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 7: pass_ip<7, 3, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 8: pass_ip<8, 2, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                case 16: pass_ip<16, 1, INV>(buf, n, Ns, lines, ls, es, tw); break;
+                default: pass_ip_generic<INV>(buf, n, r, Ns, lines, ls, es, tw); break;
             }
         }
         Ns *= r;
     }
 }
 
-// True when every radix of the plan is a power of two (the POW2 instantiation applies).
+template <typename T2> struct BluesteinTables;
+template <> struct BluesteinTables<double2> {
+    __device__ static const double2* chirp(const FftPlan& p) { return p.chirp64; }
+    __device__ static const double2* kern(const FftPlan& p) { return p.kern64; }
+    __device__ static const double2* roots(const FftPlan& p) { return p.twm64; }
+};
+template <> struct BluesteinTables<float2> {
+    __device__ static const float2* chirp(const FftPlan& p) { return p.chirp32; }
+    __device__ static const float2* kern(const FftPlan& p) { return p.kern32; }
+    __device__ static const float2* roots(const FftPlan& p) { return p.twm32; }
+};
+
+// Bluestein (chirp-z) transform of length p.n on line buffers of p.m elements: with c_j = exp(-i pi j^2 / n),
+// X_k = c_k sum_j (x_j c_j) conj(c_(k-j)), the linear convolution taken as a circular one of the
+// power-of-two length m >= 2n - 1 (kern = DFT_m of the wrapped conj(c_d), divided by m). The inverse uses
+// the conjugate chirp and the conjugate kernel spectrum (the wrapped chirp is even). Entries e >= n of
+// the buffers are overwritten.
+template <bool INV, typename T2>
+__device__ __noinline__ void fft_bluestein(T2* buf, int lines, int ls, int es, const FftPlan& p) {
+    const T2* chirp = BluesteinTables<T2>::chirp(p);
+    const T2* kern = BluesteinTables<T2>::kern(p);
+    const T2* roots = BluesteinTables<T2>::roots(p);
+    const int n = p.n, m = p.m;
+    for (int it = threadIdx.x; it < lines * m; it += blockDim.x) {
+        const int line = it % lines, e = it / lines;
+        T2& v = buf[line * ls + sk(e) * es];
+        v = e < n ? (INV ? cmulc(v, __ldg(&chirp[e])) : cmul(v, __ldg(&chirp[e]))) : czero<T2>();
+    }
+    __syncthreads();
+    fft_stages<false, true>(buf, lines, ls, es, p, m, roots);
+    for (int it = threadIdx.x; it < lines * m; it += blockDim.x) {
+        const int line = it % lines, e = it / lines;
+        T2& v = buf[line * ls + sk(e) * es];
+        v = INV ? cmulc(v, __ldg(&kern[e])) : cmul(v, __ldg(&kern[e]));
+    }
+    __syncthreads();
+    fft_stages<true, true>(buf, lines, ls, es, p, m, roots);
+    for (int it = threadIdx.x; it < lines * n; it += blockDim.x) {
+        const int line = it % lines, e = it / lines;
+        T2& v = buf[line * ls + sk(e) * es];
+        v = INV ? cmulc(v, __ldg(&chirp[e])) : cmul(v, __ldg(&chirp[e]));
+    }
+    __syncthreads();
+}
+
+// Transforms, in place, the `lines` lines of length p.n in buf (element e of line l at
+// buf[l * ls + sk(e) * es]; a line spans fft_span(p) elements); tw (global or shared) holds the p.n
+// roots. Needs blockDim.x >= fft_threads(lines, p); call it after a __syncthreads() that makes buf
+// visible; it returns after one. POW2 instantiates radices 16, 8, 4 and 2 inline (lengths that are
+// powers of two, and Bluestein plans); otherwise every radix runs as a separate function.
+template <bool INV, bool POW2, typename T2>
+__device__ __forceinline__ void fft_inplace(T2* buf, int lines, int ls, int es, const FftPlan& p, const T2* tw) {
+    if (p.m != p.n) {
+        fft_bluestein<INV>(buf, lines, ls, es, p);
+        return;
+    }
+    fft_stages<INV, POW2>(buf, lines, ls, es, p, p.n, tw);
+}
+
+// True when every radix of the plan is a power of two (the POW2 instantiation applies; Bluestein plans
+// run power-of-two transforms of length p.m).
 __host__ __device__ inline bool fft_pow2(const FftPlan& p) {
     for (int s = 0; s < p.nstages; ++s)
         if (p.radix[s] != 2 && p.radix[s] != 4 && p.radix[s] != 8 && p.radix[s] != 16) return false;

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_grid_y_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* tws = A + (size_t)L * (sk(Q - 1) + 1);
+    T2* tws = A + (size_t)L * fft_span(a.planQ);
     const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kMaxThreads, sizeof(T) == 8 ? 1 : 2) k_grid_y_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int TI = a.ti, Q = a.Q, L = a.npy * TI;
     T2* A = reinterpret_cast<T2*>(smem_raw);
-    T2* tws = A + (size_t)L * (sk(Q - 1) + 1);
+    T2* tws = A + (size_t)L * fft_span(a.planQ);
     const int c = blockIdx.y, rhs = blockIdx.z;
     const int rows = a.rows[c], cols = a.cols[c];
     const int i0 = blockIdx.x * TI;
@@ -360,7 +360,7 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     const size_t elem = sizeof(T2);
     if (g.mode == kStrip) {
         a.scale = (T)(1.0 / g.P);
-        a.ls = line_stride(g.P, g.nsx, elem);
+        a.ls = line_stride(g.tP->plan.m, g.nsx, elem);
         const size_t smem = ((size_t)g.nsx * a.ls + g.P) * elem;
         const int thr = fft_threads(g.nsx, g.tP->plan);
         if (smem > (size_t)kSmemBudget || thr > kMaxThreads)
@@ -372,6 +372,7 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
         return RTM_OK;
     }
     a.scale = (T)(1.0 / ((double)g.P * g.Q));
+    RTM_TRY(device_fault_word(&a.fault));
     a.work = static_cast<T2*>(work);
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
     if (g.mode == kGen3 && g.nsx == 2 && g.nsy == 2 && !g.lean && fast_split_eligible(g.P, g.Q, sizeof(T) == 8)) {
@@ -385,16 +386,16 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     // y passes: TI x columns per CTA (rows of 64 bytes) for every y subband at once; fewer columns
     // while the tile (plus the roots) would not fit or would need more than kMaxThreads threads.
     int ti = sizeof(T) == 8 ? 4 : 8;
-    auto y_smem = [&](int t) { return ((size_t)npy * t * (sk(g.Q - 1) + 1) + g.Q) * elem; };
+    auto y_smem = [&](int t) { return ((size_t)npy * t * fft_span(g.tQ->plan) + g.Q) * elem; };
     while (ti > 1 && (y_smem(ti) > (size_t)kSmemBudget || fft_threads(npy * ti, g.tQ->plan) > kMaxThreads)) ti /= 2;
     const int thr_y = fft_threads(npy * ti, g.tQ->plan);
     // x-mix: CB y frequencies per CTA, every x subband and component at once (CB nsx 2 lines).
-    auto x_smem = [&](int c) { return ((size_t)c * g.nsx * 2 * line_stride(g.P, c * g.nsx * 2, elem) + g.P) * elem; };
+    auto x_smem = [&](int c) { return ((size_t)c * g.nsx * 2 * line_stride(g.tP->plan.m, c * g.nsx * 2, elem) + g.P) * elem; };
     int cb = 8;
     while (cb > 1 && (x_smem(cb) > (size_t)kSmemBudget || fft_threads(cb * g.nsx * 2, g.tP->plan) > kMaxThreads))
         cb /= 2;
     while (cb > 1 && (int64_t)((g.Q + cb - 1) / cb) * npy * nrhs < 148) cb /= 2;
-    const int ls = line_stride(g.P, cb * g.nsx * 2, elem);
+    const int ls = line_stride(g.tP->plan.m, cb * g.nsx * 2, elem);
     const int thr_x = fft_threads(cb * g.nsx * 2, g.tP->plan);
     if (y_smem(ti) > (size_t)kSmemBudget || x_smem(cb) > (size_t)kSmemBudget || thr_y > kMaxThreads ||
         thr_x > kMaxThreads)
@@ -423,8 +424,10 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
 }
 
 int GridApplicator::reserve(int nrhs) {
-    // kernel attributes are set here, outside of any stream capture
+    // kernel attributes and the fault word are set up here, outside of any stream capture
     RTM_TRY(precision == RTM_FP64 ? set_smem_attrs<double>() : set_smem_attrs<float>());
+    int* fault = nullptr;
+    RTM_TRY(device_fault_word(&fault));
     if (nrhs <= max_rhs && (mode == kStrip || work.bytes >= work_bytes_per_rhs() * (size_t)nrhs)) return RTM_OK;
     if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
     max_rhs = std::max(max_rhs, nrhs);
@@ -613,12 +616,12 @@ static int run_gen(GenArgs& a, cudaStream_t s) {
     }));
     if (a.nitems == 0) return RTM_OK;
     a.ti = 4;
-    while (a.ti > 1 && ((size_t)a.ti * (sk(a.Q - 1) + 1) * sizeof(double2) > (size_t)kSmemBudget ||
+    while (a.ti > 1 && ((size_t)a.ti * fft_span(a.planQ) * sizeof(double2) > (size_t)kSmemBudget ||
                         fft_threads(a.ti, a.planQ) > kMaxThreads))
         a.ti /= 2;
     const int thr_y = fft_threads(a.ti, a.planQ), thr_x = fft_threads(1, a.planP);
-    const size_t smem_y = (size_t)a.ti * (sk(a.Q - 1) + 1) * sizeof(double2);
-    const size_t smem_x = (size_t)(sk(a.P - 1) + 1) * sizeof(double2);
+    const size_t smem_y = (size_t)a.ti * fft_span(a.planQ) * sizeof(double2);
+    const size_t smem_x = (size_t)fft_span(a.planP) * sizeof(double2);
     if (smem_y > (size_t)kSmemBudget || smem_x > (size_t)kSmemBudget || thr_y > kMaxThreads || thr_x > kMaxThreads)
         return fail(RTM_ERR_UNSUPPORTED, "spectra grid too large for this build");
     dim3 gy((a.P + a.ti - 1) / a.ti, a.nitems);
@@ -1057,16 +1060,16 @@ static int line_conv(const TwoSidedSpectra& t, int dim, const double2* K, double
         return RTM_OK;
     }));
     if (dim == 0) {
-        const size_t smem = (size_t)(sk(t.P - 1) + 1) * sizeof(double2);
+        const size_t smem = (size_t)fft_span(t.tP->plan) * sizeof(double2);
         const int thr = fft_threads(1, t.tP->plan);
         if (smem > (size_t)kSmemBudget || thr > kMaxThreads) return fail(RTM_ERR_UNSUPPORTED, "grid too large");
         k_line_conv_x<<<t.Q, thr, smem, s>>>(t.P, t.Q, t.tP->plan, t.tP->tw64, K, v);
     } else {
         int ti = 4;
-        while (ti > 1 && ((size_t)ti * (sk(t.Q - 1) + 1) * sizeof(double2) > (size_t)kSmemBudget ||
+        while (ti > 1 && ((size_t)ti * fft_span(t.tQ->plan) * sizeof(double2) > (size_t)kSmemBudget ||
                           fft_threads(ti, t.tQ->plan) > kMaxThreads))
             ti /= 2;
-        const size_t smem = (size_t)ti * (sk(t.Q - 1) + 1) * sizeof(double2);
+        const size_t smem = (size_t)ti * fft_span(t.tQ->plan) * sizeof(double2);
         const int thr = fft_threads(ti, t.tQ->plan);
         if (smem > (size_t)kSmemBudget || thr > kMaxThreads) return fail(RTM_ERR_UNSUPPORTED, "grid too large");
         k_line_conv_y<<<(t.P + ti - 1) / ti, thr, smem, s>>>(t.P, t.Q, ti, t.tQ->plan, t.tQ->tw64, K, v);

@@ -33,6 +33,7 @@ template <typename T> struct GridArgs {
     const int* skip;  // per right-hand side, nonzero: leave it alone
     int skip_stride;
     int cb, ls;  // x-mix: y frequencies per CTA and the padded line stride
+    int* fault;  // the device's fault word: set to RTM_ERR_TIMEOUT by a bounded wait that ran out
 };
 
 template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rhs) {

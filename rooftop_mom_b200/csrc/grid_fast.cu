@@ -12,8 +12,11 @@
 // The inverse runs the same steps backwards from that layout. The x-mix multiplies the spectra in this
 // layout without reordering; every global load and store is coalesced (consecutive threads touch
 // consecutive elements). The line buffers are padded (row stride R2 + 1) against bank conflicts.
+#include <algorithm>
+
 #include "grid.h"
 #include "grid_args.cuh"
+#include "bulk.cuh"
 #include "pdl.cuh"
 
 namespace rtm {
@@ -174,92 +177,163 @@ __global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) 
         for (int k2 = 0; k2 < R2; ++k2) dst[(int64_t)((t + R2 * s) + R1 * k2) * a.P] = v[s * R2 + k2];
 }
 
-// x-mix: teams of four groups (component c, x subband px) per y frequency j of subband py. Thread
-// index t + R2 (team * 4 + 2 px + c). Forward transform along x of W mod_x^px, the 2x2 block mix
-// with the subband spectra (the two components of a group pair meet through shared memory), inverse
-// transform, demodulation, the sum over px, scaled by 1 / (PQ), in place in W.
-template <typename T, int NP>
-__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NP>::value)) k_fast_x_mix(const GridArgs<T> a) {
+// x-mix: persistent CTAs. A CTA takes the iterations it = blockIdx.x, blockIdx.x + gridDim.x, ...; an
+// iteration is TEAMS consecutive y frequencies j of one (right-hand side, y subband py). Its inputs are
+// copied into shared memory one iteration ahead by bulk asynchronous copies (one thread issues them): the
+// W rows of both components (contiguous for consecutive j) as soon as the current ones are in registers,
+// and the subband spectra rows (E, MXX, MYY of both x subbands) as soon as the current mix has read them,
+// so the global-memory latency of both overlaps the transforms. Per y frequency, a team of four groups
+// (component c, x subband px), thread index t + R2 (team * 4 + 2 px + c): forward transform along x of
+// W mod_x^px, the 2x2 block mix with the subband spectra (the two components of a group pair meet through
+// shared memory), inverse transform, demodulation, the sum over px, scaled by 1 / (PQ), in place in W.
+// A bulk-copy wait that runs out records RTM_ERR_TIMEOUT in the fault word and ends the CTA.
+template <typename T, int NP> struct MixShape {
+    static constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2;
+    static constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
     using T2 = typename Cx<T>::T2;
-    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, S = R1 / R2;
-    constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // line buffers [4 TEAMS][LB], W rows [2 c][TEAMS][NP], spectra rows [2 px][3 kind][TEAMS][NP]
+    static constexpr size_t lines = (size_t)4 * TEAMS * LB * sizeof(T2);
+    static constexpr size_t wrows = (size_t)2 * TEAMS * NP * sizeof(T2);
+    static constexpr size_t srows = (size_t)6 * TEAMS * NP * sizeof(T2);
+    static constexpr size_t smem = lines + wrows + srows;
+    static constexpr int blocks = 2 * smem <= 220 * 1024 ? 2 : 1;  // CTAs per SM the registers are sized for
+};
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k_fast_x_mix(const GridArgs<T> a, int iters) {
+    using M = MixShape<T, NP>;
+    using T2 = typename Cx<T>::T2;
+    constexpr int R1 = M::R1, R2 = M::R2, S = R1 / R2, TEAMS = M::TEAMS, LB = M::LB;
+    constexpr unsigned BLOCK = TEAMS * NP * sizeof(T2);  // TEAMS consecutive rows of one grid
+    static_assert(BLOCK % 16 == 0 && M::lines % 16 == 0 && M::wrows % 16 == 0, "bulk copies need 16-byte units");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     T2* sm = reinterpret_cast<T2*>(smem_raw);
+    T2* wst = reinterpret_cast<T2*>(smem_raw + M::lines);
+    T2* sst = reinterpret_cast<T2*>(smem_raw + M::lines + M::wrows);
+    __shared__ __align__(8) uint64_t bar[2];  // 0: W rows, 1: spectra rows
     griddep_wait();
     griddep_launch_dependents();
-    const int py = blockIdx.y, rhs = blockIdx.z;
-    if (skipped(a, rhs)) return;
-    const int t = threadIdx.x % R2, gid = threadIdx.x / R2;
-    const int team = gid / 4, c = gid % 2, px = (gid / 2) % 2;
-    const int j = blockIdx.x * TEAMS + team;
-    const bool on = j < a.Q;
-    const int Q = a.Q;
+    const int Q = a.Q, per_py = Q / TEAMS, per_rhs = 2 * per_py;
     const int64_t QP = (int64_t)Q * NP;
+    const int tid = threadIdx.x;
+    const int t = tid % R2, gid = tid / R2;
+    const int team = gid / 4, c = gid % 2, px = (gid / 2) % 2;
+    auto live = [&](int it) {
+        while (it < iters && skipped(a, it / per_rhs)) it += gridDim.x;
+        return it;
+    };
+    // copies issued (thread 0) and barrier phases completed (every thread), per barrier
+    unsigned issued[2] = {0, 0}, done[2] = {0, 0};
+    auto issue = [&](int it, bool w, bool spectra) {
+        const int rhs = it / per_rhs, r = it % per_rhs, py = r / per_py, j0 = (r % per_py) * TEAMS;
+        if (w) {
+            ++issued[0];
+            mbar_expect_tx(&bar[0], 2 * BLOCK);
+            for (int cc = 0; cc < 2; ++cc)
+                bulk_load(wst + cc * TEAMS * NP,
+                          a.work + rhs * a.work_rhs + (int64_t)(py * a.ncomp + cc) * QP + (int64_t)j0 * NP, BLOCK,
+                          &bar[0]);
+        }
+        if (spectra) {
+            ++issued[1];
+            mbar_expect_tx(&bar[1], 6 * BLOCK);
+            for (int q = 0; q < 2; ++q)
+                for (int kind = 0; kind < 3; ++kind)
+                    bulk_load(sst + (q * 3 + kind) * TEAMS * NP,
+                              a.spec + (int64_t)((q + 2 * py) * 3 + kind) * QP + (int64_t)j0 * NP, BLOCK, &bar[1]);
+        }
+    };
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int it = live(blockIdx.x);
+    if (tid == 0 && it < iters) issue(it, true, true);
     const LineBuf<T2> buf{sm + gid * LB, R2 + 1, 1};
     T2* own = sm + gid * LB;
     const T2* partner = sm + (gid ^ 1) * LB;
-    const int rows = a.rows[c];
-    T2* row = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * QP + (int64_t)(on ? j : 0) * NP;
-    T2 v[R1];
-#pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) {
-        const int i = R2 * m1 + t;
-        T2 e = (on && i < rows) ? row[i] : czero<T2>();
-        if (px) e = cmul(e, __ldg(&a.modP[i]));
-        v[m1] = e;
-    }
-    fwd_first<NP>(v, t, a.twP, buf);
-    __syncthreads();
-    fwd_second<NP>(v, t, a.twP, buf);
-    __syncthreads();  // the buffers are read; they now carry the spectra values to the partner
-#pragma unroll
-    for (int r = 0; r < R1; ++r) own[r * R2 + t] = v[r];
-    __syncthreads();
-    if (on) {
-        const int sub = px + 2 * py;
-        const T2* spec = a.spec + (int64_t)(sub * 3) * QP + (int64_t)j * NP;
-        const T2* ux = px ? a.ux1 : a.ux0;
-        const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
-        const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-#pragma unroll
-            for (int k2 = 0; k2 < R2; ++k2) {
-                const int k = (t + R2 * s) + R1 * k2;
-                const T2 E = __ldg(&spec[k]);
-                const T2 M = __ldg(&spec[(1 + c) * QP + k]);
-                const T2 uu = __ldg(&ux[k]);
-                const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
-                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
-                T2 qc = cmulc(uu, vv);
-                qc.x = -qc.x * a.inv_ab;
-                qc.y = -qc.y * a.inv_ab;
-                const T2 coupling = c ? cconj(qc) : qc;
-                const T cself = c ? cv : cu;
-                const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
-                T2 o = cmul(M, me);
-                o = csub(o, cscale(cmul(E, me), cself));
-                o = cadd(o, cmul(coupling, cmul(E, other)));
-                v[s * R2 + k2] = o;
-            }
-    }
-    __syncthreads();  // the partner values are read
-    inv_first<NP>(v, t, a.twP, buf);
-    __syncthreads();
-    inv_second<NP>(v, t, a.twP, buf);
-    __syncthreads();
-    if (px) {
-#pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) own[m1 * R2 + t] = cmulc(v[m1], __ldg(&a.modP[R2 * m1 + t]));
-    }
-    __syncthreads();
-    if (px || !on) return;
     const T2* odd = sm + (gid + 2) * LB;
+    const int rows = a.rows[c];
+    const T2* ux = px ? a.ux1 : a.ux0;
+    while (it < iters) {
+        const int nxt = live(it + gridDim.x);
+        const int rhs = it / per_rhs, r = it % per_rhs, py = r / per_py, j = (r % per_py) * TEAMS + team;
+        if (__syncthreads_or(!mbar_wait(&bar[0], done[0] & 1, a.fault))) break;
+        ++done[0];
+        T2 v[R1];
+        const T2* wrow = wst + (c * TEAMS + team) * NP;
 #pragma unroll
-    for (int m1 = 0; m1 < R1; ++m1) {
-        const int i = R2 * m1 + t;
-        if (i < rows) row[i] = cscale(cadd(v[m1], odd[m1 * R2 + t]), a.scale);
+        for (int m1 = 0; m1 < R1; ++m1) {
+            const int i = R2 * m1 + t;
+            T2 e = i < rows ? wrow[i] : czero<T2>();
+            if (px) e = cmul(e, __ldg(&a.modP[i]));
+            v[m1] = e;
+        }
+        __syncthreads();  // the W rows are in registers: the next iteration's may come in
+        if (tid == 0 && nxt < iters) issue(nxt, true, false);
+        fwd_first<NP>(v, t, a.twP, buf);
+        __syncthreads();
+        fwd_second<NP>(v, t, a.twP, buf);
+        __syncthreads();  // the buffers are read; they now carry the spectra values to the partner
+#pragma unroll
+        for (int q = 0; q < R1; ++q) own[q * R2 + t] = v[q];
+        if (__syncthreads_or(!mbar_wait(&bar[1], done[1] & 1, a.fault))) break;
+        ++done[1];
+        {
+            const T2* Es = sst + (px * 3 * TEAMS + team) * NP;
+            const T2* Ms = sst + ((px * 3 + 1 + c) * TEAMS + team) * NP;
+            const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
+            const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+#pragma unroll
+                for (int k2 = 0; k2 < R2; ++k2) {
+                    const int k = (t + R2 * s) + R1 * k2;
+                    const T2 E = Es[k];
+                    const T2 Mk = Ms[k];
+                    const T2 uu = __ldg(&ux[k]);
+                    const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                    // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
+                    T2 qc = cmulc(uu, vv);
+                    qc.x = -qc.x * a.inv_ab;
+                    qc.y = -qc.y * a.inv_ab;
+                    const T2 coupling = c ? cconj(qc) : qc;
+                    const T cself = c ? cv : cu;
+                    const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
+                    T2 o = cmul(Mk, me);
+                    o = csub(o, cscale(cmul(E, me), cself));
+                    o = cadd(o, cmul(coupling, cmul(E, other)));
+                    v[s * R2 + k2] = o;
+                }
+        }
+        __syncthreads();  // the spectra and the partner values are read
+        if (tid == 0 && nxt < iters) issue(nxt, false, true);
+        inv_first<NP>(v, t, a.twP, buf);
+        __syncthreads();
+        inv_second<NP>(v, t, a.twP, buf);
+        __syncthreads();
+        if (px) {
+#pragma unroll
+            for (int m1 = 0; m1 < R1; ++m1) own[m1 * R2 + t] = cmulc(v[m1], __ldg(&a.modP[R2 * m1 + t]));
+        }
+        __syncthreads();
+        if (!px) {
+            T2* row = a.work + rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * QP + (int64_t)j * NP;
+#pragma unroll
+            for (int m1 = 0; m1 < R1; ++m1) {
+                const int i = R2 * m1 + t;
+                if (i < rows) row[i] = cscale(cadd(v[m1], odd[m1 * R2 + t]), a.scale);
+            }
+        }
+        it = nxt;
     }
+    // A wait ran out: let the copies still in flight into this CTA's shared memory land (each wait
+    // bounded) before the CTA ends.
+    if (tid == 0)
+        for (int q = 0; q < 2; ++q)
+            for (; done[q] < issued[q]; ++done[q]) mbar_wait(&bar[q], done[q] & 1, nullptr);
 }
 
 // y-inverse: TI columns of one component, a group per (column, y subband); inverse transform along y,
@@ -310,11 +384,6 @@ template <typename T, int NQ> size_t y_smem() {
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2);
     return (size_t)2 * TI * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
 }
-template <typename T, int NP> size_t x_smem() {
-    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, TEAMS = Fast<T>::threads / (4 * R2);
-    return (size_t)4 * TEAMS * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
-}
-
 template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd,
                                            cudaStream_t s) {
     using T2 = typename Cx<T>::T2;
@@ -337,15 +406,23 @@ template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const
 }
 
 template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
-    constexpr int TEAMS = Fast<T>::threads / (4 * Shape<NP>::R2);
-    const size_t smem = x_smem<T, NP>();
+    using M = MixShape<T, NP>;
     static DeviceOnce once;
-    RTM_TRY(once([smem]() -> int {
-        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static int per_sm[64] = {};
+    int dev = 0;
+    RTM_CUDA(cudaGetDevice(&dev));
+    RTM_TRY(once([dev]() -> int {
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem));
+        int blocks = 0, sms = 0;
+        RTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fast_x_mix<T, NP>, Fast<T>::threads, M::smem));
+        RTM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (dev >= 0 && dev < 64) per_sm[dev] = std::max(1, blocks) * sms;
         return RTM_OK;
     }));
-    const dim3 grid((a.Q + TEAMS - 1) / TEAMS, 2, nrhs);
-    RTM_CUDA(launch_dependent(k_fast_x_mix<T, NP>, grid, dim3(Fast<T>::threads), smem, s, a));
+    const int iters = nrhs * 2 * (a.Q / M::TEAMS);
+    const int resident = dev >= 0 && dev < 64 && per_sm[dev] > 0 ? per_sm[dev] : 148;
+    const int grid = std::max(1, std::min(iters, resident));
+    RTM_CUDA(launch_dependent(k_fast_x_mix<T, NP>, dim3(grid), dim3(Fast<T>::threads), M::smem, s, a, iters));
     count_launch();
     return RTM_OK;
 }

@@ -99,10 +99,21 @@ struct StreamSyncGuard {
 constexpr int kMaxStages = 20;
 constexpr int kMaxGenericRadix = 64;  // largest prime factor this build transforms
 
+// A length whose factorisation needs a prime above kMaxGenericRadix runs as a Bluestein (chirp-z)
+// convolution: m is then the power of two >= 2n - 1 that a line buffer must hold, the radices are those
+// of m, and the plan points to the chirp, the convolution kernel's spectrum and the roots of length m.
+// Otherwise m == n and the pointers are null.
 struct FftPlan {
     int n;
     int nstages;
     int radix[kMaxStages];
+    int m;
+    const double2* chirp64;  // exp(-i pi (j^2 mod 2n) / n), j < n
+    const float2* chirp32;
+    const double2* kern64;   // DFT_m of exp(+i pi d^2 / n) wrapped to length m, divided by m
+    const float2* kern32;
+    const double2* twm64;    // exp(-2 pi i k / m), k < m
+    const float2* twm32;
 };
 
 struct FftTables {
@@ -113,8 +124,8 @@ struct FftTables {
     const float2* mod32;
 };
 
-// Returns the cached tables of length n on the current device (RTM_ERR_UNSUPPORTED if n has a
-// prime factor above kMaxGenericRadix).
+// Returns the cached tables of length n on the current device (a Bluestein plan when n has a prime
+// factor above kMaxGenericRadix).
 int fft_tables(int n, const FftTables** out);
 
 // Shift-phase factors of generateShiftPhases.m: u(m) = 1 - exp(i pi (2m + parity) / n).
@@ -130,5 +141,12 @@ void power_moments(double size_x, double size_y, int power, double out[7][4]);
 void extracted_moments(double size_x, double size_y, double k, double out[7][4]);
 
 int fast_fft_size(int count);
+
+// The device's fault word, which kernels with bounded waits set to RTM_ERR_TIMEOUT when a wait runs
+// out (a device variable: looking it up allocates nothing; the first lookup on a device loads its
+// module, so it is made outside any stream capture), and its check: reads and clears the word after
+// synchronising the stream, returning RTM_ERR_TIMEOUT if it was set.
+int device_fault_word(int** out);
+int device_fault_check(cudaStream_t s);
 
 }  // namespace rtm

@@ -248,6 +248,7 @@ struct GmState {
     int converged;
     int zero_rhs;
     int cycle_ran;
+    int skip_update;  // = !cycle_ran: the preconditioner's skip flag for the right-preconditioned update
     unsigned int counter;
 };
 
@@ -309,6 +310,7 @@ __global__ void __launch_bounds__(kRT) k_gm_norm(const T2* __restrict__ w, int64
         S.active = !S.done;
         S.skip_step = !S.active;
         S.cycle_ran = S.active;
+        S.skip_update = !S.cycle_ran;
     }
 }
 
@@ -832,10 +834,40 @@ __global__ void __launch_bounds__(kRT) k_gm_xupdate(T2* __restrict__ x, const T2
     }
 }
 
+// u = V(:, 1:step) y (right preconditioning: x += M u follows).
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_vy(T2* __restrict__ u, const T2* __restrict__ V, int64_t n, int nrhs,
+                                               GmState* st, GmArrays ar) {
+    const int rhs = blockIdx.y;
+    const GmState& S = st[rhs];
+    if (!S.cycle_ran) return;
+    const int k = S.step;
+    const double2* y = ar.y + (int64_t)rhs * ar.m;
+    T2* ur = u + rhs * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = make_double2(0, 0);
+        for (int l = 0; l < k; ++l) v = dadd(v, dmul(to_d2(V[((int64_t)l * nrhs + rhs) * n + i]), y[l]));
+        ur[i] = from_d2<T2>(v);
+    }
+}
+
+// x += w where the cycle ran.
+template <typename T2>
+__global__ void __launch_bounds__(kRT) k_gm_addx(T2* __restrict__ x, const T2* __restrict__ w, int64_t n,
+                                                 const GmState* st) {
+    const int rhs = blockIdx.y;
+    if (!st[rhs].cycle_ran) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 a = to_d2(x[rhs * n + i]), b = to_d2(w[rhs * n + i]);
+        x[rhs * n + i] = from_d2<T2>(make_double2(a.x + b.x, a.y + b.y));
+    }
+}
+
 __global__ void k_gm_cycle_end(GmState* st, int nrhs) {
     const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
     if (rhs >= nrhs) return;
     st[rhs].cycle_ran = 0;
+    st[rhs].skip_update = 1;
     st[rhs].active = 0;
     st[rhs].skip_step = 1;
 }
@@ -981,9 +1013,10 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
     RTM_TRY(resb.alloc(sizeof(double2) * nrhs));
     RTM_TRY(cnt.alloc(sizeof(unsigned int) * nrhs));
     std::vector<CgState> init(nrhs);
-    for (auto& st : init) {
+    for (int k = 0; k < nrhs; ++k) {
+        CgState& st = init[k];
         memset(&st, 0, sizeof st);
-        st.tol = cfg.tolerance;
+        st.tol = cfg.tolerances ? cfg.tolerances[k] : cfg.tolerance;
         st.max_iterations = cfg.max_iterations;
     }
     RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(CgState) * nrhs, cudaMemcpyHostToDevice, s));
@@ -1048,6 +1081,7 @@ static int cocg(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* bv
     res.history.resize((size_t)hs * nrhs);
     RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
     RTM_CUDA(cudaStreamSynchronize(s));
+    RTM_TRY(device_fault_check(s));
     res.hist_stride = hs;
     res.stats.resize(nrhs);
     for (int k = 0; k < nrhs; ++k) {
@@ -1080,13 +1114,14 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     }
     const int nb = reduce_blocks(n);
     const size_t vec = (size_t)n * nrhs * sizeof(T2);
-    // Right (flexible) preconditioning keeps z_j = M v_j and solves A M u = b, x = Z y: the monitored
-    // residual is the residual of A x = b itself. Left preconditioning is the reference's form.
+    // Right preconditioning solves A M u = b with x = x0 + M (V y) at the end of each cycle: the
+    // monitored residual is the residual of A x = b itself. The preconditioners here are fixed linear
+    // operators, so M (V y) equals the flexible form's sum of the z_j = M v_j y_j, and no basis of the
+    // z_j is kept. Left preconditioning is the reference's form.
     const bool right = M != nullptr && cfg.right_preconditioned;
-    DeviceBuffer V, Z, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
+    DeviceBuffer V, w, t, stb, H, g, cs, sn, h, c, y, part, hist, resb, cnt;
     StreamSyncGuard guard(s);
     RTM_TRY(V.alloc(vec * (m + 1)));
-    if (right) RTM_TRY(Z.alloc(vec * m));
     RTM_TRY(w.alloc(vec));
     RTM_TRY(t.alloc(vec));
     RTM_TRY(stb.alloc(sizeof(GmState) * nrhs));
@@ -1105,12 +1140,14 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     RTM_CUDA(cudaMemsetAsync(H.ptr, 0, H.bytes, s));
     RTM_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes, s));
     std::vector<GmState> init(nrhs);
-    for (auto& st : init) {
+    for (int k = 0; k < nrhs; ++k) {
+        GmState& st = init[k];
         memset(&st, 0, sizeof st);
-        st.tol = cfg.tolerance;
+        st.tol = cfg.tolerances ? cfg.tolerances[k] : cfg.tolerance;
         st.max_iterations = cfg.max_iterations;
         st.m = m;
         st.skip_step = 1;
+        st.skip_update = 1;
     }
     RTM_CUDA(cudaMemcpyAsync(stb.ptr, init.data(), sizeof(GmState) * nrhs, cudaMemcpyHostToDevice, s));
     k_fill<<<64, 256, 0, s>>>(hist.as<double>(), (int64_t)hs * nrhs, NAN);
@@ -1123,6 +1160,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     const int stride = (int)(sizeof(GmState) / sizeof(int));
     SkipFlags skip_step{&st[0].skip_step, stride};
     SkipFlags skip_done{&st[0].done, stride};
+    SkipFlags skip_update{&st[0].skip_update, stride};
     const dim3 grid(nb, nrhs);
     // reference = ||P b|| (iterate_.m:9); ||b|| with right preconditioning
     if (M && !right) RTM_TRY(M->apply(b, w.ptr, nrhs, s, SkipFlags{}));
@@ -1163,9 +1201,8 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
         for (int j = 0; j < m; ++j) {
             T2* vj = Vp + (int64_t)j * nrhs * n;
             if (right) {
-                T2* zj = Z.as<T2>() + (int64_t)j * nrhs * n;
-                RTM_TRY(M->apply(vj, zj, nrhs, s, skip_step));
-                RTM_TRY(A->apply(zj, w.ptr, nrhs, s, skip_step));
+                RTM_TRY(M->apply(vj, t.ptr, nrhs, s, skip_step));
+                RTM_TRY(A->apply(t.ptr, w.ptr, nrhs, s, skip_step));
             } else if (M) {
                 RTM_TRY(A->apply(vj, t.ptr, nrhs, s, skip_step));
                 RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_step));
@@ -1179,9 +1216,18 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
             count_launch(1);
         }
         launch_gm_solve(st, ar, nrhs, s);
-        k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, right ? Z.as<T2>() : Vp, n, nrhs, st, ar);
+        if (right) {
+            k_gm_vy<T2><<<grid, kRT, 0, s>>>(t.as<T2>(), Vp, n, nrhs, st, ar);
+            count_launch();
+            RTM_TRY(M->apply(t.ptr, w.ptr, nrhs, s, skip_update));
+            k_gm_addx<T2><<<grid, kRT, 0, s>>>(x, w.as<T2>(), n, st);
+            count_launch();
+        } else {
+            k_gm_xupdate<T2><<<grid, kRT, 0, s>>>(x, Vp, n, nrhs, st, ar);
+            count_launch();
+        }
         k_gm_cycle_end<<<(nrhs + 31) / 32, 32, 0, s>>>(st, nrhs);
-        count_launch(2);
+        count_launch();
         RTM_TRY(A->apply(x, t.ptr, nrhs, s, skip_done));
         k_residual<T2><<<grid, kRT, 0, s>>>(b, t.as<T2>(), t.as<T2>(), n, &st[0].done, stride);
         count_launch();
@@ -1215,6 +1261,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     res.history.resize((size_t)hs * nrhs);
     RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
     RTM_CUDA(cudaStreamSynchronize(s));
+    RTM_TRY(device_fault_check(s));
     res.hist_stride = hs;
     res.stats.resize(nrhs);
     for (int k = 0; k < nrhs; ++k) {
@@ -1230,9 +1277,13 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
 
 // ============================================================================================
 // Mixed precision: FP64 iterative refinement around an FP32 inner solve.
-//   r = b - A64 x (FP64); r32 = r / ||r||; d32 ~ A32^-1 r32 (one FP32 FGMRES cycle, or FP32 COCG);
+//   r = b - A64 x (FP64); r32 = r / ||r||; d32 ~ A32^-1 r32 (FP32 flexible GMRES, or FP32 COCG);
 //   x += ||r|| d32; repeat until ||b - A64 x|| / ||b|| < tolerance. The outer residual is always
 //   the true FP64 residual, so the stopping test holds for the FP64 operator.
+// Each right-hand side's inner solve stops at the relative residual that meets the outer tolerance
+// in this step, 0.5 tolerance ||b|| / ||r|| (an inner residual eps leaves an outer one of about
+// eps ||r|| plus the FP32 operator's error), but never aims below inner_tolerance, the accuracy an
+// FP32 solve reaches safely; a step that stops there leaves the rest to the next refinement.
 
 __global__ void k_ir_to32(const double2* __restrict__ r, float2* __restrict__ r32, int64_t n, const double2* res,
                           const int* done) {
@@ -1311,6 +1362,8 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     int inner_total = 0, steps = 0;
     res.matvecs = 0;
     std::vector<int> hd(nrhs);
+    std::vector<double2> hr(nrhs);
+    std::vector<double> inner_tol(nrhs);
     for (int step = 0;; ++step) {
         RTM_TRY(A64->apply(x, t64.ptr, nrhs, s, SkipFlags{}));
         k_residual<double2><<<grid, kRT, 0, s>>>(b, t64.as<double2>(), r64.as<double2>(), n, nullptr, 0);
@@ -1321,6 +1374,7 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         count_launch(3);
         res.matvecs += 1;
         RTM_CUDA(cudaMemcpyAsync(hd.data(), done.ptr, sizeof(int) * nrhs, cudaMemcpyDeviceToHost, s));
+        RTM_CUDA(cudaMemcpyAsync(hr.data(), resb.ptr, sizeof(double2) * nrhs, cudaMemcpyDeviceToHost, s));
         RTM_CUDA(cudaStreamSynchronize(s));
         steps = step;
         bool all = true;
@@ -1330,9 +1384,14 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         k_ir_to32<<<grid, kRT, 0, s>>>(r64.as<double2>(), r32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
         // The inner FP32 solve of A32 d = r / ||r||: COCG, or restarted flexible GMRES(m).
+        for (int k = 0; k < nrhs; ++k) {
+            const double need = hr[k].x > 0 ? 0.5 * cfg.tolerance * hr[k].y / hr[k].x : 0.5;
+            inner_tol[k] = std::max(cfg.inner_tolerance, std::min(0.5, need));
+        }
         SolveConfig ic;
         ic.method = inner_cg ? RTM_METHOD_CG : RTM_METHOD_GMRES;
         ic.tolerance = cfg.inner_tolerance;
+        ic.tolerances = inner_tol.data();
         ic.max_iterations = std::max(1, cfg.max_iterations - inner_total);
         ic.restart = m;
         ic.check_every = cfg.check_every;
@@ -1355,6 +1414,7 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     res.history.resize((size_t)hs * nrhs);
     RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
     RTM_CUDA(cudaStreamSynchronize(s));
+    RTM_TRY(device_fault_check(s));
     res.hist_stride = hs;
     res.stats.resize(nrhs);
     for (int k = 0; k < nrhs; ++k) {

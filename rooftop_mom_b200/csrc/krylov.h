@@ -11,10 +11,11 @@ namespace rtm {
 struct SolveConfig {
     int method = RTM_METHOD_CG;
     double tolerance = 1e-6;
+    const double* tolerances = nullptr;  // host, one per right-hand side: overrides `tolerance` when set
     int max_iterations = 1000;
     int restart = 50;
     int check_every = 0;
-    double inner_tolerance = 1e-4;
+    double inner_tolerance = 1e-4;  // mixed: the tightest relative residual an inner FP32 solve aims at
     int max_refinements = 20;
     int right_preconditioned = 0;  // GMRES: 0 left (the reference's form), 1 right (flexible)
     const std::atomic<int>* cancel = nullptr;  // nonzero: stop at the next host check (unconverged result)

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <complex>
 #include <map>
 #include <mutex>
 #include <string>
@@ -160,7 +161,9 @@ int fast_fft_size(int count) {
 }
 
 static bool make_plan(int n, FftPlan& p) {
+    p = FftPlan{};
     p.n = n;
+    p.m = n;
     p.nstages = 0;
     int m = n;
     auto push = [&](int r) {
@@ -205,6 +208,60 @@ static void root_table(int n, long double scale, std::vector<double2>& out) {
     }
 }
 
+// In-place radix-2 DFT of a power-of-two length in long double (host; the Bluestein kernel spectrum).
+static void host_dft_pow2(std::vector<std::complex<long double>>& a) {
+    const size_t m = a.size();
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (size_t i = 1, j = 0; i < m; ++i) {
+        size_t bit = m >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= m; len <<= 1) {
+        for (size_t i = 0; i < m; i += len)
+            for (size_t k = 0; k < len / 2; ++k) {
+                const long double ang = -2.0L * pi * (long double)k / (long double)len;
+                const std::complex<long double> w(cosl(ang), sinl(ang));
+                const std::complex<long double> u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+    }
+}
+
+// Bluestein plan of length n: X_k = c_k sum_j (x_j c_j) b_(k-j) with c_j = exp(-i pi j^2 / n) and
+// b_d = conj(c_d), the linear convolution evaluated as a circular one of length m >= 2n - 1 by two
+// power-of-two transforms. Fills the radices of m and the three tables' host values.
+static bool make_bluestein(int n, FftPlan& p, std::vector<double2>& chirp, std::vector<double2>& kern,
+                           std::vector<double2>& twm) {
+    int m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    if (!make_plan(m, p)) return false;
+    p.n = n;
+    p.m = m;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    chirp.resize(n);
+    std::vector<std::complex<long double>> b(m, 0.0L);
+    for (int j = 0; j < n; ++j) {
+        // j^2 mod 2n keeps the angle small (exp(-i pi 2n / n) = 1)
+        const long double a = pi * (long double)((int64_t)j * j % (2 * (int64_t)n)) / (long double)n;
+        chirp[j] = make_double2((double)cosl(a), (double)(-sinl(a)));
+        const std::complex<long double> bj(cosl(a), sinl(a));
+        b[j] = bj;
+        if (j) b[m - j] = bj;
+    }
+    host_dft_pow2(b);
+    kern.resize(m);
+    for (int k = 0; k < m; ++k) kern[k] = make_double2((double)(b[k].real() / m), (double)(b[k].imag() / m));
+    twm.resize(m);
+    for (int k = 0; k < m; ++k) {
+        const long double a = 2.0L * pi * (long double)k / (long double)m;
+        twm[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+    }
+    return true;
+}
+
 int fft_tables(int n, const FftTables** out) {
     if (n < 1) return fail(RTM_ERR_ARG, "FFT length must be positive");
     int dev = 0;
@@ -216,9 +273,9 @@ int fft_tables(int n, const FftTables** out) {
         return RTM_OK;
     }
     TableEntry e;
-    if (!make_plan(n, e.t.plan))
-        return fail(RTM_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has a prime factor above " +
-                                             std::to_string(kMaxGenericRadix));
+    std::vector<double2> chirp, kern, twm;
+    if (!make_plan(n, e.t.plan) && !make_bluestein(n, e.t.plan, chirp, kern, twm))
+        return fail(RTM_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " has no plan in this build");
     std::vector<double2> tw, mod;
     root_table(n, 2.0L, tw);
     root_table(n, 1.0L, mod);
@@ -242,6 +299,28 @@ int fft_tables(int n, const FftTables** out) {
     e.t.mod64 = d_mod;
     e.t.tw32 = d_tw32;
     e.t.mod32 = d_mod32;
+    if (e.t.plan.m != n) {
+        // the Bluestein tables, FP64 then FP32: chirp (n), kernel spectrum (m), roots of length m (m)
+        const size_t cnt = chirp.size() + kern.size() + twm.size();
+        void* mem = nullptr;
+        RTM_CUDA(cudaMalloc(&mem, cnt * (sizeof(double2) + sizeof(float2))));
+        std::vector<double2> all;
+        all.insert(all.end(), chirp.begin(), chirp.end());
+        all.insert(all.end(), kern.begin(), kern.end());
+        all.insert(all.end(), twm.begin(), twm.end());
+        std::vector<float2> all32(cnt);
+        for (size_t i = 0; i < cnt; ++i) all32[i] = make_float2((float)all[i].x, (float)all[i].y);
+        double2* d64 = (double2*)mem;
+        float2* d32 = (float2*)(d64 + cnt);
+        RTM_CUDA(cudaMemcpy(d64, all.data(), cnt * sizeof(double2), cudaMemcpyHostToDevice));
+        RTM_CUDA(cudaMemcpy(d32, all32.data(), cnt * sizeof(float2), cudaMemcpyHostToDevice));
+        e.t.plan.chirp64 = d64;
+        e.t.plan.kern64 = d64 + chirp.size();
+        e.t.plan.twm64 = d64 + chirp.size() + kern.size();
+        e.t.plan.chirp32 = d32;
+        e.t.plan.kern32 = d32 + chirp.size();
+        e.t.plan.twm32 = d32 + chirp.size() + kern.size();
+    }
     auto res = g_tables.emplace(TableKey{dev, n}, e);
     *out = &res.first->second.t;
     return RTM_OK;
@@ -510,3 +589,4 @@ extern "C" int rtm_budget_query(double* ceiling_bytes, double* held_bytes) {
     if (held_bytes) *held_bytes = rtm::g_held;
     return RTM_OK;
 }
+

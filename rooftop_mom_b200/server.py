@@ -20,20 +20,6 @@ from . import _lib as L
 
 
 PRECONDITIONERS = {None: 0, "blockJacobi": 1, "rChan": 2}
-LARGEST_RADIX = 61  # the largest prime factor the FFT plans transform
-
-
-def circulant_supported(countX, countY):
-    """True when the rChan circulant can be built on the face grid: no prime factor of the face counts above
-    the largest radix of the FFT plans (the circulant's period is the face grid itself; it cannot pad)."""
-    def ok(n):
-        p = 2
-        while p * p <= n:
-            while n % p == 0:
-                n //= p
-            p += 1
-        return n <= LARGEST_RADIX
-    return ok(int(countX)) and ok(int(countY))
 
 
 class Request:

@@ -35,18 +35,9 @@ def test_the_batch_of_waves_is_seeded_and_within_its_ranges():
     assert np.all(np.abs(np.einsum("ij,ij->i", d1, p1)) < 1e-15)
 
 
-def test_circulant_eligibility_follows_the_largest_radix():
-    from rooftop_mom_b200.server import circulant_supported
-
-    assert circulant_supported(64, 48) and circulant_supported(61, 1) and circulant_supported(768, 1)
-    assert not circulant_supported(67, 10) and not circulant_supported(10, 2 * 71)
-
-
-def test_the_request_stream_is_seeded_and_chooses_a_preconditioner_per_grid():
+def test_the_request_stream_is_seeded_and_takes_the_rchan_circulant():
     import bench
     import rooftop_mom_b200 as R
-    from rooftop_mom_b200.server import circulant_supported
-
     a = bench.serving_requests(R, 50, 0)
     b = bench.serving_requests(R, 50, 0)
     for qa, qb in zip(a, b):
@@ -55,8 +46,7 @@ def test_the_request_stream_is_seeded_and_chooses_a_preconditioner_per_grid():
         assert 16 <= sa.count_x <= 768 and (sa.count_y == 1 or 16 <= sa.count_y <= 768)
         # strips carry the delta gap, plates the plane wave
         assert (sa.count_y == 1) == (sa.excitation == 1)
-        expect = 2 if circulant_supported(sa.count_x, sa.count_y) else 1
-        assert sa.preconditioner == expect
+        assert sa.preconditioner == 2 and sa.method == 0  # rChan COCG on every face grid
         lam = 2 * math.pi / sa.wavenumber
         assert 10 - 1e-9 <= lam / sa.size_x <= 25 + 1e-9
 
@@ -77,3 +67,16 @@ def test_the_reference_arm_prints_its_line_on_the_host():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_takes_the_oracle_iteration_count_of_each_sampled_workload():
+    """The reference arm extrapolates a sampled step to a whole solve with the oracle's own iteration count
+    (not the GPU's) for every workload too large to run whole per step, and says where the count comes
+    from."""
+    import bench
+
+    for name, w in bench.WORKLOADS.items():
+        if name in ("c4", "c5") or w["n"] <= bench.FULL_SOLVE_MAX_FACES:
+            continue
+        assert bench.ORACLE_ITERATIONS[name] > 0
+        assert bench.ORACLE_ITERATION_SOURCE[name]

@@ -279,3 +279,92 @@ def test_a_singular_circulant_raises(kernel):
     with pytest.raises(L.RtmError) as e:
         R.Preconditioner(prob, kernel=kernel)
     assert e.value.identifier == "rooftopMoM:preconditioner:singular"
+
+
+# Face grids whose counts have a prime factor above the largest direct radix (61): their transforms run as
+# Bluestein (chirp-z) convolutions of a power-of-two length (FFTApplicator.m:57,70 takes any face count).
+BLUESTEIN_GRIDS = {
+    "prime67": (67, 67, 0.05, 0.05),
+    "prime127x131": (127, 131, 0.05, 0.04),
+    "strip1x127": (1, 127, 0.01, 0.05),
+    "strip127x1": (127, 1, 0.05, 0.01),
+    "mixed134x71": (134, 71, 0.05, 0.05),
+}
+
+
+@pytest.mark.parametrize("name", sorted(BLUESTEIN_GRIDS))
+@pytest.mark.parametrize("kernel", ["rChan", "strang", "tChan"])
+def test_circulants_on_large_prime_face_grids_match_the_oracle(name, kernel):
+    """The reference's default rChan / partwise preconditioner (Preconditioner.m:26-29) and the Strang and
+    T. Chan ones on face grids of 67, 127, 131 faces: built and applied through Bluestein transforms,
+    against the oracle's circulant (1e-11, as the folds on the other grids)."""
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, geometry as G, preconditioner as PC, spectra as S
+
+    cx, cy, a, b = BLUESTEIN_GRIDS[name]
+    prob = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3)
+    pc = R.Preconditioner(prob, kernel=kernel)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, a, b, 3)
+    inv = PC.circulant(A.Generators(xx, yy, e, rt.content), a, b, kernel, "partwise")
+    v = random_vector(rt.count, seed=7)
+    assert rel(pc.apply(v), S.fft_apply(rt, inv, rt.content, v)) < 1e-11
+
+
+@pytest.mark.parametrize("builder", ["blockwise", "hybrid"])
+def test_other_builders_on_a_large_prime_face_grid_match_the_oracle(builder):
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, geometry as G, preconditioner as PC, spectra as S
+
+    cx, cy, a, b = BLUESTEIN_GRIDS["prime67"]
+    prob = R.Problem(R.Mesh(cx, cy, a, b), 2 * np.pi, quadratureOrder=3)
+    pc = R.Preconditioner(prob, kernel="rChan", builder=builder)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, a, b, 3)
+    inv = PC.circulant(A.Generators(xx, yy, e, rt.content), a, b, "rChan", builder)
+    v = random_vector(rt.count, seed=8)
+    assert rel(pc.apply(v), S.fft_apply(rt, inv, rt.content, v)) < 1e-11
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_large_prime_circulant_in_both_precisions_against_fp64(precision):
+    """The FP32 Bluestein tables (the precision form's inner preconditioner) against the FP64 apply."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(127, 131, 0.05, 0.04), 2 * np.pi, quadratureOrder=3)
+    v = random_vector(prob.rooftopCount(), seed=9)
+    ref = R.Preconditioner(prob, kernel="rChan").apply(v)
+    got = R.Preconditioner(prob, kernel="rChan", precision=precision).apply(v)
+    assert rel(got, ref) < (1e-14 if precision == "double" else 2e-5)
+
+
+@pytest.mark.parametrize("count", [(68, 40), (40, 68), (68, 1)])
+def test_fft_product_with_a_large_prime_embedding_matches_the_dense_matrix(count):
+    """The 'fft' product embeds on 2n - 2 faces (generateEmbeddingSpectra.m); 2 * 68 - 2 = 2 * 67 runs as a
+    Bluestein transform."""
+    import rooftop_mom_b200 as R
+    from oracle import assembly as A, excitation as EX, geometry as G
+
+    cx, cy = count
+    prob = R.Problem(R.Mesh(cx, cy, 0.05, 0.05), 2 * np.pi, quadratureOrder=3)
+    xx, yy, e = prob.generators().arrays()
+    rt = G.Rooftops(cx, cy, 0.05, 0.05, 3)
+    dense = EX.dense_matrix(A.Generators(xx, yy, e, rt.content), rt)
+    v = random_vector(rt.count, seed=10)
+    assert rel(R.Operator(prob, product="fft").apply(v), dense @ v) < 1e-12
+
+
+def test_a_rchan_cocg_solve_on_a_large_prime_plate_converges():
+    """COCG with the reference's default preconditioner on a 67 x 67 plate (before the Bluestein stage
+    this preconditioner could not be built on it)."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(67, 67, 1 / 20, 1 / 20), 2 * np.pi)
+    op = R.Operator(prob)
+    exc = R.Excitation.planeWave(prob)
+    plain = R.Solver(method="cg", tolerance=1e-8, maxIterationCount=5000).solve(op, exc)
+    pre = R.Solver(method="cg", tolerance=1e-8, maxIterationCount=5000).solve(op, exc,
+                                                                              preconditioner=R.Preconditioner(prob))
+    assert plain.converged() and pre.converged()
+    assert pre.iterationCount() < plain.iterationCount()
+    assert rel(pre.solution(), plain.solution()) < 1e-6
