@@ -149,6 +149,32 @@ RTM_API int rtm_operator_apply_fixed_scratch(const rtm_operator* op, const void*
 /* Size of the fixed scratch array in bytes. */
 RTM_API int rtm_fixed_scratch_bytes(double* bytes);
 
+/* Autotuner of the split product. No counterpart in the reference (whose benchmarks/measureFFTPlanner.m
+ * times FFTW's planner for the same purpose). For a plate of count_x x count_y faces (both at least 2) and
+ * a precision, measures every candidate transform grid, the reference's 7-smooth sizes
+ * (generateFastFFTSize.m:11-15) and the next powers of two, and on power-of-two grids every kernel
+ * schedule (CTAs per SM of the y passes, form of the x-mix), each timed on the device over applies to
+ * nrhs vectors; with RTM_TUNE_FLUSH_L2 each apply follows a write of 256 MB, so that the spectra start
+ * out of L2 as inside a solve. The fastest is kept for this device: split products created afterwards for
+ * that face grid and precision use it (a larger transform grid gives the same product up to rounding).
+ * RTM_TUNE_REFERENCE_SIZES keeps the reference's sizes and sweeps the schedules only; RTM_TUNE_VERBOSE
+ * writes every configuration's time to stderr. */
+#define RTM_TUNE_FLUSH_L2 1
+#define RTM_TUNE_REFERENCE_SIZES 2
+#define RTM_TUNE_VERBOSE 4
+typedef struct rtm_tune_result {
+    int fft_x, fft_y;          /* chosen transform grid */
+    int y_blocks, mix_kind;    /* chosen schedule: CTAs per SM of the y passes (1..3) and the x-mix form
+                                  (0..2 direct with 1..3 CTAs per SM, 3 pipelined); 0 and -1 off the
+                                  power-of-two path */
+    double seconds;            /* device time of one product (nrhs vectors) with the choice */
+    double reference_seconds;  /* the same with the reference's sizes and the default schedule */
+    int candidates;            /* configurations measured */
+} rtm_tune_result;
+RTM_API int rtm_tune_product(int count_x, int count_y, int precision, int nrhs, int flags, rtm_tune_result* out);
+/* Forgets every choice of the autotuner (products created afterwards take the reference's sizes). */
+RTM_API int rtm_tune_clear(void);
+
 /* A dense n x n complex operator (column-major), for solving any small system with the same solvers
  * (the matrix operator of IterativeMethod.solve, convertToHandle.m:10-16). */
 RTM_API int rtm_operator_create_dense(const double* matrix, int64_t n, int where, rtm_operator** out);

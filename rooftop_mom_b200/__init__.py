@@ -13,7 +13,9 @@ from .api import (  # noqa: F401
     Resources,
     Result,
     Solver,
+    clearTuning,
     fast_fft_size,
+    tuneProduct,
 )
 from .server import Request, Server  # noqa: F401
 

@@ -56,6 +56,16 @@ class SolveStats(C.Structure):
 
 _P = C.c_void_p
 _PP = C.POINTER(C.c_void_p)
+class TuneResult(C.Structure):
+    _fields_ = [("fft_x", C.c_int), ("fft_y", C.c_int), ("y_blocks", C.c_int), ("mix_kind", C.c_int),
+                ("seconds", C.c_double), ("reference_seconds", C.c_double), ("candidates", C.c_int)]
+
+
+TUNE_FLUSH_L2 = 1
+TUNE_REFERENCE_SIZES = 2
+TUNE_VERBOSE = 4
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_double), ("max_active", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
 
@@ -97,6 +107,8 @@ _SIGNATURES = {
     "rtm_operator_apply": [_P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
     "rtm_operator_apply_fixed_scratch": [_P, _P, _P, C.c_int64, C.c_int, _P],
     "rtm_fixed_scratch_bytes": [_P],
+    "rtm_tune_product": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(TuneResult)],
+    "rtm_tune_clear": [],
     "rtm_operator_create_dense": [_P, C.c_int64, C.c_int, _PP],
     "rtm_operator_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                           C.POINTER(C.c_double)],

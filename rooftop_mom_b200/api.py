@@ -739,6 +739,28 @@ class Solver:
         return [Result(x[k * count:(k + 1) * count], stats[k], hist[k], excitation) for k in range(nrhs)]
 
 
+def tuneProduct(mesh: Mesh, precision="double", nrhs: int = 1, flushL2: bool = True, referenceSizes: bool = False,
+                verbose: bool = False):
+    """Autotunes the split product of a plate (rtm_tune_product): measures the candidate transform grids (the
+    reference's 7-smooth sizes, generateFastFFTSize.m, and the next powers of two) and kernel schedules on the
+    device and keeps the fastest for the operators created afterwards for this face grid and precision.
+    Returns the choice and its time beside the reference sizes' time."""
+    if precision not in L.PRECISIONS:
+        raise _err("rooftopMoM:operator:invalidPrecision", "The precision is 'double' or 'single'.")
+    cx, cy = mesh.count()
+    out = L.TuneResult()
+    flags = ((L.TUNE_FLUSH_L2 if flushL2 else 0) | (L.TUNE_REFERENCE_SIZES if referenceSizes else 0)
+             | (L.TUNE_VERBOSE if verbose else 0))
+    L.call("rtm_tune_product", cx, cy, L.PRECISIONS[precision], int(nrhs), flags, C.byref(out))
+    return {"fftSize": (out.fft_x, out.fft_y), "yBlocks": out.y_blocks, "mixKind": out.mix_kind,
+            "seconds": out.seconds, "referenceSeconds": out.reference_seconds, "candidates": out.candidates}
+
+
+def clearTuning():
+    """Forgets every autotuner choice (rtm_tune_clear)."""
+    L.call("rtm_tune_clear")
+
+
 class Resources:
     """src/+rooftopMoM/Resources.m for device memory: the HBM ceiling and the byte models."""
 

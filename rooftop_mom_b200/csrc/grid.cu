@@ -322,7 +322,7 @@ size_t GridApplicator::work_bytes_per_rhs() const {
 
 template <typename T>
 static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip,
-                   void* work) {
+                   void* work, int* fault) {
     using T2 = typename Cx<T>::T2;
     RTM_TRY(set_smem_attrs<T>());
     const T2* x = static_cast<const T2*>(xv);
@@ -372,14 +372,14 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
         return RTM_OK;
     }
     a.scale = (T)(1.0 / ((double)g.P * g.Q));
-    RTM_TRY(device_fault_word(&a.fault));
+    a.fault = fault;
     a.work = static_cast<T2*>(work);
     a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)elem;
     if (g.mode == kGen3 && g.nsx == 2 && g.nsy == 2 && !g.lean && fast_split_eligible(g.P, g.Q, sizeof(T) == 8)) {
         a.py0 = 0;
         a.npy = 2;
         a.accumulate = 0;
-        return launch_fast_split<T>(a, nrhs, x, y, s);
+        return launch_fast_split<T>(a, nrhs, x, y, g.sched, s);
     }
     const int passes = g.lean ? g.nsy : 1;
     const int npy = g.lean ? 1 : g.nsy;
@@ -426,7 +426,6 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
 int GridApplicator::reserve(int nrhs) {
     // kernel attributes and the fault word are set up here, outside of any stream capture
     RTM_TRY(precision == RTM_FP64 ? set_smem_attrs<double>() : set_smem_attrs<float>());
-    int* fault = nullptr;
     RTM_TRY(device_fault_word(&fault));
     if (nrhs <= max_rhs && (mode == kStrip || work.bytes >= work_bytes_per_rhs() * (size_t)nrhs)) return RTM_OK;
     if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
@@ -436,8 +435,9 @@ int GridApplicator::reserve(int nrhs) {
 
 int GridApplicator::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) {
     if (nrhs < 1 || nrhs > max_rhs) return fail(RTM_ERR_ARG, "more right-hand sides than the product reserved");
-    return precision == RTM_FP64 ? apply_t<double>(*this, x, y, nrhs, s, skip, work.ptr)
-                                 : apply_t<float>(*this, x, y, nrhs, s, skip, work.ptr);
+    if (!fault) RTM_TRY(device_fault_word(&fault));
+    return precision == RTM_FP64 ? apply_t<double>(*this, x, y, nrhs, s, skip, work.ptr, fault)
+                                 : apply_t<float>(*this, x, y, nrhs, s, skip, work.ptr, fault);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -457,8 +457,10 @@ int apply_fixed_scratch(const GridApplicator& g, const void* x, void* y, int nrh
                                       std::to_string(cap) + " bytes");
     void* work = nullptr;
     if (g.mode != kStrip) RTM_TRY(fixed_scratch_address(&work));
-    return g.precision == RTM_FP64 ? apply_t<double>(g, x, y, nrhs, s, SkipFlags{}, work)
-                                   : apply_t<float>(g, x, y, nrhs, s, SkipFlags{}, work);
+    int* fault = nullptr;
+    RTM_TRY(device_fault_word(&fault));
+    return g.precision == RTM_FP64 ? apply_t<double>(g, x, y, nrhs, s, SkipFlags{}, work, fault)
+                                   : apply_t<float>(g, x, y, nrhs, s, SkipFlags{}, work, fault);
 }
 
 // ============================================================================================
@@ -729,7 +731,7 @@ static void layout(GridApplicator& o, int cx, int cy) {
 }
 
 int build_product(const DeviceGenerators& g, double size_x, double size_y, int product, int precision, int max_rhs,
-                  GridApplicator& out, cudaStream_t s) {
+                  GridApplicator& out, cudaStream_t s, int force_P, int force_Q, const FastSchedule* force_sched) {
     const int cx = g.count_x, cy = g.count_y;
     layout(out, cx, cy);
     out.precision = precision;
@@ -751,8 +753,24 @@ int build_product(const DeviceGenerators& g, double size_x, double size_y, int p
         a.scale = 1.0;
     } else {
         // generateSubbandSpectra.m: fast FFT size and 2 subbands along every direction with more than one face.
+        // Any P >= countX gives the same product (the period 2P holds the whole two-sided generator), so the
+        // autotuner may pick another size for speed; the result differs by rounding only.
         out.P = cx > 1 ? fast_fft_size(cx) : 1;
         out.Q = cy > 1 ? fast_fft_size(cy) : 1;
+        out.sched = default_fast_schedule(out.P, out.Q, precision == RTM_FP64);
+        int tp = 0, tq = 0;
+        FastSchedule ts;
+        if (force_P > 0 || force_Q > 0) {
+            if (force_P > 0 && cx > 1) out.P = force_P;
+            if (force_Q > 0 && cy > 1) out.Q = force_Q;
+            out.sched = default_fast_schedule(out.P, out.Q, precision == RTM_FP64);
+        } else if (product == RTM_PRODUCT_SPLIT && tuned_choice(cx, cy, precision, &tp, &tq, &ts)) {
+            out.P = tp;
+            out.Q = tq;
+            out.sched = ts;
+        }
+        if (force_sched) out.sched = *force_sched;
+        if (out.P < cx || out.Q < cy) return fail(RTM_ERR_ARG, "a transform grid smaller than the face grid");
         out.nsx = cx > 1 ? 2 : 1;
         out.nsy = cy > 1 ? 2 : 1;
         a.Lx = out.nsx * out.P;

@@ -21,6 +21,20 @@ namespace rtm {
 
 enum GridMode { kGen3 = 0, kBlock4 = 1, kStrip = 2 };
 
+// How the three kernels of a power-of-two split product run (grid_fast.cu): the CTAs an SM holds in
+// the y passes (the launch bound; 1 to 3, 3 for FP64 only) and the form of the x-mix. A product takes the
+// schedule the autotuner measured best for its precision and transform grid (tune.cpp), or the rules of
+// default_fast_schedule when none was measured.
+enum MixKind { kMixDirect1 = 0, kMixDirect2 = 1, kMixDirect3 = 2, kMixPipelined = 3 };
+struct FastSchedule {
+    int y_blocks = 2;
+    int x_kind = kMixDirect1;
+};
+// True when both transform sizes take the power-of-two kernels: powers of two in [32, 1024] (FP64:
+// [32, 512]).
+bool fast_split_eligible(int P, int Q, bool fp64);
+FastSchedule default_fast_schedule(int P, int Q, bool fp64);
+
 struct GridApplicator : LinearOp {
     int mode = kGen3;
     int content = RTM_BOTH;
@@ -39,6 +53,8 @@ struct GridApplicator : LinearOp {
     DeviceBuffer spec;      // GEN3: [sub][3][Q][P]; BLOCK4: [4][Q][P]; STRIP: [sub][P]
     DeviceBuffer work;      // W
     int spec_blocks = 0;    // blocks stored
+    int* fault = nullptr;   // the device's fault word (looked up in reserve(), outside any capture)
+    FastSchedule sched;     // schedule of the power-of-two kernels (set when the product is built)
 
     // y = A x on the device for nrhs vectors of length n (precision of the product).
     int apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) override;
@@ -61,9 +77,17 @@ struct DeviceGenerators {
     DeviceBuffer xx, yy, e;
 };
 
-// Builds the split ('splitFFT' / 'leanSplitFFT') or embedding ('fft') product of the generators.
+// Builds the split ('splitFFT' / 'leanSplitFFT') or embedding ('fft') product of the generators. A split
+// product takes the transform grid and schedule the autotuner chose for its face grid and precision
+// (tuned_choice), else the reference's sizes (generateFastFFTSize.m) and default_fast_schedule;
+// force_P / force_Q (> 0) impose a transform grid (the autotuner's candidates).
 int build_product(const DeviceGenerators& g, double size_x, double size_y, int product, int precision, int max_rhs,
-                  GridApplicator& out, cudaStream_t s);
+                  GridApplicator& out, cudaStream_t s, int force_P = 0, int force_Q = 0,
+                  const FastSchedule* force_sched = nullptr);
+
+// The autotuner's measured choice for a face grid and precision on the current device (tune.cpp): false
+// when none was measured.
+bool tuned_choice(int count_x, int count_y, int precision, int* P, int* Q, FastSchedule* sched);
 
 // Builds the inverted circulant preconditioner on the face grid (generateCirculant.m:16-25).
 int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int kernel, int builder,

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "fft.cuh"
+#include "grid.h"
 #include "internal.h"
 
 namespace rtm {
@@ -43,9 +44,8 @@ template <typename A> __device__ __forceinline__ bool skipped(const A& a, int rh
 
 // Power-of-two split products with register-resident line transforms (grid_fast.cu). Eligible when
 // both transform sizes are powers of two in [32, 1024] (FP64: [32, 512]) for a product that keeps both
-// y subbands. Returns RTM_OK after launching the three kernels.
-bool fast_split_eligible(int P, int Q, bool fp64);
+// y subbands. Returns RTM_OK after launching the three kernels with the given schedule (grid.h).
 template <typename T>
-int launch_fast_split(const GridArgs<T>& a, int nrhs, const void* x, void* y, cudaStream_t s);
+int launch_fast_split(const GridArgs<T>& a, int nrhs, const void* x, void* y, const FastSchedule& f, cudaStream_t s);
 
 }  // namespace rtm

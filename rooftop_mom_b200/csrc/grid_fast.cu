@@ -22,14 +22,10 @@
 namespace rtm {
 namespace {
 
-// CTA size and CTAs per SM: FP32 256 threads x 2 (128 registers a thread), FP64 128 threads x 3 (170),
-// and for FP64 lines of 512 (32 values a thread) one CTA per SM (up to 255 registers, no spills).
+// CTA size: FP32 256 threads, FP64 128. How many CTAs an SM holds (the launch bound, which sets the
+// registers a thread may use) is part of the schedule a product runs with (FastSchedule, grid.h).
 template <typename T> struct Fast {
     static constexpr int threads = sizeof(T) == 8 ? 128 : 256;
-    static constexpr int blocks = sizeof(T) == 8 ? 3 : 2;
-};
-template <typename T, int N> struct FastBlocks {
-    static constexpr int value = (sizeof(T) == 8 && N >= 512) || (sizeof(T) == 4 && N >= 1024) ? 1 : Fast<T>::blocks;
 };
 
 template <int N> struct Shape;
@@ -40,8 +36,19 @@ template <> struct Shape<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Shape<512> { static constexpr int R1 = 32, R2 = 16; };
 template <> struct Shape<1024> { static constexpr int R1 = 32, R2 = 32; };
 
+// cos(pi k / 16) for k = 0 .. 8 (the real parts of the 32nd roots of unity).
+__host__ __device__ constexpr double cos_pi16(int k) {
+    return k == 0 ? 1.0 : k == 1 ? 0.980785280403230449126182236134239 : k == 2 ? 0.923879532511286756128183189396788
+         : k == 3 ? 0.831469612302545237078788377617906 : k == 4 ? 0.707106781186547524400844362104849
+         : k == 5 ? 0.555570233019602224742830813948533 : k == 6 ? 0.382683432365089771728459984030399
+         : k == 7 ? 0.195090322016128267848284868477022 : 0.0;
+}
+// The forward root w_32^k = exp(-i pi k / 16) = (cos, -sin), k < 16, as compile-time constants.
+__host__ __device__ constexpr double root32_re(int k) { return k <= 8 ? cos_pi16(k) : -cos_pi16(16 - k); }
+__host__ __device__ constexpr double root32_im(int k) { return k <= 8 ? -cos_pi16(8 - k) : -cos_pi16(k - 8); }
+
 // In-register DFT of R points, natural order in and out. R = 32 splits by decimation in frequency
-// into two 16-point transforms with the roots w_32^k = tw[k n / 32] of the length-n table.
+// into two 16-point transforms with the roots w_32^k (constants, no table reads).
 template <int R, bool INV, typename T2>
 __device__ __forceinline__ void dft_reg(T2 (&v)[R], const T2* __restrict__ tw, int n) {
     if constexpr (R == 4) {
@@ -52,16 +59,13 @@ __device__ __forceinline__ void dft_reg(T2 (&v)[R], const T2* __restrict__ tw, i
         dft16<INV>(v);
     } else {
         static_assert(R == 32, "radix");
+        using S = decltype(v[0].x);
         T2 a[16], b[16];
-        const int st = n / 32;
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             a[k] = cadd(v[k], v[k + 16]);
             b[k] = csub(v[k], v[k + 16]);
-            if (k) {
-                const T2 w = __ldg(&tw[k * st]);
-                b[k] = INV ? cmulc(b[k], w) : cmul(b[k], w);
-            }
+            if (k) b[k] = twc<INV>(b[k], (S)root32_re(k), (S)root32_im(k));
         }
         dft16<INV>(a);
         dft16<INV>(b);
@@ -71,6 +75,13 @@ __device__ __forceinline__ void dft_reg(T2 (&v)[R], const T2* __restrict__ tw, i
             v[2 * k + 1] = b[k];
         }
     }
+}
+
+template <typename T2> __device__ __forceinline__ T2 make_vec2(decltype(T2{}.x) x, decltype(T2{}.x) y) {
+    T2 r;
+    r.x = x;
+    r.y = y;
+    return r;
 }
 
 // Element (r, c) of a line buffer at base[r * RS + c * CS].
@@ -141,8 +152,8 @@ __device__ __forceinline__ void inv_second(T2 (&v)[Shape<N>::R1], int t, const T
 // y-forward: TI x-columns of one component; a group per (column, y subband). Thread index
 // l + TI (py + 2 t): consecutive threads take consecutive columns, so rows of TI elements are read
 // and written at once. W[py][c][k][i] = FFT_y(x_c(i, j) mod_y(j)^py).
-template <typename T, int NQ>
-__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) k_fast_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
+template <typename T, int NQ, int MINB>
+__global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_y_fwd(const GridArgs<T> a, const typename Cx<T>::T2* __restrict__ x) {
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -177,7 +188,96 @@ __global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) 
         for (int k2 = 0; k2 < R2; ++k2) dst[(int64_t)((t + R2 * s) + R1 * k2) * a.P] = v[s * R2 + k2];
 }
 
-// x-mix: persistent CTAs. A CTA takes the iterations it = blockIdx.x, blockIdx.x + gridDim.x, ...; an
+// x-mix, direct form (one CTA per TEAMS y frequencies; inputs loaded straight into registers, the spectra
+// read in the mix): teams of four groups (component c, x subband px) per y frequency j of subband py. Thread
+// index t + R2 (team * 4 + 2 px + c). Forward transform along x of W mod_x^px, the 2x2 block mix
+// with the subband spectra (the two components of a group pair meet through shared memory), inverse
+// transform, demodulation, the sum over px, scaled by 1 / (PQ), in place in W.
+template <typename T, int NP, int MINB>
+__global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_x_mix_direct(const GridArgs<T> a) {
+    using T2 = typename Cx<T>::T2;
+    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, S = R1 / R2;
+    constexpr int TEAMS = Fast<T>::threads / (4 * R2), LB = R1 * (R2 + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* sm = reinterpret_cast<T2*>(smem_raw);
+    griddep_wait();
+    griddep_launch_dependents();
+    const int py = blockIdx.y, rhs = blockIdx.z;
+    if (skipped(a, rhs)) return;
+    const int t = threadIdx.x % R2, gid = threadIdx.x / R2;
+    const int team = gid / 4, c = gid % 2, px = (gid / 2) % 2;
+    const int j = blockIdx.x * TEAMS + team;
+    const bool on = j < a.Q;
+    const int Q = a.Q;
+    const int64_t QP = (int64_t)Q * NP;
+    const LineBuf<T2> buf{sm + gid * LB, R2 + 1, 1};
+    T2* own = sm + gid * LB;
+    const T2* partner = sm + (gid ^ 1) * LB;
+    const int rows = a.rows[c];
+    T2* row = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * QP + (int64_t)(on ? j : 0) * NP;
+    T2 v[R1];
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int i = R2 * m1 + t;
+        T2 e = (on && i < rows) ? row[i] : czero<T2>();
+        if (px) e = cmul(e, __ldg(&a.modP[i]));
+        v[m1] = e;
+    }
+    fwd_first<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    fwd_second<NP>(v, t, a.twP, buf);
+    __syncthreads();  // the buffers are read; they now carry the spectra values to the partner
+#pragma unroll
+    for (int r = 0; r < R1; ++r) own[r * R2 + t] = v[r];
+    __syncthreads();
+    if (on) {
+        const int sub = px + 2 * py;
+        const T2* spec = a.spec + (int64_t)(sub * 3) * QP + (int64_t)j * NP;
+        const T2* ux = px ? a.ux1 : a.ux0;
+        const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
+        const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) {
+                const int k = (t + R2 * s) + R1 * k2;
+                const T2 E = __ldg(&spec[k]);
+                const T2 M = __ldg(&spec[(1 + c) * QP + k]);
+                const T2 uu = __ldg(&ux[k]);
+                const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
+                T2 qc = cmulc(uu, vv);
+                qc.x = -qc.x * a.inv_ab;
+                qc.y = -qc.y * a.inv_ab;
+                const T2 coupling = c ? cconj(qc) : qc;
+                const T cself = c ? cv : cu;
+                const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
+                // M me - cself E me + coupling E other = M me + E (coupling other - cself me)
+                const T2 cp = cmul(coupling, other);
+                const T2 d = make_vec2<T2>(cp.x - cself * me.x, cp.y - cself * me.y);
+                v[s * R2 + k2] = cadd(cmul(M, me), cmul(E, d));
+            }
+    }
+    __syncthreads();  // the partner values are read
+    inv_first<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    inv_second<NP>(v, t, a.twP, buf);
+    __syncthreads();
+    if (px) {
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) own[m1 * R2 + t] = cmulc(v[m1], __ldg(&a.modP[R2 * m1 + t]));
+    }
+    __syncthreads();
+    if (px || !on) return;
+    const T2* odd = sm + (gid + 2) * LB;
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) {
+        const int i = R2 * m1 + t;
+        if (i < rows) row[i] = cscale(cadd(v[m1], odd[m1 * R2 + t]), a.scale);
+    }
+}
+
+// x-mix, pipelined form: persistent CTAs. A CTA takes the iterations it = blockIdx.x, blockIdx.x + gridDim.x, ...; an
 // iteration is TEAMS consecutive y frequencies j of one (right-hand side, y subband py). Its inputs are
 // copied into shared memory one iteration ahead by bulk asynchronous copies (one thread issues them): the
 // W rows of both components (contiguous for consecutive j) as soon as the current ones are in registers,
@@ -200,13 +300,13 @@ template <typename T, int NP> struct MixShape {
 };
 
 template <typename T, int NP>
-__global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k_fast_x_mix(const GridArgs<T> a, int iters) {
+__global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k_fast_x_mix_pipe(const GridArgs<T> a, int iters) {
     using M = MixShape<T, NP>;
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = M::R1, R2 = M::R2, S = R1 / R2, TEAMS = M::TEAMS, LB = M::LB;
     constexpr unsigned BLOCK = TEAMS * NP * sizeof(T2);  // TEAMS consecutive rows of one grid
     static_assert(BLOCK % 16 == 0 && M::lines % 16 == 0 && M::wrows % 16 == 0, "bulk copies need 16-byte units");
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* sm = reinterpret_cast<T2*>(smem_raw);
     T2* wst = reinterpret_cast<T2*>(smem_raw + M::lines);
     T2* sst = reinterpret_cast<T2*>(smem_raw + M::lines + M::wrows);
@@ -302,10 +402,10 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
                     const T2 coupling = c ? cconj(qc) : qc;
                     const T cself = c ? cv : cu;
                     const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
-                    T2 o = cmul(Mk, me);
-                    o = csub(o, cscale(cmul(E, me), cself));
-                    o = cadd(o, cmul(coupling, cmul(E, other)));
-                    v[s * R2 + k2] = o;
+                    // Mk me - cself E me + coupling E other = Mk me + E (coupling other - cself me)
+                    const T2 cp = cmul(coupling, other);
+                    const T2 d = make_vec2<T2>(cp.x - cself * me.x, cp.y - cself * me.y);
+                    v[s * R2 + k2] = cadd(cmul(Mk, me), cmul(E, d));
                 }
         }
         __syncthreads();  // the spectra and the partner values are read
@@ -338,8 +438,8 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
 
 // y-inverse: TI columns of one component, a group per (column, y subband); inverse transform along y,
 // demodulation, the sum over py through shared memory, cropped into y.
-template <typename T, int NQ>
-__global__ void __launch_bounds__(Fast<T>::threads, (FastBlocks<T, NQ>::value)) k_fast_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
+template <typename T, int NQ, int MINB>
+__global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_y_inv(const GridArgs<T> a, typename Cx<T>::T2* __restrict__ y) {
     using T2 = typename Cx<T>::T2;
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2), G = 2 * TI;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -384,37 +484,69 @@ template <typename T, int NQ> size_t y_smem() {
     constexpr int R1 = Shape<NQ>::R1, R2 = Shape<NQ>::R2, TI = Fast<T>::threads / (2 * R2);
     return (size_t)2 * TI * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
 }
-template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd,
-                                           cudaStream_t s) {
+template <typename T, int NQ, int MINB> int launch_y_b(const GridArgs<T>& a, int nrhs, const void* x, void* y,
+                                                       bool fwd, cudaStream_t s) {
     using T2 = typename Cx<T>::T2;
     constexpr int TI = Fast<T>::threads / (2 * Shape<NQ>::R2);
     const size_t smem = y_smem<T, NQ>();
     static DeviceOnce once;
     RTM_TRY(once([smem]() -> int {
-        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_fwd<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_inv<T, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_fwd<T, NQ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_y_inv<T, NQ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         return RTM_OK;
     }));
     const int rows_max = a.rows[0] > a.rows[1] ? a.rows[0] : a.rows[1];
     const dim3 grid((rows_max + TI - 1) / TI, 2, nrhs);
     if (fwd)
-        k_fast_y_fwd<T, NQ><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<const T2*>(x));
+        k_fast_y_fwd<T, NQ, MINB><<<grid, Fast<T>::threads, smem, s>>>(a, static_cast<const T2*>(x));
     else
-        RTM_CUDA(launch_dependent(k_fast_y_inv<T, NQ>, grid, dim3(Fast<T>::threads), smem, s, a, static_cast<T2*>(y)));
+        RTM_CUDA(launch_dependent(k_fast_y_inv<T, NQ, MINB>, grid, dim3(Fast<T>::threads), smem, s, a,
+                                  static_cast<T2*>(y)));
     count_launch();
     return RTM_OK;
 }
 
-template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
+template <typename T, int NQ> int launch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd,
+                                           int minb, cudaStream_t s) {
+    if (minb <= 1) return launch_y_b<T, NQ, 1>(a, nrhs, x, y, fwd, s);
+    if constexpr (sizeof(T) == 8) {
+        if (minb >= 3) return launch_y_b<T, NQ, 3>(a, nrhs, x, y, fwd, s);
+    }
+    return launch_y_b<T, NQ, 2>(a, nrhs, x, y, fwd, s);
+}
+
+template <typename T, int NP> size_t x_direct_smem() {
+    constexpr int R1 = Shape<NP>::R1, R2 = Shape<NP>::R2, TEAMS = Fast<T>::threads / (4 * R2);
+    return (size_t)4 * TEAMS * R1 * (R2 + 1) * sizeof(typename Cx<T>::T2);
+}
+
+template <typename T, int NP, int MINB> int launch_x_direct(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
+    constexpr int TEAMS = Fast<T>::threads / (4 * Shape<NP>::R2);
+    const size_t smem = x_direct_smem<T, NP>();
+    static DeviceOnce once;
+    RTM_TRY(once([smem]() -> int {
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix_direct<T, NP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        return RTM_OK;
+    }));
+    const dim3 grid((a.Q + TEAMS - 1) / TEAMS, 2, nrhs);
+    RTM_CUDA(launch_dependent(k_fast_x_mix_direct<T, NP, MINB>, grid, dim3(Fast<T>::threads), smem, s, a));
+    count_launch();
+    return RTM_OK;
+}
+
+template <typename T, int NP> int launch_x_pipe(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
     using M = MixShape<T, NP>;
     static DeviceOnce once;
     static int per_sm[64] = {};
     int dev = 0;
     RTM_CUDA(cudaGetDevice(&dev));
     RTM_TRY(once([dev]() -> int {
-        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem));
+        RTM_CUDA(cudaFuncSetAttribute(k_fast_x_mix_pipe<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)M::smem));
         int blocks = 0, sms = 0;
-        RTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fast_x_mix<T, NP>, Fast<T>::threads, M::smem));
+        RTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fast_x_mix_pipe<T, NP>, Fast<T>::threads,
+                                                               M::smem));
         RTM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if (dev >= 0 && dev < 64) per_sm[dev] = std::max(1, blocks) * sms;
         return RTM_OK;
@@ -422,33 +554,43 @@ template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, cudaS
     const int iters = nrhs * 2 * (a.Q / M::TEAMS);
     const int resident = dev >= 0 && dev < 64 && per_sm[dev] > 0 ? per_sm[dev] : 148;
     const int grid = std::max(1, std::min(iters, resident));
-    RTM_CUDA(launch_dependent(k_fast_x_mix<T, NP>, dim3(grid), dim3(Fast<T>::threads), M::smem, s, a, iters));
+    RTM_CUDA(launch_dependent(k_fast_x_mix_pipe<T, NP>, dim3(grid), dim3(Fast<T>::threads), M::smem, s, a, iters));
     count_launch();
     return RTM_OK;
 }
 
-template <typename T> int dispatch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd, cudaStream_t s) {
+template <typename T, int NP> int launch_x(const GridArgs<T>& a, int nrhs, int kind, cudaStream_t s) {
+    if (kind == kMixPipelined) return launch_x_pipe<T, NP>(a, nrhs, s);
+    if (kind == kMixDirect2) return launch_x_direct<T, NP, 2>(a, nrhs, s);
+    if constexpr (sizeof(T) == 8) {
+        if (kind == kMixDirect3) return launch_x_direct<T, NP, 3>(a, nrhs, s);
+    }
+    return launch_x_direct<T, NP, 1>(a, nrhs, s);
+}
+
+template <typename T> int dispatch_y(const GridArgs<T>& a, int nrhs, const void* x, void* y, bool fwd, int minb,
+                                     cudaStream_t s) {
     switch (a.Q) {
-        case 32: return launch_y<T, 32>(a, nrhs, x, y, fwd, s);
-        case 64: return launch_y<T, 64>(a, nrhs, x, y, fwd, s);
-        case 128: return launch_y<T, 128>(a, nrhs, x, y, fwd, s);
-        case 256: return launch_y<T, 256>(a, nrhs, x, y, fwd, s);
-        case 512: return launch_y<T, 512>(a, nrhs, x, y, fwd, s);
+        case 32: return launch_y<T, 32>(a, nrhs, x, y, fwd, minb, s);
+        case 64: return launch_y<T, 64>(a, nrhs, x, y, fwd, minb, s);
+        case 128: return launch_y<T, 128>(a, nrhs, x, y, fwd, minb, s);
+        case 256: return launch_y<T, 256>(a, nrhs, x, y, fwd, minb, s);
+        case 512: return launch_y<T, 512>(a, nrhs, x, y, fwd, minb, s);
         default:
-            if constexpr (sizeof(T) == 4) return launch_y<T, 1024>(a, nrhs, x, y, fwd, s);
+            if constexpr (sizeof(T) == 4) return launch_y<T, 1024>(a, nrhs, x, y, fwd, minb, s);
             return fail(RTM_ERR_UNSUPPORTED, "transform size");
     }
 }
 
-template <typename T> int dispatch_x(const GridArgs<T>& a, int nrhs, cudaStream_t s) {
+template <typename T> int dispatch_x(const GridArgs<T>& a, int nrhs, int kind, cudaStream_t s) {
     switch (a.P) {
-        case 32: return launch_x<T, 32>(a, nrhs, s);
-        case 64: return launch_x<T, 64>(a, nrhs, s);
-        case 128: return launch_x<T, 128>(a, nrhs, s);
-        case 256: return launch_x<T, 256>(a, nrhs, s);
-        case 512: return launch_x<T, 512>(a, nrhs, s);
+        case 32: return launch_x<T, 32>(a, nrhs, kind, s);
+        case 64: return launch_x<T, 64>(a, nrhs, kind, s);
+        case 128: return launch_x<T, 128>(a, nrhs, kind, s);
+        case 256: return launch_x<T, 256>(a, nrhs, kind, s);
+        case 512: return launch_x<T, 512>(a, nrhs, kind, s);
         default:
-            if constexpr (sizeof(T) == 4) return launch_x<T, 1024>(a, nrhs, s);
+            if constexpr (sizeof(T) == 4) return launch_x<T, 1024>(a, nrhs, kind, s);
             return fail(RTM_ERR_UNSUPPORTED, "transform size");
     }
 }
@@ -460,16 +602,31 @@ bool fast_split_eligible(int P, int Q, bool fp64) {
     return ok(P) && ok(Q);
 }
 
+FastSchedule default_fast_schedule(int P, int Q, bool fp64) {
+    FastSchedule f;
+    // y passes: FP32 two CTAs of 256 threads an SM (128 registers, no spills up to lines of 1024); FP64
+    // three CTAs of 128 threads below lines of 512, two at 512 (up to 255 registers).
+    f.y_blocks = fp64 ? (Q >= 512 ? 2 : 3) : 2;
+    // x-mix: the pipelined form at FP32 1024 (one CTA of 256 threads an SM either way, and 100 MB of spectra
+    // that do not stay in L2 between products); elsewhere the direct form, which keeps more warps resident.
+    if (!fp64 && P >= 1024) f.x_kind = kMixPipelined;
+    else if (fp64) f.x_kind = P >= 512 ? kMixDirect1 : kMixDirect3;
+    else f.x_kind = kMixDirect2;
+    return f;
+}
+
 template <typename T>
-int launch_fast_split(const GridArgs<T>& a, int nrhs, const void* x, void* y, cudaStream_t s) {
-    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, true, s));
-    RTM_TRY(dispatch_x<T>(a, nrhs, s));
-    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, false, s));
+int launch_fast_split(const GridArgs<T>& a, int nrhs, const void* x, void* y, const FastSchedule& f, cudaStream_t s) {
+    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, true, f.y_blocks, s));
+    RTM_TRY(dispatch_x<T>(a, nrhs, f.x_kind, s));
+    RTM_TRY(dispatch_y<T>(a, nrhs, x, y, false, f.y_blocks, s));
     RTM_CUDA(cudaGetLastError());
     return RTM_OK;
 }
 
-template int launch_fast_split<float>(const GridArgs<float>&, int, const void*, void*, cudaStream_t);
-template int launch_fast_split<double>(const GridArgs<double>&, int, const void*, void*, cudaStream_t);
+template int launch_fast_split<float>(const GridArgs<float>&, int, const void*, void*, const FastSchedule&,
+                                      cudaStream_t);
+template int launch_fast_split<double>(const GridArgs<double>&, int, const void*, void*, const FastSchedule&,
+                                       cudaStream_t);
 
 }  // namespace rtm
