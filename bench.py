@@ -89,16 +89,25 @@ def batch_rhs(R, prob, dirs, pols):
     return out
 
 
-def solve_batch(R, w, b=None):
-    """One batched solve of the c4 workload: all right-hand sides in one preconditioned COCG solve."""
+def solve_batch(R, w, b=None, mixed=False):
+    """One batched solve of the c4 workload, all right-hand sides in one solve: FP64 COCG preconditioned by the
+    rChan circulant; or (mixed) FP32 flexible GMRES(50) with the FP32 product and FP32 block-Jacobi inside FP64
+    iterative refinement to the same FP64 true residual (FP32 COCG diverges on this plate)."""
     prob = build_plate(R, w)
     dirs, pols = random_waves(w["rhs"], np.random.default_rng(w["seed"]))
     op = R.Operator(prob, maxRhs=w["rhs"])
-    pc = R.Preconditioner(prob, kernel="rChan")
     if b is None:
         b = batch_rhs(R, prob, dirs, pols)
-    res = R.Solver(method=w["method"], tolerance=w["tol"], maxIterationCount=20000).solve(op, b, preconditioner=pc,
-                                                                                        nrhs=w["rhs"])
+    if mixed:
+        inner = R.Operator(prob, precision="single", maxRhs=w["rhs"])
+        pc = R.Preconditioner.blockJacobi(prob, (2, 2), precision="single")
+        res = R.Solver(method="fgmres", tolerance=w["tol"], restart=50, innerTolerance=INNER_FLOOR,
+                       maxIterationCount=20000).solve(op, b, innerOperator=inner, innerPreconditioner=pc,
+                                                      nrhs=w["rhs"])
+    else:
+        pc = R.Preconditioner(prob, kernel="rChan")
+        res = R.Solver(method=w["method"], tolerance=w["tol"], maxIterationCount=20000).solve(
+            op, b, preconditioner=pc, nrhs=w["rhs"])
     return prob, res
 
 
@@ -220,6 +229,23 @@ def run_batched(args, w):
     e2[1].record()
     torch.cuda.synchronize()
     t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
+    # the precision form of the batch: FP32 inner FGMRES(50) + block-Jacobi, FP64 refinement
+    mixed = {}
+    if not args.no_arms:
+        solve_batch(R, w, mixed=True)
+        torch.cuda.synchronize()
+        e3 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e3[0].record()
+        for _ in range(args.steps):
+            _, mres = solve_batch(R, w, mixed=True)
+        e3[1].record()
+        torch.cuda.synchronize()
+        t_mix = e3[0].elapsed_time(e3[1]) / 1e3
+        mixed = {"value": w["rhs"] * args.steps / t_mix, "unit": "solves/s", "ms_per_step": t_mix / args.steps * 1e3,
+                 "method": "FP32 flexible GMRES(50), FP32 product and block-Jacobi (2 x 2 faces), FP64 refinement",
+                 "inner_iterations": max(r.iterationCount() for r in mres),
+                 "true_residual": max(r.residualNorm() for r in mres),
+                 "all_converged_to_tolerance": all(r.converged() and r.residualNorm() <= w["tol"] for r in mres)}
     n, N = w["n"], prob.rooftopCount()
     line = {
         "metric": "batched solves/s (right-hand sides) at rel. residual 1e-6, rChan-preconditioned COCG, FP64",
@@ -235,6 +261,9 @@ def run_batched(args, w):
                 "d2h_bytes_per_step": 16 * N * w["rhs"]},
         "gpu_launches": int(L.launch_count() - launches0), "clocks": clk.summary(),
     }
+    if mixed:
+        line["mixed"] = mixed
+        line["mixed_over_fp64"] = mixed["value"] / line["value"]
     print(json.dumps(line))
 
 
@@ -692,6 +721,8 @@ def main():
                     help="with --impl reference: one whole oracle solve of the workload (its iteration count)")
     ap.add_argument("--once", action="store_true",
                     help="one untimed solve of the workload, no JSON line (the command profiler captures run)")
+    ap.add_argument("--arm", choices=["fp64", "mixed", "fp64_batched", "mixed_batched"],
+                    help="with --once: one step of that arm of the workload's plate instead")
     ap.add_argument("--matvec", action="store_true",
                     help="only the product of the workload, applied --steps times (the command profiler captures run)")
     ap.add_argument("--assembly", action="store_true",
@@ -758,6 +789,15 @@ def main():
               f"{rf['bytes'] / rf['seconds'] / 1e9:.0f} GB/s")
         return
     if args.once:
+        if args.arm:
+            # one step of an arm of the workload's plate (the profiler captures run)
+            count = BATCH_RHS if args.arm.endswith("batched") else 1
+            d, p = batch_waves(w, count)
+            _, res, rcs = solve_arm(R, w, args.arm.startswith("mixed"), d, p)
+            torch.cuda.synchronize()
+            print(f"{args.arm}: {count} right-hand sides, iterations {max(r.iterationCount() for r in res)}, "
+                  f"residual {max(r.residualNorm() for r in res):.3e}")
+            return
         _, _, res, rcs = solve_plate(R, w)
         torch.cuda.synchronize()
         print(f"iterations {res.iterationCount()} residual {res.residualNorm():.3e} rcs {rcs:.6g}")

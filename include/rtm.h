@@ -279,11 +279,19 @@ RTM_API int rtm_input_impedance(int count_x, int count_y, double size_x, double 
  * depend on what else runs: every kernel's launch shape follows from the request alone. */
 typedef struct rtm_server rtm_server;
 
+typedef enum rtm_transform_sizes {
+    RTM_SIZES_REFERENCE = 0,    /* the reference's 7-smooth transform sizes (generateFastFFTSize.m) */
+    RTM_SIZES_POWER_OF_TWO = 1, /* plates: the next powers of two where the power-of-two kernels take them */
+    RTM_SIZES_AUTOTUNE = 2      /* plates: rtm_tune_product on the first request of each face grid */
+} rtm_transform_sizes;
+
 typedef struct rtm_server_config {
     double budget_bytes;   /* device bytes the admitted requests may hold together (<= 0: 150e9) */
     int max_active;        /* requests admitted at once, one worker thread each (<= 0: 8) */
     int precision;         /* RTM_FP64, or RTM_FP32 for the mixed form (FP32 inner FGMRES, FP64 refinement) */
     int device;            /* CUDA device of the workers */
+    int transform_sizes;   /* rtm_transform_sizes of the requests' split products (any size at least the face
+                              count gives the same product up to rounding) */
 } rtm_server_config;
 
 typedef enum rtm_excitation { RTM_EXCITE_PLANE_WAVE = 0, RTM_EXCITE_DELTA_GAP = 1 } rtm_excitation;

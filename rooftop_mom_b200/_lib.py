@@ -64,10 +64,12 @@ class TuneResult(C.Structure):
 TUNE_FLUSH_L2 = 1
 TUNE_REFERENCE_SIZES = 2
 TUNE_VERBOSE = 4
+TRANSFORM_SIZES = {"reference": 0, "powerOfTwo": 1, "autotune": 2}
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("budget_bytes", C.c_double), ("max_active", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+    _fields_ = [("budget_bytes", C.c_double), ("max_active", C.c_int), ("precision", C.c_int), ("device", C.c_int),
+                ("transform_sizes", C.c_int)]
 
 
 class Request(C.Structure):

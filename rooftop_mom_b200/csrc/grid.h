@@ -88,6 +88,9 @@ int build_product(const DeviceGenerators& g, double size_x, double size_y, int p
 // The autotuner's measured choice for a face grid and precision on the current device (tune.cpp): false
 // when none was measured.
 bool tuned_choice(int count_x, int count_y, int precision, int* P, int* Q, FastSchedule* sched);
+// Records a transform grid for a face grid and precision as if the autotuner had chosen it (schedule by
+// default_fast_schedule).
+void register_choice(int count_x, int count_y, int precision, int P, int Q);
 
 // Builds the inverted circulant preconditioner on the face grid (generateCirculant.m:16-25).
 int build_circulant(const DeviceGenerators& g, double size_x, double size_y, int kernel, int builder,

@@ -548,7 +548,29 @@ template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
 constexpr int kStreamCols = 64;
 constexpr int kStreamRows = 3072;  // rows per CTA chunk the launcher aims at (bounds the shared w chunk)
 
-template <typename T2>
+// RL consecutive rows of one basis column, read with one load where RL = 2 (two FP32 complex values in 16
+// bytes): FP32 threads then keep as many bytes in flight as FP64 ones, which the passes' throughput
+// follows (they are bound by the memory requests in flight, not by arithmetic).
+template <typename T2, int RL> struct RowPack {
+    T2 v[RL];
+};
+template <typename T2, int RL>
+__device__ __forceinline__ RowPack<T2, RL> load_rows(const T2* __restrict__ p, int valid) {
+    RowPack<T2, RL> r;
+    if constexpr (RL == 2) {
+        if (valid == 2) {
+            const float4 f = *reinterpret_cast<const float4*>(p);
+            r.v[0] = make_float2(f.x, f.y);
+            r.v[1] = make_float2(f.z, f.w);
+            return r;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < RL; ++q) r.v[q] = q < valid ? p[q] : from_d2<T2>(make_double2(0, 0));
+    return r;
+}
+
+template <typename T2, int RL>
 __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict__ V, T2* __restrict__ w, int64_t n,
                                                            int nrhs, GmState* st, GmArrays ar, int mode, int chunk) {
     constexpr int NW = kRT / 32, KQ = kStreamCols / NW;
@@ -572,51 +594,67 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
     double nrm = 0;
     __syncthreads();  // coef
     if (mode) {
-        // two rows a thread at once (r and r + kRT): twice the loads in flight per batch of columns
-        for (int r = threadIdx.x; r < len; r += 2 * kRT) {
-            const int r2 = r + kRT;
-            const bool two = r2 < len;
-            double2 v = to_d2(wr[r]);
-            double2 v2 = two ? to_d2(wr[r2]) : make_double2(0, 0);
+        // two groups of RL rows a thread at once (r and r + RL kRT): twice the loads in flight per batch
+        // of columns; every row takes its columns in order, as in k_gm_orth
+        for (int r = RL * threadIdx.x; r < len; r += 2 * RL * kRT) {
+            const int r2 = r + RL * kRT;
+            const int n0 = min(RL, len - r), n1 = max(0, min(RL, len - r2));
+            double2 v[RL], v2[RL];
+#pragma unroll
+            for (int q = 0; q < RL; ++q) {
+                v[q] = q < n0 ? to_d2(wr[r + q]) : make_double2(0, 0);
+                v2[q] = q < n1 ? to_d2(wr[r2 + q]) : make_double2(0, 0);
+            }
+            constexpr int UB = 8 / RL;  // columns a batch: the same bytes in flight for every RL
             int k = 0;
-            for (; k + 8 <= cols; k += 8) {
-                T2 t[8], t2[8];
+            for (; k + UB <= cols; k += UB) {
+                RowPack<T2, RL> t[UB], t2[UB];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    t[u] = Vr[(k + u) * col + r];
-                    t2[u] = two ? Vr[(k + u) * col + r2] : from_d2<T2>(make_double2(0, 0));
+                for (int u = 0; u < UB; ++u) {
+                    t[u] = load_rows<T2, RL>(Vr + (k + u) * col + r, n0);
+                    t2[u] = load_rows<T2, RL>(Vr + (k + u) * col + r2, n1);
                 }
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const double2 p = dmul(to_d2(t[u]), coef[k + u]);
-                    v.x -= p.x;
-                    v.y -= p.y;
-                    const double2 p2 = dmul(to_d2(t2[u]), coef[k + u]);
-                    v2.x -= p2.x;
-                    v2.y -= p2.y;
-                }
+                for (int u = 0; u < UB; ++u)
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) {
+                        const double2 p = dmul(to_d2(t[u].v[q]), coef[k + u]);
+                        v[q].x -= p.x;
+                        v[q].y -= p.y;
+                        const double2 p2 = dmul(to_d2(t2[u].v[q]), coef[k + u]);
+                        v2[q].x -= p2.x;
+                        v2[q].y -= p2.y;
+                    }
             }
             for (; k < cols; ++k) {
-                const double2 p = dmul(to_d2(Vr[k * col + r]), coef[k]);
-                v.x -= p.x;
-                v.y -= p.y;
-                if (two) {
-                    const double2 p2 = dmul(to_d2(Vr[k * col + r2]), coef[k]);
-                    v2.x -= p2.x;
-                    v2.y -= p2.y;
+                const RowPack<T2, RL> t = load_rows<T2, RL>(Vr + k * col + r, n0);
+                const RowPack<T2, RL> t2 = load_rows<T2, RL>(Vr + k * col + r2, n1);
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    const double2 p = dmul(to_d2(t.v[q]), coef[k]);
+                    v[q].x -= p.x;
+                    v[q].y -= p.y;
+                    const double2 p2 = dmul(to_d2(t2.v[q]), coef[k]);
+                    v2[q].x -= p2.x;
+                    v2[q].y -= p2.y;
                 }
             }
-            const T2 vs = from_d2<T2>(v);
-            wr[r] = vs;
-            if (mode == 1) ws[r] = vs;
-            const double2 vd = to_d2(vs);
-            nrm += vd.x * vd.x + vd.y * vd.y;
-            if (two) {
-                const T2 vs2 = from_d2<T2>(v2);
-                wr[r2] = vs2;
-                if (mode == 1) ws[r2] = vs2;
-                const double2 vd2 = to_d2(vs2);
-                nrm += vd2.x * vd2.x + vd2.y * vd2.y;
+#pragma unroll
+            for (int q = 0; q < RL; ++q) {
+                if (q < n0) {
+                    const T2 vs = from_d2<T2>(v[q]);
+                    wr[r + q] = vs;
+                    if (mode == 1) ws[r + q] = vs;
+                    const double2 vd = to_d2(vs);
+                    nrm += vd.x * vd.x + vd.y * vd.y;
+                }
+                if (q < n1) {
+                    const T2 vs2 = from_d2<T2>(v2[q]);
+                    wr[r2 + q] = vs2;
+                    if (mode == 1) ws[r2 + q] = vs2;
+                    const double2 vd2 = to_d2(vs2);
+                    nrm += vd2.x * vd2.x + vd2.y * vd2.y;
+                }
             }
         }
     } else {
@@ -633,24 +671,48 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
         if (wide || warp < G * cols) {
             const int kw = wide ? warp : warp % cols;
             const int slice = wide ? 0 : warp / cols;
-            const int rs = (int)((int64_t)len * slice / G), re = (int)((int64_t)len * (slice + 1) / G);
-            // two rows a lane per step: up to 2 KQ loads in flight
-            for (int r = rs + lane; r < re; r += 64) {
-                const bool second = r + 32 < re;
-                T2 t[KQ], u[KQ];
+            // slices start on multiples of RL (the packed loads' alignment)
+            const int rs = (int)((int64_t)len * slice / G) / RL * RL;
+            const int re = slice + 1 == G ? len : (int)((int64_t)len * (slice + 1) / G) / RL * RL;
+            // two groups of RL rows a lane per step: up to 2 KQ loads in flight
+            for (int r = rs + RL * lane; r < re; r += 64 * RL) {
+                const int r2 = r + 32 * RL;
+                const int n0 = min(RL, re - r), n1 = max(0, min(RL, re - r2));
+                RowPack<T2, RL> t[KQ], u[KQ];
 #pragma unroll
                 for (int q = 0; q < KQ; ++q) {
                     const int k = kw + NW * q;
                     const bool use = (wide || q == 0) && k < cols;
-                    t[q] = use ? Vr[k * col + r] : from_d2<T2>(make_double2(0, 0));
-                    u[q] = (use && second) ? Vr[k * col + r + 32] : from_d2<T2>(make_double2(0, 0));
+                    t[q] = load_rows<T2, RL>(Vr + k * col + r, use ? n0 : 0);
+                    u[q] = load_rows<T2, RL>(Vr + k * col + r2, use ? n1 : 0);
                 }
-                const double2 x = to_d2(ws[r]);
-                const double2 x2 = second ? to_d2(ws[r + 32]) : make_double2(0, 0);
+                T2 x[RL], x2[RL];  // kept in the stored precision until used (registers)
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    x[q] = q < n0 ? ws[r + q] : from_d2<T2>(make_double2(0, 0));
+                    x2[q] = q < n1 ? ws[r2 + q] : from_d2<T2>(make_double2(0, 0));
+                }
 #pragma unroll
                 for (int q = 0; q < KQ; ++q) {
-                    acc[q] = dadd(acc[q], dmulc(to_d2(t[q]), x));
-                    acc[q] = dadd(acc[q], dmulc(to_d2(u[q]), x2));
+                    if constexpr (RL == 2) {
+                        // FP32 basis: the 4 products of a step summed in FP32 (a lane sums a few tens of
+                        // products a chunk), added to the FP64 partial
+                        float2 f = make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int e = 0; e < RL; ++e) {
+                            const float2 a = t[q].v[e], b = x[e], c = u[q].v[e], d = x2[e];
+                            f.x += a.x * b.x + a.y * b.y + c.x * d.x + c.y * d.y;
+                            f.y += a.x * b.y - a.y * b.x + c.x * d.y - c.y * d.x;
+                        }
+                        acc[q].x += f.x;
+                        acc[q].y += f.y;
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < RL; ++e) {
+                            acc[q] = dadd(acc[q], dmulc(to_d2(t[q].v[e]), to_d2(x[e])));
+                            acc[q] = dadd(acc[q], dmulc(to_d2(u[q].v[e]), to_d2(x2[e])));
+                        }
+                    }
                 }
             }
         }
@@ -736,8 +798,13 @@ template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, in
     if (ar.m + 1 <= kStreamCols) {
         int blocks, chunk;
         stream_config(n, &blocks, &chunk);
-        k_gm_orth_stream<T2><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar, mode,
-                                                                                        chunk);
+        // FP32 reads two rows a load where every column starts on 16 bytes (an even length)
+        if (sizeof(T2) == 8 && n % 2 == 0)
+            k_gm_orth_stream<T2, (sizeof(T2) == 8 ? 2 : 1)><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(
+                V, w, n, nrhs, st, ar, mode, chunk);
+        else
+            k_gm_orth_stream<T2, 1><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar,
+                                                                                               mode, chunk);
         count_launch();
         return;
     }
@@ -1186,7 +1253,10 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     {
         int sb, sc;
         stream_config(n, &sb, &sc);
-        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      std::max<int>(sc * (int)sizeof(T2), 48 * 1024)));
+        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, (sizeof(T2) == 8 ? 2 : 1)>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       std::max<int>(sc * (int)sizeof(T2), 48 * 1024)));
     }
     RTM_CUDA(cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

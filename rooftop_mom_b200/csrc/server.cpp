@@ -24,6 +24,7 @@
 #include <thread>
 #include <vector>
 
+#include "grid.h"
 #include "handles.h"
 #include "krylov.h"
 
@@ -78,12 +79,28 @@ int check_request(const rtm_request& q) {
     return RTM_OK;
 }
 
+int next_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
 // Device bytes of a request's pipeline (generators, product spectra and working grids, preconditioner,
-// solver vectors, excitation and solution), in the server's precision.
-int request_bytes(const rtm_request& q, int precision, double* bytes) {
+// solver vectors, excitation and solution), in the server's precision. Under a power-of-two or autotuned
+// size policy a plate's product is counted at the power-of-two grid where the power-of-two kernels take it
+// (the larger of the candidates).
+int request_bytes(const rtm_request& q, int precision, int sizes, double* bytes) {
     double est[6];
     RTM_TRY(rtm_estimate_bytes(q.count_x, q.count_y, RTM_PRODUCT_SPLIT, q.method, q.preconditioner != 0, q.restart,
                                q.max_iterations, est));
+    if (sizes != RTM_SIZES_REFERENCE && q.count_x > 1 && q.count_y > 1) {
+        const int P = next_pow2(q.count_x), Q = next_pow2(q.count_y);
+        if (fast_split_eligible(P, Q, precision == RTM_FP64)) {
+            const double grow = (double)P * Q / ((double)fast_fft_size(q.count_x) * fast_fft_size(q.count_y));
+            est[1] *= grow;
+            est[2] *= grow;
+        }
+    }
     const double n = (double)(q.count_x - 1) * q.count_y + (double)q.count_x * (q.count_y - 1);
     const double blocks = (double)((q.count_x + 1) / 2) * ((q.count_y + 1) / 2);
     double pc = 0;
@@ -173,6 +190,22 @@ struct rtm_server {
         }
     }
 
+    // The transform grid of a plate's split products under the server's policy (strips keep the
+    // reference's sizes). Choices are per device and face grid, shared by all requests of that grid.
+    int choose_sizes(int cx, int cy, int precision) {
+        if (cfg.transform_sizes == RTM_SIZES_REFERENCE || cx < 2 || cy < 2) return RTM_OK;
+        int P = 0, Q = 0;
+        FastSchedule f;
+        if (tuned_choice(cx, cy, precision, &P, &Q, &f)) return RTM_OK;
+        if (cfg.transform_sizes == RTM_SIZES_AUTOTUNE) {
+            rtm_tune_result r{};
+            return rtm_tune_product(cx, cy, precision, 1, RTM_TUNE_FLUSH_L2, &r);
+        }
+        if (fast_split_eligible(next_pow2(cx), next_pow2(cy), precision == RTM_FP64))
+            register_choice(cx, cy, precision, next_pow2(cx), next_pow2(cy));
+        return RTM_OK;
+    }
+
     // The whole pipeline of one request on this thread. Its results go to `out`, which the worker
     // copies into the record under the lock, so a concurrent poll never sees them half written.
     int run(const Record& r, Outcome& out) {
@@ -190,6 +223,8 @@ struct rtm_server {
             }
         } h;
         const bool mixed = cfg.precision == RTM_FP32;
+        RTM_TRY(choose_sizes(q.count_x, q.count_y, RTM_FP64));
+        if (mixed) RTM_TRY(choose_sizes(q.count_x, q.count_y, RTM_FP32));
         RTM_TRY(rtm_generators_assemble(q.count_x, q.count_y, q.size_x, q.size_y, q.wavenumber, 16, 8, nullptr, &h.g));
         RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP64, 1, &h.op));
         if (mixed) RTM_TRY(rtm_operator_create(h.g, q.size_x, q.size_y, RTM_PRODUCT_SPLIT, RTM_FP32, 1, &h.op32));
@@ -275,6 +310,8 @@ int rtm_server_create(const rtm_server_config* config, rtm_server** out) {
     if (srv->cfg.precision != RTM_FP64 && srv->cfg.precision != RTM_FP32)
         return fail(RTM_ERR_ARG, "precision must be RTM_FP64 or RTM_FP32");
     if (srv->cfg.max_active > 256) return fail(RTM_ERR_ARG, "at most 256 active requests");
+    if (srv->cfg.transform_sizes < RTM_SIZES_REFERENCE || srv->cfg.transform_sizes > RTM_SIZES_AUTOTUNE)
+        return fail(RTM_ERR_ARG, "unknown transform size policy");
     srv->epoch = Clock::now();
     rtm_server* p = srv.get();
     for (int i = 0; i < srv->cfg.max_active; ++i) srv->workers.emplace_back([p] { p->worker(); });
@@ -287,7 +324,7 @@ int rtm_server_submit(rtm_server* srv, const rtm_request* request, uint64_t* id)
     RTM_TRY(check_request(*request));
     auto rec = std::make_unique<Record>();
     rec->req = *request;
-    RTM_TRY(request_bytes(*request, srv->cfg.precision, &rec->res.bytes));
+    RTM_TRY(request_bytes(*request, srv->cfg.precision, srv->cfg.transform_sizes, &rec->res.bytes));
     std::lock_guard<std::mutex> lk(srv->mu);
     if (srv->stopping) return fail(RTM_ERR_ARG, "the server is stopping");
     rec->id = srv->next_id++;

@@ -94,6 +94,17 @@ bool tuned_choice(int count_x, int count_y, int precision, int* P, int* Q, FastS
     return true;
 }
 
+void register_choice(int count_x, int count_y, int precision, int P, int Q) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    TuneChoice c;
+    c.P = P;
+    c.Q = Q;
+    c.sched = default_fast_schedule(P, Q, precision == RTM_FP64);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[{dev, precision, count_x, count_y}] = c;
+}
+
 }  // namespace rtm
 
 using namespace rtm;

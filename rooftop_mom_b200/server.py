@@ -79,8 +79,15 @@ def _result_dict(res: L.RequestResult):
 class Server:
     """rtm_server: admission by byte budget, maxActive requests on the device at once."""
 
-    def __init__(self, budgetBytes=150e9, maxActive=8, precision="double", device=0):
-        cfg = L.ServerConfig(float(budgetBytes), int(maxActive), L.PRECISIONS[precision], int(device))
+    def __init__(self, budgetBytes=150e9, maxActive=8, precision="double", device=0, transformSizes="reference"):
+        """transformSizes: "reference" (generateFastFFTSize.m's 7-smooth sizes), "powerOfTwo" (plates: the next
+        powers of two where the power-of-two kernels take them) or "autotune" (plates: rtm_tune_product on the
+        first request of each face grid)."""
+        if transformSizes not in L.TRANSFORM_SIZES:
+            raise L.RtmError(L.ERR_ARG, "transformSizes is 'reference', 'powerOfTwo' or 'autotune'.",
+                             "rooftopMoM:gpu:invalidArgument")
+        cfg = L.ServerConfig(float(budgetBytes), int(maxActive), L.PRECISIONS[precision], int(device),
+                             L.TRANSFORM_SIZES[transformSizes])
         h = C.c_void_p()
         L.call("rtm_server_create", C.byref(cfg), C.byref(h))
         self._h = h

@@ -140,3 +140,24 @@ def test_a_circulant_request_equals_the_direct_cocg_solve():
     assert served["state"] == "done" and served["converged"]
     assert served["iterations"] == res.iterationCount()
     assert _rel(served["current"], res.solution()) < 1e-12
+
+
+@pytest.mark.parametrize("policy", ["powerOfTwo", "autotune"])
+def test_transform_size_policies_give_the_reference_sizes_results(policy):
+    """A server whose plates take power-of-two or autotuned transform grids (a larger grid gives the same
+    product up to rounding) returns the currents of the reference-size server within the solve tolerance,
+    for plates whose face counts are not powers of two, and strips unchanged."""
+    import rooftop_mom_b200 as R
+
+    reqs = [_plate(37, 30), _plate(45, 23, method="cg"), _strip(41)]
+    with R.Server(budgetBytes=50e9, maxActive=3) as ref_srv:
+        ref = [ref_srv.wait(ref_srv.submit(q), release=True) for q in reqs]
+    R.clearTuning()
+    try:
+        with R.Server(budgetBytes=50e9, maxActive=3, transformSizes=policy) as srv:
+            got = [srv.wait(srv.submit(q), release=True) for q in reqs]
+    finally:
+        R.clearTuning()
+    for a, b in zip(got, ref):
+        assert a["state"] == "done" and a["converged"]
+        assert _rel(a["current"], b["current"]) < 1e-6

@@ -155,3 +155,17 @@ def test_cancelled_admitted_requests_release_their_bytes_under_concurrent_polls(
         # every released byte is back: four requests' worth fits again
         big = [srv.submit(_request()) for _ in range(4)]
         assert all(srv.poll(rid, wait=60.0)["state"] in ("failed", "cancelled") for rid in big)
+
+
+def test_an_unknown_transform_size_policy_is_rejected():
+    import ctypes as C
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    with pytest.raises(L.RtmError):
+        R.Server(transformSizes="primes")
+    cfg = L.ServerConfig(1e9, 1, 0, 0, 5)
+    h = C.c_void_p()
+    with pytest.raises(L.RtmError):
+        L.call("rtm_server_create", C.byref(cfg), C.byref(h))
