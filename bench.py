@@ -137,56 +137,68 @@ def serving_requests(R, count, seed):
     return out
 
 
-def run_serving(args):
-    """c5: a closed-loop burst measures capacity; then the stream arrives as a Poisson process at 0.8 x
-    capacity; per-request latency (submission to result) gives p50 / p99."""
+def serve_stream(R, count, slots, precision, sizes, seed=0):
+    """The c5 stream on a server: a closed-loop burst measures capacity (a tenth of the stream, at least four
+    requests a slot), then the stream arrives as a Poisson process at 0.8 x capacity; per-request latency
+    (submission to result) gives p50 / p99. precision "double" (FP64) or "mixed" (FP32 inner solves, FP64
+    refinement); sizes: the servers' transform-size policy."""
     import torch
 
-    import rooftop_mom_b200 as R
-
-    R.load()
-    reqs = serving_requests(R, args.requests, 0)
-    prec = "single" if args.serving_precision == "mixed" else "double"
-    with R.Server(budgetBytes=150e9, maxActive=args.slots, precision=prec) as srv:
-        warm = serving_requests(R, 4, 1)
+    reqs = serving_requests(R, count, seed)
+    prec = "single" if precision == "mixed" else "double"
+    with R.Server(budgetBytes=150e9, maxActive=slots, precision=prec, transformSizes=sizes) as srv:
+        warm = serving_requests(R, 4, seed + 1)
         for r in [srv.submit(q) for q in warm]:
             srv.wait(r, release=True)
-        # capacity from a closed-loop burst of a tenth of the stream (at least four requests a slot)
-        burst = reqs[: min(len(reqs), max(args.slots * 4, len(reqs) // 10))]
+        burst = reqs[: min(len(reqs), max(slots * 4, len(reqs) // 10))]
         ids = [srv.submit(q) for q in burst]
         res = [srv.wait(r, release=True) for r in ids]
         span = max(x["finished"] for x in res) - min(x["submitted"] for x in res)
         capacity = len(burst) / span
         rate = 0.8 * capacity
-        rng = np.random.default_rng(2)
+        rng = np.random.default_rng(seed + 2)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
         torch.cuda.synchronize()
-        with Clocks(0) as clk:
-            t0 = time.perf_counter()
-            ids = []
-            for q, ta in zip(reqs, arrivals):
-                dt = ta - (time.perf_counter() - t0)
-                if dt > 0:
-                    time.sleep(dt)
-                ids.append(srv.submit(q))
-            res = [srv.wait(r, release=True) for r in ids]
+        t0 = time.perf_counter()
+        ids = []
+        for q, ta in zip(reqs, arrivals):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(q))
+        res = [srv.wait(r, release=True) for r in ids]
     done = [x for x in res if x["state"] == "done"]
     lat = np.array([x["latency"] for x in done])
     span = max(x["finished"] for x in res) - min(x["submitted"] for x in res)
     ok = [x for x in done if x["converged"] and x["residual"] <= 1e-6]
+    return {"value": len(ok) / span, "unit": "solves/s", "requests": len(reqs), "slots": slots,
+            "precision": precision, "transform_sizes": sizes, "capacity_solves_per_s": capacity,
+            "arrival_rate": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "converged": len(ok), "failed": len(res) - len(done),
+            "max_unknowns": int(max(x["unknowns"] for x in res)), "span_s": span}
+
+
+def run_serving(args):
+    """c5: the request stream on one server (serve_stream), one JSON line."""
+    import rooftop_mom_b200 as R
+
+    R.load()
+    with Clocks(0) as clk:
+        out = serve_stream(R, args.requests, args.slots, args.serving_precision, args.serving_sizes)
+    prec = "single" if args.serving_precision == "mixed" else "double"
     line = {
         "metric": "serving: solves/s and p50/p99 latency of a Poisson request stream at 0.8 x measured capacity",
-        "value": len(ok) / span, "unit": "solves/s", "n_gpus": 1, "steps": len(reqs), "warmup": len(warm),
-        "ms_per_step": span / len(reqs) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c128" if prec == "double" else "c64/c128", "data": "synthetic request stream, seed 0",
-        "config": {"workload": f"c5: {len(reqs)} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
+        "value": out["value"], "unit": "solves/s", "n_gpus": 1, "steps": out["requests"], "warmup": 4,
+        "ms_per_step": out["span_s"] / out["requests"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128" if prec == "double" else "c64/c128",
+        "data": "synthetic request stream, seed 0",
+        "config": {"workload": f"c5: {out['requests']} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
                                f"cell lambda/U[10,25], f U[0.5,3] GHz, COCG + rChan to 1e-6, "
-                               f"{args.serving_precision}", "slots": args.slots, "budget_bytes": 150e9,
-                   "capacity_solves_per_s": capacity, "arrival_rate": rate},
-        "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-        "converged": len(ok), "failed": len(res) - len(done),
-        "max_unknowns": int(max(x["unknowns"] for x in res)),
-        "clocks": clk.summary(),
+                               f"{args.serving_precision}, {args.serving_sizes} transform sizes",
+                   "slots": args.slots, "budget_bytes": 150e9, "capacity_solves_per_s": out["capacity_solves_per_s"],
+                   "arrival_rate": out["arrival_rate"]},
+        "p50_ms": out["p50_ms"], "p99_ms": out["p99_ms"], "converged": out["converged"], "failed": out["failed"],
+        "max_unknowns": out["max_unknowns"], "clocks": clk.summary(),
     }
     print(json.dumps(line))
 
@@ -730,6 +742,10 @@ def main():
     ap.add_argument("--requests", type=int, default=100, help="c5: requests in the stream (2000 in the full form)")
     ap.add_argument("--slots", type=int, default=8, help="c5: requests on the device at once")
     ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
+    ap.add_argument("--serving-sizes", default="powerOfTwo", choices=["reference", "powerOfTwo", "autotune"],
+                    help="c5: the server's transform-size policy")
+    ap.add_argument("--serving-requests", type=int, default=32,
+                    help="c2: requests of the short serving stream in the default line (0: none)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.workload in ("c4", "c5") and not args.matvec:
@@ -903,6 +919,10 @@ def main():
                                 "sample": sample, "matvec_ms": mv_ms}
     if rank == 0 and world == 1 and w["precision"] == "mixed":
         line["error_vs_fp64"] = precision_error(R, w)
+    if args.workload == "c2" and args.serving_requests > 0 and world == 1:
+        # the metric's p50 / p99: a short serving stream (c5's mix), FP64 and mixed
+        line["serving"] = {p: serve_stream(R, args.serving_requests, args.slots, p, args.serving_sizes)
+                           for p in ("double", "mixed")}
     if args.workload == "c2" and not args.no_arms:
         # the metric's "mixed vs FP64": both precisions, single and batched, on the same plate
         arms = precision_arms(R, w, min(args.steps, 5), min(args.warmup, 2))

@@ -548,6 +548,20 @@ template <typename T2> static void orth_config(int m, int* TR, size_t* smem) {
 constexpr int kStreamCols = 64;
 constexpr int kStreamRows = 3072;  // rows per CTA chunk the launcher aims at (bounds the shared w chunk)
 
+// Arithmetic type of the Gram-Schmidt passes: a basis kept in FP32 (the precision form's inner solves) is
+// updated and multiplied in FP32, with the sums over lanes, CTAs and chunks in FP64; an FP64 basis in FP64.
+// (Converting every FP32 element to FP64 made the FP32 passes slower than the FP64 ones.)
+template <typename T2> struct OrthAcc { using type = double2; };
+template <> struct OrthAcc<float2> { using type = float2; };
+__device__ __forceinline__ double2 amul(double2 a, double2 b) { return dmul(a, b); }
+__device__ __forceinline__ float2 amul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 amulc(double2 a, double2 b) { return dmulc(a, b); }
+__device__ __forceinline__ float2 amulc(float2 a, float2 b) {  // conj(a) * b
+    return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
 // RL consecutive rows of one basis column, read with one load where RL = 2 (two FP32 complex values in 16
 // bytes): FP32 threads then keep as many bytes in flight as FP64 ones, which the passes' throughput
 // follows (they are bound by the memory requests in flight, not by arithmetic).
@@ -574,8 +588,9 @@ template <typename T2, int RL>
 __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict__ V, T2* __restrict__ w, int64_t n,
                                                            int nrhs, GmState* st, GmArrays ar, int mode, int chunk) {
     constexpr int NW = kRT / 32, KQ = kStreamCols / NW;
+    using A2 = typename OrthAcc<T2>::type;  // arithmetic of the passes: FP64 for an FP64 basis, FP32 for FP32
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double2 coef[kStreamCols];
+    __shared__ A2 coef[kStreamCols];
     __shared__ double2 red[NW][KQ];
     T2* ws = reinterpret_cast<T2*>(smem_raw);  // [chunk]
     const int rhs = blockIdx.y;
@@ -586,7 +601,7 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
     const int64_t c0 = (int64_t)blockIdx.x * chunk < n ? (int64_t)blockIdx.x * chunk : n;
     const int len = (int)(n - c0 < (int64_t)chunk ? n - c0 : (int64_t)chunk);
     const double2* cf = mode == 1 ? ar.h + (int64_t)rhs * mc : ar.c + (int64_t)rhs * mc;
-    for (int k = threadIdx.x; k < cols; k += kRT) coef[k] = mode ? cf[k] : make_double2(0, 0);
+    for (int k = threadIdx.x; k < cols; k += kRT) coef[k] = from_d2<A2>(mode ? cf[k] : make_double2(0, 0));
     T2* wr = w + (int64_t)rhs * n + c0;
     const T2* Vr = V + (int64_t)rhs * n + c0;        // column k at Vr + k * col
     const int64_t col = (int64_t)nrhs * n;
@@ -599,11 +614,11 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
         for (int r = RL * threadIdx.x; r < len; r += 2 * RL * kRT) {
             const int r2 = r + RL * kRT;
             const int n0 = min(RL, len - r), n1 = max(0, min(RL, len - r2));
-            double2 v[RL], v2[RL];
+            A2 v[RL], v2[RL];
 #pragma unroll
             for (int q = 0; q < RL; ++q) {
-                v[q] = q < n0 ? to_d2(wr[r + q]) : make_double2(0, 0);
-                v2[q] = q < n1 ? to_d2(wr[r2 + q]) : make_double2(0, 0);
+                v[q] = q < n0 ? wr[r + q] : from_d2<A2>(make_double2(0, 0));
+                v2[q] = q < n1 ? wr[r2 + q] : from_d2<A2>(make_double2(0, 0));
             }
             constexpr int UB = 8 / RL;  // columns a batch: the same bytes in flight for every RL
             int k = 0;
@@ -618,10 +633,10 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
                 for (int u = 0; u < UB; ++u)
 #pragma unroll
                     for (int q = 0; q < RL; ++q) {
-                        const double2 p = dmul(to_d2(t[u].v[q]), coef[k + u]);
+                        const A2 p = amul(t[u].v[q], coef[k + u]);
                         v[q].x -= p.x;
                         v[q].y -= p.y;
-                        const double2 p2 = dmul(to_d2(t2[u].v[q]), coef[k + u]);
+                        const A2 p2 = amul(t2[u].v[q], coef[k + u]);
                         v2[q].x -= p2.x;
                         v2[q].y -= p2.y;
                     }
@@ -631,10 +646,10 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
                 const RowPack<T2, RL> t2 = load_rows<T2, RL>(Vr + k * col + r2, n1);
 #pragma unroll
                 for (int q = 0; q < RL; ++q) {
-                    const double2 p = dmul(to_d2(t.v[q]), coef[k]);
+                    const A2 p = amul(t.v[q], coef[k]);
                     v[q].x -= p.x;
                     v[q].y -= p.y;
-                    const double2 p2 = dmul(to_d2(t2.v[q]), coef[k]);
+                    const A2 p2 = amul(t2.v[q], coef[k]);
                     v2[q].x -= p2.x;
                     v2[q].y -= p2.y;
                 }
@@ -642,14 +657,14 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
 #pragma unroll
             for (int q = 0; q < RL; ++q) {
                 if (q < n0) {
-                    const T2 vs = from_d2<T2>(v[q]);
+                    const T2 vs = v[q];
                     wr[r + q] = vs;
                     if (mode == 1) ws[r + q] = vs;
                     const double2 vd = to_d2(vs);
                     nrm += vd.x * vd.x + vd.y * vd.y;
                 }
                 if (q < n1) {
-                    const T2 vs2 = from_d2<T2>(v2[q]);
+                    const T2 vs2 = v2[q];
                     wr[r2 + q] = vs2;
                     if (mode == 1) ws[r2 + q] = vs2;
                     const double2 vd2 = to_d2(vs2);
@@ -665,9 +680,9 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
         __syncthreads();  // the chunk of w
         const bool wide = cols >= NW;
         const int G = wide ? 1 : NW / cols;  // warps per column
-        double2 acc[KQ];
+        A2 acc[KQ];
 #pragma unroll
-        for (int q = 0; q < KQ; ++q) acc[q] = make_double2(0, 0);
+        for (int q = 0; q < KQ; ++q) acc[q] = from_d2<A2>(make_double2(0, 0));
         if (wide || warp < G * cols) {
             const int kw = wide ? warp : warp % cols;
             const int slice = wide ? 0 : warp / cols;
@@ -693,32 +708,20 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
                     x2[q] = q < n1 ? ws[r2 + q] : from_d2<T2>(make_double2(0, 0));
                 }
 #pragma unroll
-                for (int q = 0; q < KQ; ++q) {
-                    if constexpr (RL == 2) {
-                        // FP32 basis: the 4 products of a step summed in FP32 (a lane sums a few tens of
-                        // products a chunk), added to the FP64 partial
-                        float2 f = make_float2(0.f, 0.f);
+                for (int q = 0; q < KQ; ++q)
 #pragma unroll
-                        for (int e = 0; e < RL; ++e) {
-                            const float2 a = t[q].v[e], b = x[e], c = u[q].v[e], d = x2[e];
-                            f.x += a.x * b.x + a.y * b.y + c.x * d.x + c.y * d.y;
-                            f.y += a.x * b.y - a.y * b.x + c.x * d.y - c.y * d.x;
-                        }
-                        acc[q].x += f.x;
-                        acc[q].y += f.y;
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < RL; ++e) {
-                            acc[q] = dadd(acc[q], dmulc(to_d2(t[q].v[e]), to_d2(x[e])));
-                            acc[q] = dadd(acc[q], dmulc(to_d2(u[q].v[e]), to_d2(x2[e])));
-                        }
+                    for (int e = 0; e < RL; ++e) {
+                        const A2 a = amulc(t[q].v[e], x[e]), b = amulc(u[q].v[e], x2[e]);
+                        acc[q].x += a.x;
+                        acc[q].y += a.y;
+                        acc[q].x += b.x;
+                        acc[q].y += b.y;
                     }
-                }
             }
         }
 #pragma unroll
         for (int q = 0; q < KQ; ++q) {
-            double2 v = acc[q];
+            double2 v = to_d2(acc[q]);  // the sums over lanes, CTAs and chunks in FP64
             for (int o = 16; o > 0; o >>= 1) {
                 v.x += __shfl_down_sync(0xffffffffu, v.x, o);
                 v.y += __shfl_down_sync(0xffffffffu, v.y, o);
