@@ -222,6 +222,11 @@ typedef struct rtm_solve_config {
     int right_preconditioned; /* GMRES: 0 left preconditioning (GeneralizedMinimumResidual.m:2-5), 1 right
                                  (x = x0 + M V y at the end of each cycle: the monitored residual is that
                                  of op * x = b) */
+    int gram_schmidt_passes;  /* classical Gram-Schmidt passes of each Arnoldi step: 2 (CGS2, the
+                                 reference's orthogonalize_.m:15-23) or 1. GMRES: 0 selects 2. FGMRES_IR applies
+                                 it to its FP32 inner solves, where 0 selects 1: the FP64 refinement measures
+                                 the true residual, so orthogonality lost in one pass costs inner iterations,
+                                 never accuracy */
 } rtm_solve_config;
 
 typedef struct rtm_solve_stats {

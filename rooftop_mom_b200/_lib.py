@@ -46,7 +46,7 @@ class RtmError(RuntimeError):
 class SolveConfig(C.Structure):
     _fields_ = [("method", C.c_int), ("tolerance", C.c_double), ("max_iterations", C.c_int),
                 ("restart", C.c_int), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int),
-                ("check_every", C.c_int), ("right_preconditioned", C.c_int)]
+                ("check_every", C.c_int), ("right_preconditioned", C.c_int), ("gram_schmidt_passes", C.c_int)]
 
 
 class SolveStats(C.Structure):

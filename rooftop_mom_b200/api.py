@@ -635,7 +635,7 @@ class Solver:
     precision form 'fgmres' (FP32 flexible GMRES inside FP64 iterative refinement)."""
 
     def __init__(self, method="cg", tolerance=1e-6, maxIterationCount=1000, restart=50, innerTolerance=1e-4,
-                 maxRefinements=20, checkEvery=0, innerMethod="fgmres", side="left"):
+                 maxRefinements=20, checkEvery=0, innerMethod="fgmres", side="left", gramSchmidtPasses=0):
         if method not in ("cg", "gmres", "fgmres"):
             raise _err("rooftopMoM:solver:invalidMethod", "The method is 'cg', 'gmres' or 'fgmres'.")
         if not (0 < tolerance < 1):
@@ -655,10 +655,15 @@ class Solver:
         if side not in ("left", "right"):
             raise _err("rooftopMoM:solver:invalidSide", "The preconditioning side is 'left' or 'right'.")
         self.side = side
+        if gramSchmidtPasses not in (0, 1, 2):
+            raise _err("rooftopMoM:solver:invalidGramSchmidtPasses",
+                       "gramSchmidtPasses is 0 (the method's default), 1 or 2.")
+        self.gramSchmidtPasses = int(gramSchmidtPasses)
 
     def _config(self, method_id):
         return L.SolveConfig(method_id, self.tolerance, self.maxIterationCount, self.restart, self.innerTolerance,
-                             self.maxRefinements, self.checkEvery, int(self.side == "right"))
+                             self.maxRefinements, self.checkEvery, int(self.side == "right"),
+                             self.gramSchmidtPasses)
 
     def solve(self, operator, rightHandSide, preconditioner=None, initialGuess=None, innerOperator=None,
               innerPreconditioner=None, nrhs: int = 1):

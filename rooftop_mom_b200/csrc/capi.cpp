@@ -485,6 +485,8 @@ static int check_config(const rtm_solve_config* c) {
     if (!(c->tolerance > 0) || !(c->tolerance < 1)) return fail(RTM_ERR_ARG, "tolerance must lie in (0, 1)");
     if (c->max_iterations < 1) return fail(RTM_ERR_ARG, "maxIterationCount must be positive");
     if (c->method == RTM_METHOD_GMRES && c->restart < 1) return fail(RTM_ERR_ARG, "The restart is a positive integer.");
+    if (c->gram_schmidt_passes < 0 || c->gram_schmidt_passes > 2)
+        return fail(RTM_ERR_ARG, "gram_schmidt_passes is 0 (the default), 1 or 2");
     return RTM_OK;
 }
 
@@ -535,6 +537,7 @@ int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_config* 
     cfg.restart = config->restart;
     cfg.check_every = config->check_every;
     cfg.right_preconditioned = config->right_preconditioned;
+    cfg.gram_schmidt_passes = config->gram_schmidt_passes == 0 ? 2 : config->gram_schmidt_passes;
     cudaEvent_t e0, e1;
     RTM_CUDA(cudaEventCreate(&e0));
     RTM_CUDA(cudaEventCreate(&e1));
@@ -580,6 +583,7 @@ int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner
     cfg.check_every = config->check_every;
     cfg.inner_tolerance = config->inner_tolerance > 0 ? config->inner_tolerance : 1e-4;
     cfg.max_refinements = config->max_refinements > 0 ? config->max_refinements : 20;
+    cfg.inner_gram_schmidt_passes = config->gram_schmidt_passes == 0 ? 1 : config->gram_schmidt_passes;
     cudaEvent_t e0, e1;
     RTM_CUDA(cudaEventCreate(&e0));
     RTM_CUDA(cudaEventCreate(&e1));

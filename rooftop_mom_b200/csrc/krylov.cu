@@ -1282,8 +1282,11 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
             } else {
                 RTM_TRY(A->apply(vj, w.ptr, nrhs, s, skip_step));
             }
+            // CGS2: project (mode 0), subtract and project again (1), subtract the correction and take the
+            // norm (2). One pass skips mode 1: mode 2 then subtracts the first projection, which mode 0
+            // left in the coefficients it reads.
             launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 0, s);
-            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, s);
+            if (cfg.gram_schmidt_passes != 1) launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, s);
             launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 2, s);
             k_gm_next<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
             count_launch(1);
@@ -1400,7 +1403,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
                  int nrhs, SolveResult& res, cudaStream_t s);
 
 int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& cfg, const void* bv, const void* x0v,
-                void* xv, int64_t n, int nrhs, SolveResult& res, cudaStream_t s) {
+                void* xv, int64_t n, int nrhs, SolveResult& res, cudaStream_t s, LinearOp* M64) {
     const double2* b = static_cast<const double2*>(bv);
     const double2* x0 = static_cast<const double2*>(x0v);
     double2* x = static_cast<double2*>(xv);
@@ -1435,8 +1438,9 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     int inner_total = 0, steps = 0;
     res.matvecs = 0;
     std::vector<int> hd(nrhs);
-    std::vector<double2> hr(nrhs);
+    std::vector<double2> hr(nrhs), hr_prev(nrhs);
     std::vector<double> inner_tol(nrhs);
+    bool fallback = false;
     for (int step = 0;; ++step) {
         RTM_TRY(A64->apply(x, t64.ptr, nrhs, s, SkipFlags{}));
         k_residual<double2><<<grid, kRT, 0, s>>>(b, t64.as<double2>(), r64.as<double2>(), n, nullptr, 0);
@@ -1450,10 +1454,19 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         RTM_CUDA(cudaMemcpyAsync(hr.data(), resb.ptr, sizeof(double2) * nrhs, cudaMemcpyDeviceToHost, s));
         RTM_CUDA(cudaStreamSynchronize(s));
         steps = step;
-        bool all = true;
-        for (int v : hd) all = all && v;
-        if (all || step >= cfg.max_refinements || inner_total >= cfg.max_iterations || (cfg.cancel && *cfg.cancel))
+        bool all = true, stalled = false;
+        for (int k = 0; k < nrhs; ++k) {
+            all = all && hd[k];
+            // a step that leaves a right-hand side's FP64 residual above half of what it was
+            if (step > 0 && !hd[k] && hr[k].x > 0.5 * hr_prev[k].x) stalled = true;
+        }
+        hr_prev = hr;
+        if (all || (cfg.cancel && *cfg.cancel)) break;
+        if (cfg.fallback_fp64 && stalled) {
+            fallback = true;
             break;
+        }
+        if (step >= cfg.max_refinements || inner_total >= cfg.max_iterations) break;
         k_ir_to32<<<grid, kRT, 0, s>>>(r64.as<double2>(), r32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
         // The inner FP32 solve of A32 d = r / ||r||: COCG, or restarted flexible GMRES(m).
@@ -1466,9 +1479,11 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         ic.tolerance = cfg.inner_tolerance;
         ic.tolerances = inner_tol.data();
         ic.max_iterations = std::max(1, cfg.max_iterations - inner_total);
+        if (cfg.inner_max_iterations > 0) ic.max_iterations = std::min(ic.max_iterations, cfg.inner_max_iterations);
         ic.restart = m;
         ic.check_every = cfg.check_every;
         ic.right_preconditioned = 1;
+        ic.gram_schmidt_passes = cfg.inner_gram_schmidt_passes;
         ic.cancel = cfg.cancel;
         SolveResult ir;
         if (inner_cg) RTM_TRY(cocg<float>(A32, M32, ic, r32.ptr, nullptr, d32.ptr, n, nrhs, ir, s));
@@ -1479,6 +1494,31 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
         res.matvecs += ir.matvecs + most + 1;
         k_ir_update<<<grid, kRT, 0, s>>>(x, d32.as<float2>(), n, resb.as<double2>(), done.as<int>());
         count_launch();
+    }
+    if (fallback) {
+        // the FP32 inner solves stopped making progress: finish every right-hand side in FP64 from the current
+        // iterate (those already converged stop at once, their first residual meeting the tolerance)
+        DeviceBuffer xs;
+        RTM_TRY(xs.alloc(vec64));
+        RTM_CUDA(cudaMemcpyAsync(xs.ptr, x, vec64, cudaMemcpyDeviceToDevice, s));
+        SolveConfig fc = cfg;
+        fc.method = inner_cg ? RTM_METHOD_CG : RTM_METHOD_GMRES;
+        fc.tolerances = nullptr;
+        fc.max_iterations = std::max(1, cfg.max_iterations - inner_total);
+        fc.restart = m;
+        fc.right_preconditioned = 1;
+        SolveResult fr;
+        RTM_TRY(solve(A64, M64, fc, b, xs.ptr, x, n, nrhs, fr, s));
+        res.history = fr.history;
+        res.hist_stride = fr.hist_stride;
+        res.matvecs += fr.matvecs;
+        res.stats = fr.stats;
+        for (auto& o : res.stats) {
+            o.iteration_count += inner_total;
+            o.refinements = steps;
+            o.matvecs = res.matvecs;
+        }
+        return RTM_OK;
     }
     std::vector<double2> rb(nrhs);
     std::vector<int> hc(nrhs);

@@ -18,6 +18,10 @@ struct SolveConfig {
     double inner_tolerance = 1e-4;  // mixed: the tightest relative residual an inner FP32 solve aims at
     int max_refinements = 20;
     int right_preconditioned = 0;  // GMRES: 0 left (the reference's form), 1 right (flexible)
+    int inner_max_iterations = 0;  // mixed: iterations one inner FP32 solve may take (0: the remaining budget)
+    int fallback_fp64 = 0;         // mixed: finish in FP64 when a refinement step does not halve the residual
+    int gram_schmidt_passes = 2;   // GMRES: classical Gram-Schmidt passes per Arnoldi step (2: CGS2, or 1)
+    int inner_gram_schmidt_passes = 1;  // mixed: the passes of the FP32 inner solves
     const std::atomic<int>* cancel = nullptr;  // nonzero: stop at the next host check (unconverged result)
 };
 
@@ -32,8 +36,11 @@ struct SolveResult {
 int solve(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b, const void* x0, void* x, int64_t n, int nrhs,
           SolveResult& res, cudaStream_t s);
 
-// FP64 outer iterative refinement around FP32 inner flexible GMRES (A64 FP64, A32 / M32 FP32).
+// FP64 outer iterative refinement around FP32 inner flexible GMRES (A64 FP64, A32 / M32 FP32). With
+// cfg.fallback_fp64, a refinement step that does not halve some right-hand side's FP64 residual (the FP32
+// inner solve diverged or stalled) ends the refinement, and the solve finishes in FP64 (A64 and M64, which
+// may be null) from the current iterate.
 int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& cfg, const void* b, const void* x0,
-                void* x, int64_t n, int nrhs, SolveResult& res, cudaStream_t s);
+                void* x, int64_t n, int nrhs, SolveResult& res, cudaStream_t s, LinearOp* M64 = nullptr);
 
 }  // namespace rtm

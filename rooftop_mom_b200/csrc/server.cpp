@@ -36,6 +36,7 @@ using Clock = std::chrono::steady_clock;
 
 constexpr int kBlockJacobiUnknowns = 8;  // packed unknowns a 2 x 2-face block of the block-Jacobi inverse (ops.cu)
 constexpr int kPcBlockJacobi = 1, kPcCirculant = 2;  // rtm_request.preconditioner
+constexpr int kInnerCap = 3000;  // iterations of one inner FP32 solve of the mixed server
 
 struct Record {
     uint64_t id = 0;
@@ -109,7 +110,8 @@ int request_bytes(const rtm_request& q, int precision, int sizes, double* bytes)
     else if (q.preconditioner == kPcCirculant)
         pc = est[3] + est[4];
     double total = est[0] + est[1] + est[2] + pc + est[5] + 2 * 16 * n;
-    if (precision == RTM_FP32) total += 0.5 * (est[1] + est[2] + est[5]) + 4 * 16 * n;  // inner FP32 copies
+    // inner FP32 copies, and the FP32 preconditioner beside the FP64 one of the FP64 finish
+    if (precision == RTM_FP32) total += 0.5 * (est[1] + est[2] + est[5] + pc) + 4 * 16 * n;
     *bytes = total;
     return RTM_OK;
 }
@@ -215,7 +217,9 @@ struct rtm_server {
             rtm_operator* op = nullptr;
             rtm_operator* op32 = nullptr;
             rtm_preconditioner* pc = nullptr;
+            rtm_preconditioner* pc64 = nullptr;  // mixed: the FP64 preconditioner of the FP64 finish
             ~Handles() {
+                rtm_preconditioner_destroy(pc64);
                 rtm_preconditioner_destroy(pc);
                 rtm_operator_destroy(op32);
                 rtm_operator_destroy(op);
@@ -234,6 +238,11 @@ struct rtm_server {
         else if (q.preconditioner == kPcCirculant)
             RTM_TRY(rtm_preconditioner_create(h.g, q.size_x, q.size_y, RTM_KERNEL_RCHAN, RTM_BUILDER_PARTWISE, nullptr,
                                               mixed ? RTM_FP32 : RTM_FP64, &h.pc));
+        if (mixed && q.preconditioner == kPcBlockJacobi)
+            RTM_TRY(rtm_preconditioner_create_block_jacobi(h.g, q.size_x, q.size_y, 2, 2, RTM_FP64, &h.pc64));
+        else if (mixed && q.preconditioner == kPcCirculant)
+            RTM_TRY(rtm_preconditioner_create(h.g, q.size_x, q.size_y, RTM_KERNEL_RCHAN, RTM_BUILDER_PARTWISE, nullptr,
+                                              RTM_FP64, &h.pc64));
         const int64_t n = h.op->op->n;
         out.res.unknowns = n;
         cudaStream_t s = h.op->stream;
@@ -265,9 +274,14 @@ struct rtm_server {
         cudaEventRecord(e0, s);
         int st;
         if (mixed) {
+            // FP32 COCG can diverge on large plates (its short recurrence loses accuracy in FP32): a refinement
+            // step that does not halve the FP64 residual hands the solve to FP64 COCG from the current iterate,
+            // and no inner solve takes more than kInnerCap iterations
             sc.inner_tolerance = 1e-4;
+            sc.inner_max_iterations = kInnerCap;
+            sc.fallback_fp64 = 1;
             st = solve_mixed(h.op->op.get(), h.op32->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr,
-                             x.ptr, n, 1, res, s);
+                             x.ptr, n, 1, res, s, h.pc64 ? h.pc64->op.get() : nullptr);
         } else {
             st = solve(h.op->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr, x.ptr, n, 1, res, s);
         }

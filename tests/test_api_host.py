@@ -179,6 +179,9 @@ def test_invalid_solvers_and_solver_inputs_raise():
     with pytest.raises(RtmError) as e:
         Solver(restart=2.5)
     assert e.value.identifier == "rooftopMoM:solver:invalidRestart"
+    with pytest.raises(RtmError) as e:
+        Solver(method="gmres", gramSchmidtPasses=3)
+    assert e.value.identifier == "rooftopMoM:solver:invalidGramSchmidtPasses"
     solver = Solver()
     with pytest.raises(RtmError) as e:
         solver.solve("matrix", np.ones(3))

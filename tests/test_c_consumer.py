@@ -92,3 +92,32 @@ def test_the_mex_gateway_compiles_against_the_header():
     subprocess.run(["gcc", "-std=c99", "-fsyntax-only", "-Wall", "-Wextra", "-Werror",
                     "-I", os.path.join(ROOT, "tests", "c", "mex_stub"), "-I", os.path.join(ROOT, "include"), path],
                    check=True, capture_output=True, text=True)
+
+
+def test_ctypes_structures_match_the_header_layout(tmp_path):
+    """Every ABI structure the Python binding mirrors has the header's size and field offsets (a field added
+    to one side only would shift the others)."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib as L
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    mirrors = {"rtm_solve_config": L.SolveConfig, "rtm_solve_stats": L.SolveStats, "rtm_tune_result": L.TuneResult,
+               "rtm_server_config": L.ServerConfig, "rtm_request": L.Request, "rtm_request_result": L.RequestResult}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "rtm.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'    printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'    printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["    return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=60).stdout
+    got = {(a, b): int(c) for a, b, c in (line.split() for line in out.splitlines())}
+    for cname, cls in mirrors.items():
+        assert got[(cname, "sizeof")] == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)

@@ -161,3 +161,22 @@ def test_transform_size_policies_give_the_reference_sizes_results(policy):
     for a, b in zip(got, ref):
         assert a["state"] == "done" and a["converged"]
         assert _rel(a["current"], b["current"]) < 1e-6
+
+
+def test_the_mixed_server_converges_on_large_plates():
+    """FP32 COCG with the rChan circulant can diverge on large plates; the mixed server's refinement then
+    hands the solve to FP64 COCG from its iterate. Every request converges to its FP64 tolerance and its
+    current stays within the tolerance's reach of the FP64 server's."""
+    import rooftop_mom_b200 as R
+
+    reqs = [R.Request.planeWave(n, m, LAM / 20, LAM / 20, K, direction=(0.5, 0.0, -math.sqrt(0.75)),
+                                polarization=(0.0, 1.0, 0.0), tolerance=1e-6, keepCurrent=True, method="cg",
+                                preconditioner="rChan", maxIterationCount=20000)
+            for n, m in ((384, 320), (300, 260))]
+    with R.Server(budgetBytes=100e9, maxActive=2) as ref_srv:
+        ref = [ref_srv.wait(ref_srv.submit(q), release=True) for q in reqs]
+    with R.Server(budgetBytes=100e9, maxActive=2, precision="single") as srv:
+        got = [srv.wait(srv.submit(q), release=True) for q in reqs]
+    for a, b in zip(got, ref):
+        assert a["state"] == "done" and a["converged"] and a["residual"] <= 1e-6
+        assert _rel(a["current"], b["current"]) < 1e-4

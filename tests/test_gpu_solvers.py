@@ -164,6 +164,41 @@ def test_mixed_precision_refinement_reaches_fp64_tolerance():
     assert rel(mix.solution(), ref.solution()) < 1e-6
 
 
+@pytest.mark.parametrize("passes", [1, 2])
+def test_mixed_refinement_reaches_fp64_tolerance_with_either_inner_gram_schmidt(passes):
+    """The FP32 inner solves with one or two classical Gram-Schmidt passes: the FP64 refinement reaches the
+    same solution either way, since it measures the true residual."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(64, 64, 1 / 15, 1 / 15), 2 * np.pi)
+    op64 = R.Operator(prob)
+    op32 = R.Operator(prob, precision="single")
+    pc32 = R.Preconditioner.blockJacobi(prob, (2, 2), precision="single")
+    exc = R.Excitation.planeWave(prob, direction=[0.5, 0, -np.sqrt(3) / 2], polarization=[0, 1, 0])
+    ref = R.Solver(method="gmres", tolerance=1e-10, restart=100, maxIterationCount=5000).solve(op64, exc)
+    mix = R.Solver(method="fgmres", tolerance=1e-8, restart=50, innerTolerance=1e-3, gramSchmidtPasses=passes,
+                   maxIterationCount=5000).solve(op64, exc, innerOperator=op32, innerPreconditioner=pc32)
+    assert mix.converged() and mix.residualNorm() < 1e-8
+    assert rel(mix.solution(), ref.solution()) < 1e-6
+
+
+def test_one_gram_schmidt_pass_gmres_matches_two_on_a_plate():
+    """FP64 GMRES with one classical Gram-Schmidt pass against the reference's two: on a well-conditioned
+    block-Jacobi system both reach the tolerance and agree to it."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(48, 48, 0.05, 0.05), 2 * np.pi)
+    op = R.Operator(prob)
+    pc = R.Preconditioner.blockJacobi(prob, (2, 2))
+    exc = R.Excitation.planeWave(prob, direction=[0.5, 0, -np.sqrt(3) / 2], polarization=[0, 1, 0])
+    two = R.Solver(method="gmres", tolerance=1e-8, restart=50).solve(op, exc, preconditioner=pc)
+    one = R.Solver(method="gmres", tolerance=1e-8, restart=50, gramSchmidtPasses=1).solve(op, exc,
+                                                                                          preconditioner=pc)
+    assert one.converged() and two.converged()
+    assert rel(one.solution(), two.solution()) < 1e-6
+    assert abs(one.iterationCount() - two.iterationCount()) <= max(2, two.iterationCount() // 20)
+
+
 @pytest.mark.parametrize("precision", ["double", "single"])
 def test_batched_circulant_apply_equals_single_applies(precision):
     import rooftop_mom_b200 as R
