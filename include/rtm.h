@@ -173,6 +173,10 @@ typedef struct rtm_tune_result {
 } rtm_tune_result;
 RTM_API int rtm_tune_product(int count_x, int count_y, int precision, int nrhs, int flags, rtm_tune_result* out);
 /* Forgets every choice of the autotuner (products created afterwards take the reference's sizes). */
+/* Records fft_x x fft_y (at least the face counts) as the transform grid of the split products built
+ * afterwards for this face grid and precision on the calling thread's device, with the default kernel
+ * schedule, as if the autotuner had chosen it (e.g. powers of two for plates that go into one batch). */
+RTM_API int rtm_tune_set(int count_x, int count_y, int precision, int fft_x, int fft_y);
 RTM_API int rtm_tune_clear(void);
 
 /* A dense n x n complex operator (column-major), for solving any small system with the same solvers
@@ -251,6 +255,29 @@ RTM_API int rtm_solve(rtm_operator* op, rtm_preconditioner* pc, const rtm_solve_
 RTM_API int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_preconditioner* inner_pc,
                     const rtm_solve_config* config, const void* b, const void* x0, void* x, int64_t n, int nrhs,
                     int where, double* history, rtm_solve_stats* stats, void* stream);
+
+/* Plate batches (not in the reference) ------------------------------------------------------- */
+
+/* A batch of count entries, entry k one right-hand side on the plate of ops[k]: plates of uneven size
+ * (and several right-hand sides of one plate, as entries that share its operator) solved together. The
+ * vectors of a batch hold count entries of `stride` elements, the largest entry's unknowns; entry k's own
+ * n_k unknowns come first, the elements after them are ignored on input and zero on output. The operators
+ * have one precision; split products that share their transform grid on the power-of-two path
+ * (rtm_tune_product chooses such grids) run as one launch of each of their kernels for the whole batch
+ * (`fused` of rtm_plate_batch_info), any others one entry after another. pcs is NULL or count
+ * preconditioners, one per entry. The operators and preconditioners must outlive the batch. */
+typedef struct rtm_plate_batch rtm_plate_batch;
+RTM_API int rtm_plate_batch_create(rtm_operator* const* ops, rtm_preconditioner* const* pcs, int count,
+                                   rtm_plate_batch** out);
+RTM_API int rtm_plate_batch_info(const rtm_plate_batch* batch, int64_t* stride, int* count, int* fused);
+/* y = A x entry by entry (x and y count x stride elements). */
+RTM_API int rtm_plate_batch_apply(rtm_plate_batch* batch, const void* x, void* y, int where, void* stream);
+/* rtm_solve over the batch (method RTM_METHOD_CG or RTM_METHOD_GMRES): every entry stops on its own
+ * tolerance; history (count x (max_iterations+1)) and stats (count) as rtm_solve's. */
+RTM_API int rtm_plate_batch_solve(rtm_plate_batch* batch, const rtm_solve_config* config, const void* b,
+                                  const void* x0, void* x, int where, double* history, rtm_solve_stats* stats,
+                                  void* stream);
+RTM_API int rtm_plate_batch_destroy(rtm_plate_batch* batch);
 
 /* Excitation and results (src/+rooftopMoM/+operator) ------------------------------------------ */
 

@@ -8,6 +8,7 @@ from .api import (  # noqa: F401
     Generators,
     Mesh,
     Operator,
+    PlateBatch,
     Preconditioner,
     Problem,
     Resources,
@@ -15,6 +16,7 @@ from .api import (  # noqa: F401
     Solver,
     clearTuning,
     fast_fft_size,
+    setTransformSize,
     tuneProduct,
 )
 from .server import Request, Server  # noqa: F401

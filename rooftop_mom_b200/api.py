@@ -630,6 +630,20 @@ class Result:
         return self.radarCrossSection() / wavelength**2
 
 
+def _require_finite_rhs(b):
+    """Solver.m:162-168: a right-hand side is numeric (which logical arrays are not) and finite."""
+    if _is_device(b):
+        return
+    try:
+        a = np.asarray(b)
+        finite = a.dtype.kind in "iufc" and bool(np.all(np.isfinite(a)))
+    except (TypeError, ValueError):
+        finite = False
+    if not finite:
+        raise _err("rooftopMoM:solver:invalidRightHandSide",
+                   "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+
+
 class Solver:
     """src/+rooftopMoM/Solver.m: 'cg' (COCG) or 'gmres' (restarted GMRES), plus the GPU-only
     precision form 'fgmres' (FP32 flexible GMRES inside FP64 iterative refinement)."""
@@ -660,6 +674,36 @@ class Solver:
                        "gramSchmidtPasses is 0 (the method's default), 1 or 2.")
         self.gramSchmidtPasses = int(gramSchmidtPasses)
 
+    def solveBatch(self, batch: "PlateBatch", rightHandSides, initialGuesses=None):
+        """Solves every entry of a PlateBatch (its operator and preconditioner) for its right-hand side, all
+        entries at once, each to this solver's tolerance; 'cg' or 'gmres'. Returns one Result per entry."""
+        if self.method not in ("cg", "gmres"):
+            raise _err("rooftopMoM:solver:invalidMethod", "A plate batch solves by 'cg' or 'gmres'.")
+        excitations = [v if isinstance(v, Excitation) else None for v in rightHandSides]
+        vectors = [v.vector() if isinstance(v, Excitation) else v for v in rightHandSides]
+        for v, e in zip(vectors, excitations):
+            if e is None:
+                _require_finite_rhs(v)
+        device = _is_device(vectors[0])
+        b = batch._pack(vectors, device)
+        x0 = batch._pack(initialGuesses, device) if initialGuesses is not None else None
+        count = batch.count()
+        hist = np.full((count, self.maxIterationCount + 1), np.nan)
+        stats = (L.SolveStats * count)()
+        cfg = self._config(L.METHODS[self.method])
+        if device:
+            import torch
+            x = torch.empty_like(b)
+            ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+            L.call("rtm_plate_batch_solve", batch._handle, C.byref(cfg), ptr(b), ptr(x0), ptr(x), L.DEVICE,
+                   hist.ctypes.data_as(C.c_void_p), stats, None)
+        else:
+            x = np.empty_like(b)
+            ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None  # noqa: E731
+            L.call("rtm_plate_batch_solve", batch._handle, C.byref(cfg), ptr(b), ptr(x0), ptr(x), L.HOST,
+                   hist.ctypes.data_as(C.c_void_p), stats, None)
+        return [Result(xk, stats[k], hist[k], excitations[k]) for k, xk in enumerate(batch._unpack(x))]
+
     def _config(self, method_id):
         return L.SolveConfig(method_id, self.tolerance, self.maxIterationCount, self.restart, self.innerTolerance,
                              self.maxRefinements, self.checkEvery, int(self.side == "right"),
@@ -673,16 +717,7 @@ class Solver:
             b = rightHandSide.vector()
         else:
             b = rightHandSide
-            if not _is_device(b):
-                try:
-                    a = np.asarray(b)
-                    # Solver.m:162-168: isnumeric, which logical arrays are not
-                    finite = a.dtype.kind in "iufc" and bool(np.all(np.isfinite(a)))
-                except (TypeError, ValueError):
-                    finite = False
-                if not finite:
-                    raise _err("rooftopMoM:solver:invalidRightHandSide",
-                               "The right-hand side is a rooftopMoM.Excitation or a numeric vector of finite values.")
+            _require_finite_rhs(b)
         if initialGuess is not None and not _is_device(initialGuess):
             # Solver.m:62: mustBeNumeric (which rejects logical arrays) and mustBeFinite
             try:
@@ -764,6 +799,100 @@ def tuneProduct(mesh: Mesh, precision="double", nrhs: int = 1, flushL2: bool = T
 def clearTuning():
     """Forgets every autotuner choice (rtm_tune_clear)."""
     L.call("rtm_tune_clear")
+
+
+def setTransformSize(mesh: Mesh, fftSize, precision="double"):
+    """Records fftSize = (P, Q), at least the face counts, as the transform grid of the split products built
+    afterwards for this plate's face grid and precision (rtm_tune_set): e.g. powers of two for plates that
+    go into one PlateBatch."""
+    if precision not in L.PRECISIONS:
+        raise _err("rooftopMoM:operator:invalidPrecision", "The precision is 'double' or 'single'.")
+    cx, cy = mesh.count()
+    L.call("rtm_tune_set", cx, cy, L.PRECISIONS[precision], int(fftSize[0]), int(fftSize[1]))
+
+
+class PlateBatch:
+    """Plates of uneven size solved together (rtm_plate_batch_*; not in the reference): entry k is one
+    right-hand side on the plate of operators[k] (an entry may repeat a plate's operator for another
+    right-hand side), with preconditioners[k] if given. Split products that share their transform grid
+    on the power-of-two path run as one launch of each kernel for the whole batch (fused()); vectors are
+    the entries' own vectors, which solve() pads to the batch's stride and crops again."""
+
+    def __init__(self, operators, preconditioners=None):
+        self._ops = list(operators)
+        self._pcs = list(preconditioners) if preconditioners is not None else None
+        if not self._ops:
+            raise _err("rooftopMoM:batch:empty", "A plate batch holds at least one entry.")
+        if self._pcs is not None and len(self._pcs) != len(self._ops):
+            raise _err("rooftopMoM:batch:sizeMismatch", "One preconditioner per entry.")
+        count = len(self._ops)
+        ops = (C.c_void_p * count)(*[o.handle for o in self._ops])
+        pcs = (C.c_void_p * count)(*[p.handle for p in self._pcs]) if self._pcs is not None else None
+        out = C.c_void_p()
+        L.call("rtm_plate_batch_create", ops, pcs, count, C.byref(out))
+        self._handle = out
+        stride, n, fused = C.c_int64(), C.c_int(), C.c_int()
+        L.call("rtm_plate_batch_info", out, C.byref(stride), C.byref(n), C.byref(fused))
+        self._stride, self._fused = stride.value, bool(fused.value)
+        self._counts = [o.rooftopCount() for o in self._ops]
+        self.precision = getattr(self._ops[0], "precision", "double")
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            try:
+                L.load().rtm_plate_batch_destroy(self._handle)
+            except Exception:  # interpreter shutdown
+                pass
+            self._handle = None
+
+    def count(self):
+        return len(self._ops)
+
+    def stride(self):
+        return self._stride
+
+    def fused(self):
+        return self._fused
+
+    def rooftopCounts(self):
+        return list(self._counts)
+
+    def _pack(self, vectors, device):
+        if len(vectors) != len(self._ops):
+            raise _err("rooftopMoM:batch:sizeMismatch", f"The batch takes {len(self._ops)} vectors.")
+        for v, n in zip(vectors, self._counts):
+            if (v.numel() if _is_device(v) else np.size(v)) != n:
+                raise RtmError(L.ERR_SIZE, f"The input must be a numeric {n}x1 vector.",
+                               "rooftopMoM:product:sizeMismatch")
+        if device:
+            import torch
+            dt = torch.complex64 if self.precision == "single" else torch.complex128
+            out = torch.zeros(len(vectors) * self._stride, dtype=dt, device=vectors[0].device)
+            for k, v in enumerate(vectors):
+                out[k * self._stride:k * self._stride + self._counts[k]] = v.reshape(-1).to(dt)
+            return out
+        out = np.zeros(len(vectors) * self._stride, np.complex128)
+        for k, v in enumerate(vectors):
+            out[k * self._stride:k * self._stride + self._counts[k]] = np.asarray(v, np.complex128).reshape(-1)
+        return out
+
+    def _unpack(self, packed):
+        return [packed[k * self._stride:k * self._stride + n] for k, n in enumerate(self._counts)]
+
+    def apply(self, vectors):
+        """y_k = A_k x_k for every entry."""
+        device = _is_device(vectors[0])
+        x = self._pack(vectors, device)
+        if device:
+            import torch
+            y = torch.empty_like(x)
+            L.call("rtm_plate_batch_apply", self._handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                   L.DEVICE, None)
+        else:
+            y = np.empty_like(x)
+            L.call("rtm_plate_batch_apply", self._handle, x.ctypes.data_as(C.c_void_p),
+                   y.ctypes.data_as(C.c_void_p), L.HOST, None)
+        return self._unpack(y)
 
 
 class Resources:

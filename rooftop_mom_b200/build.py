@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "librtm.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["runtime.cpp", "capi.cpp", "server.cpp", "grid.cu", "grid_fast.cu", "assembly.cu", "krylov.cu", "ops.cu", "excitation.cu", "fixed_scratch.cu", "fault.cu", "tune.cpp"]
+SOURCES = ["runtime.cpp", "capi.cpp", "server.cpp", "grid.cu", "grid_fast.cu", "assembly.cu", "krylov.cu", "ops.cu", "excitation.cu", "fixed_scratch.cu", "fault.cu", "tune.cpp", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Wno-deprecated-gpu-targets"]

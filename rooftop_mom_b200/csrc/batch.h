@@ -1,0 +1,42 @@
+// Plate batches: several plates of uneven size, one right-hand side each, solved together.
+//
+// The vectors of a batch hold `count` entries of `stride` elements (the largest plate's rooftops); entry k
+// keeps its plate's n_k rooftops first and zeros after them. A batch operator applies every entry's own
+// operator: split products that share their transform grid and precision on the power-of-two path run as
+// one launch of each of their three kernels for the whole batch (grid_fast.cu reads each right-hand side's
+// plate from a descriptor table); other operators and the preconditioners run one after another on their
+// entries. Every apply zeroes the entries' tails, so the Krylov solvers run on the batch unchanged: the
+// padding adds zeros to every sum.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "grid.h"
+
+namespace rtm {
+
+struct BatchOp : LinearOp {
+    std::vector<LinearOp*> ops;          // per entry (borrowed; the handles outlive the batch)
+    std::vector<int64_t> counts;         // per entry: unknowns
+    int64_t stride = 0;                  // elements of an entry
+    bool fused = false;                  // one launch per kernel for the whole batch
+    std::vector<const GridApplicator*> plates;  // fused: the entries' products
+    DeviceBuffer descs, tails, work;     // fused: plate table, per-entry unknowns (device), working grids
+    int* fault = nullptr;
+
+    int apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) override;
+    int reserve(int nrhs) override;
+    double working_bytes() const override { return (double)work.bytes; }
+};
+
+// A batch over the given per-entry operators (all of one precision, each of n_k <= stride unknowns).
+// fuse: join split products of one transform grid into single launches when they allow it.
+std::unique_ptr<BatchOp> make_batch(const std::vector<LinearOp*>& ops, int64_t stride, bool fuse, cudaStream_t s,
+                                    int* status);
+
+// Zeroes elements [counts[k], stride) of entry k of y (k < count, where the skip flag is zero).
+int zero_tails(void* y, int precision, int64_t stride, const int64_t* counts_device, int count, cudaStream_t s,
+               SkipFlags skip);
+
+}  // namespace rtm

@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "excitation.h"
 #include "handles.h"
 #include "krylov.h"
@@ -682,6 +683,143 @@ int rtm_input_impedance(int count_x, int count_y, double size_x, double size_y, 
         st = input_impedance(count_x, count_y, size_x, size_y, static_cast<const double2*>(j.ptr), port, port_count,
                              voltage, out, s);
     return st;
+}
+
+struct rtm_plate_batch {
+    std::unique_ptr<rtm::BatchOp> op, pc;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ~rtm_plate_batch() {
+        if (stream) cudaStreamSynchronize(stream);
+        op.reset();
+        pc.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+int rtm_plate_batch_create(rtm_operator* const* ops, rtm_preconditioner* const* pcs, int count,
+                           rtm_plate_batch** out) {
+    if (!ops || !out) return fail(RTM_ERR_ARG, "null argument");
+    *out = nullptr;
+    RTM_TRY(check_rhs(count));
+    std::vector<LinearOp*> o(count), p;
+    int64_t stride = 0;
+    for (int k = 0; k < count; ++k) {
+        if (!ops[k]) return fail(RTM_ERR_ARG, "null operator in a plate batch");
+        o[k] = ops[k]->op.get();
+        stride = std::max(stride, o[k]->n);
+    }
+    if (pcs) {
+        p.resize(count);
+        for (int k = 0; k < count; ++k) {
+            if (!pcs[k]) return fail(RTM_ERR_ARG, "null preconditioner in a plate batch");
+            if (pcs[k]->op->n != o[k]->n)
+                return fail(RTM_ERR_SIZE, "The preconditioner does not match the " + std::to_string(o[k]->n) +
+                                              " unknowns of its plate.");
+            if (pcs[k]->op->precision != o[k]->precision)
+                return fail(RTM_ERR_ARG, "operator and preconditioner must have one precision");
+            p[k] = pcs[k]->op.get();
+        }
+    }
+    auto h = std::make_unique<rtm_plate_batch>();
+    h->device = ops[0]->device;
+    RTM_TRY(make_stream(&h->stream));
+    int st = RTM_OK;
+    h->op = make_batch(o, stride, true, h->stream, &st);
+    RTM_TRY(st);
+    if (pcs) {
+        h->pc = make_batch(p, stride, false, h->stream, &st);
+        RTM_TRY(st);
+    }
+    *out = h.release();
+    return RTM_OK;
+}
+
+int rtm_plate_batch_info(const rtm_plate_batch* b, int64_t* stride, int* count, int* fused) {
+    if (!b) return fail(RTM_ERR_ARG, "null handle");
+    if (stride) *stride = b->op->stride;
+    if (count) *count = (int)b->op->ops.size();
+    if (fused) *fused = b->op->fused ? 1 : 0;
+    return RTM_OK;
+}
+
+int rtm_plate_batch_apply(rtm_plate_batch* b, const void* x, void* y, int where, void* stream) {
+    if (!b || !x || !y) return fail(RTM_ERR_ARG, "null argument");
+    RTM_TRY(check_where(where));
+    cudaStream_t s = pick(stream, b->stream);
+    const int count = (int)b->op->ops.size();
+    const int64_t total = b->op->stride * count;
+    const int prec = b->op->precision;
+    Staged in;
+    Out o;
+    RTM_TRY(stage_in(x, total, prec, where, in, s));
+    RTM_TRY(out_prepare(y, total, prec, where, o, s));
+    RTM_TRY(b->op->reserve(count));
+    RTM_TRY(b->op->apply(in.ptr, o.ptr, count, s, SkipFlags{}));
+    RTM_TRY(out_finish(y, total, prec, where, o, s));
+    if (where == RTM_HOST || !stream) RTM_CUDA(cudaStreamSynchronize(s));
+    return device_fault_check(s);
+}
+
+int rtm_plate_batch_solve(rtm_plate_batch* b, const rtm_solve_config* config, const void* rhs, const void* x0,
+                          void* x, int where, double* history, rtm_solve_stats* stats, void* stream) {
+    if (!b || !rhs || !x) return fail(RTM_ERR_ARG, "null argument");
+    RTM_TRY(check_config(config));
+    RTM_TRY(check_where(where));
+    if (config->method == RTM_METHOD_FGMRES_IR) return fail(RTM_ERR_ARG, "a plate batch solves by COCG or GMRES");
+    const int count = (int)b->op->ops.size();
+    const int64_t stride = b->op->stride, total = stride * count;
+    const int prec = b->op->precision;
+    const size_t elem = prec == RTM_FP64 ? sizeof(double2) : sizeof(float2);
+    // the solver's vectors: GMRES the basis and three more, COCG six
+    const int m = (int)std::max<int64_t>(1, std::min<int64_t>(config->restart, stride));
+    const double vectors = config->method == RTM_METHOD_GMRES ? m + 4.0 : 6.0;
+    RTM_TRY(budget_require(vectors * (double)total * elem, "The solve"));
+    cudaStream_t s = pick(stream, b->stream);
+    Staged sb, sx0;
+    Out o;
+    RTM_TRY(stage_in(rhs, total, prec, where, sb, s));
+    RTM_TRY(stage_in(x0, total, prec, where, sx0, s));
+    RTM_TRY(out_prepare(x, total, prec, where, o, s));
+    // the solver reads the right-hand sides and the initial guesses with their tails zeroed
+    DeviceBuffer bz, xz;
+    RTM_TRY(bz.alloc(total * elem));
+    RTM_CUDA(cudaMemcpyAsync(bz.ptr, sb.ptr, total * elem, cudaMemcpyDeviceToDevice, s));
+    RTM_TRY(zero_tails(bz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, s, SkipFlags{}));
+    if (x0) {
+        RTM_TRY(xz.alloc(total * elem));
+        RTM_CUDA(cudaMemcpyAsync(xz.ptr, sx0.ptr, total * elem, cudaMemcpyDeviceToDevice, s));
+        RTM_TRY(zero_tails(xz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, s, SkipFlags{}));
+    }
+    SolveConfig cfg;
+    cfg.method = config->method;
+    cfg.tolerance = config->tolerance;
+    cfg.max_iterations = config->max_iterations;
+    cfg.restart = config->restart;
+    cfg.check_every = config->check_every;
+    cfg.right_preconditioned = config->right_preconditioned;
+    cfg.gram_schmidt_passes = config->gram_schmidt_passes == 0 ? 2 : config->gram_schmidt_passes;
+    cudaEvent_t e0, e1;
+    RTM_CUDA(cudaEventCreate(&e0));
+    RTM_CUDA(cudaEventCreate(&e1));
+    RTM_CUDA(cudaEventRecord(e0, s));
+    SolveResult res;
+    int st = rtm::solve(b->op.get(), b->pc.get(), cfg, bz.ptr, x0 ? xz.ptr : nullptr, o.ptr, stride, count, res, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != RTM_OK) return st;
+    RTM_TRY(out_finish(x, total, prec, where, o, s));
+    copy_out_stats(res, history, stats, count, config->max_iterations, ms);
+    return RTM_OK;
+}
+
+int rtm_plate_batch_destroy(rtm_plate_batch* b) {
+    delete b;
+    return RTM_OK;
 }
 
 }  // extern "C"

@@ -320,13 +320,9 @@ size_t GridApplicator::work_bytes_per_rhs() const {
     return (size_t)npy * 2 * P * Q * elem;
 }
 
-template <typename T>
-static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip,
-                   void* work, int* fault) {
+// The launch arguments of a product (the transform grid's tables, the face grid, the spectra).
+template <typename T> static GridArgs<T> product_args(const GridApplicator& g, SkipFlags skip) {
     using T2 = typename Cx<T>::T2;
-    RTM_TRY(set_smem_attrs<T>());
-    const T2* x = static_cast<const T2*>(xv);
-    T2* y = static_cast<T2*>(yv);
     GridArgs<T> a{};
     a.skip = skip.ptr;
     a.skip_stride = skip.stride;
@@ -357,6 +353,17 @@ static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, 
     a.inv_a2 = (T)(1.0 / (g.size_x * g.size_x));
     a.inv_b2 = (T)(1.0 / (g.size_y * g.size_y));
     a.inv_ab = (T)(1.0 / (g.size_x * g.size_y));
+    return a;
+}
+
+template <typename T>
+static int apply_t(const GridApplicator& g, const void* xv, void* yv, int nrhs, cudaStream_t s, SkipFlags skip,
+                   void* work, int* fault) {
+    using T2 = typename Cx<T>::T2;
+    RTM_TRY(set_smem_attrs<T>());
+    const T2* x = static_cast<const T2*>(xv);
+    T2* y = static_cast<T2*>(yv);
+    GridArgs<T> a = product_args<T>(g, skip);
     const size_t elem = sizeof(T2);
     if (g.mode == kStrip) {
         a.scale = (T)(1.0 / g.P);
@@ -431,6 +438,68 @@ int GridApplicator::reserve(int nrhs) {
     if (mode != kStrip) RTM_TRY(work.alloc(work_bytes_per_rhs() * (size_t)nrhs));
     max_rhs = std::max(max_rhs, nrhs);
     return RTM_OK;
+}
+
+bool batchable(const GridApplicator& g) {
+    return g.mode == kGen3 && g.nsx == 2 && g.nsy == 2 && !g.lean &&
+           fast_split_eligible(g.P, g.Q, g.precision == RTM_FP64);
+}
+
+template <typename T>
+static int plate_descs_t(const std::vector<const GridApplicator*>& plates, DeviceBuffer& out, cudaStream_t s) {
+    std::vector<PlateDesc<T>> d(plates.size());
+    for (size_t k = 0; k < plates.size(); ++k) {
+        const GridApplicator& g = *plates[k];
+        for (int c = 0; c < 2; ++c) {
+            d[k].rows[c] = g.rows[c];
+            d[k].cols[c] = g.cols[c];
+            d[k].off[c] = g.off[c];
+        }
+        d[k].spec = g.spec.as<typename Cx<T>::T2>();
+        d[k].inv_a2 = (T)(1.0 / (g.size_x * g.size_x));
+        d[k].inv_b2 = (T)(1.0 / (g.size_y * g.size_y));
+        d[k].inv_ab = (T)(1.0 / (g.size_x * g.size_y));
+    }
+    RTM_TRY(out.alloc(sizeof(PlateDesc<T>) * d.size()));
+    RTM_CUDA(cudaMemcpyAsync(out.ptr, d.data(), out.bytes, cudaMemcpyHostToDevice, s));
+    RTM_CUDA(cudaStreamSynchronize(s));
+    return RTM_OK;
+}
+
+int plate_descs(const std::vector<const GridApplicator*>& plates, DeviceBuffer& out, cudaStream_t s) {
+    if (plates.empty()) return fail(RTM_ERR_ARG, "an empty plate batch");
+    return plates[0]->precision == RTM_FP64 ? plate_descs_t<double>(plates, out, s)
+                                            : plate_descs_t<float>(plates, out, s);
+}
+
+template <typename T>
+static int apply_batch_t(const std::vector<const GridApplicator*>& plates, const void* descs, int64_t stride,
+                         void* work, int* fault, const void* xv, void* yv, cudaStream_t s, SkipFlags skip) {
+    const GridApplicator& g = *plates[0];
+    RTM_TRY(set_smem_attrs<T>());
+    GridArgs<T> a = product_args<T>(g, skip);
+    a.plates = static_cast<const PlateDesc<T>*>(descs);
+    a.n = stride;
+    for (const GridApplicator* p : plates)  // the launch grids span the largest plate
+        for (int c = 0; c < 2; ++c) {
+            a.rows[c] = std::max(a.rows[c], p->rows[c]);
+            a.cols[c] = std::max(a.cols[c], p->cols[c]);
+        }
+    a.scale = (T)(1.0 / ((double)g.P * g.Q));
+    a.fault = fault;
+    a.work = static_cast<typename Cx<T>::T2*>(work);
+    a.work_rhs = (int64_t)g.work_bytes_per_rhs() / (int64_t)sizeof(typename Cx<T>::T2);
+    a.py0 = 0;
+    a.npy = 2;
+    a.accumulate = 0;
+    return launch_fast_split<T>(a, (int)plates.size(), xv, yv, g.sched, s);
+}
+
+int apply_plate_batch(const std::vector<const GridApplicator*>& plates, const void* descs, int64_t stride, void* work,
+                      int* fault, const void* x, void* y, cudaStream_t s, SkipFlags skip) {
+    return plates[0]->precision == RTM_FP64
+               ? apply_batch_t<double>(plates, descs, stride, work, fault, x, y, s, skip)
+               : apply_batch_t<float>(plates, descs, stride, work, fault, x, y, s, skip);
 }
 
 int GridApplicator::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) {

@@ -14,6 +14,8 @@
 //   y-inverse: inverse FFT along y, demodulate, sum over the y subbands, crop to the rooftop grids.
 #pragma once
 
+#include <vector>
+
 #include "internal.h"
 #include "ops.h"
 
@@ -63,6 +65,15 @@ struct GridApplicator : LinearOp {
     double stored_bytes() const override { return (double)spec.bytes; }
     double working_bytes() const override { return (double)work.bytes; }
 };
+
+// Plate batches (several plates, one right-hand side each, in one launch of each kernel): whether a
+// product can join one (a split product on the power-of-two path), the device table of the plates'
+// descriptors, and the product of a batch whose products share their transform grid and precision (vectors
+// of `stride` elements, one per plate; work holds a working grid per plate).
+bool batchable(const GridApplicator& g);
+int plate_descs(const std::vector<const GridApplicator*>& plates, DeviceBuffer& out, cudaStream_t s);
+int apply_plate_batch(const std::vector<const GridApplicator*>& plates, const void* descs, int64_t stride, void* work,
+                      int* fault, const void* x, void* y, cudaStream_t s, SkipFlags skip);
 
 // y = A x with the working grid in a fixed device array of fixed_scratch_bytes() instead of the
 // product's own buffer; allocates nothing (RTM_ERR_SIZE when nrhs working grids do not fit).

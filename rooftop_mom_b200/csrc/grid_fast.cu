@@ -162,13 +162,15 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_y_fwd(const Gri
     griddep_launch_dependents();
     const int c = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
+    const PlateDesc<T> pd = plate_of(a, rhs);
+    const int rows = pd.rows[c], cols = pd.cols[c];
+    if ((int)blockIdx.x * TI >= rows) return;  // a smaller plate of a batch
     const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
     const int g = l + TI * py;
-    const int rows = a.rows[c], cols = a.cols[c];
     const int i = blockIdx.x * TI + l;
     const bool on = i < rows;
     const LineBuf<T2> buf{sm + g, (R2 + 1) * G, G};
-    const T2* xr = x + (int64_t)rhs * a.n + a.off[c];
+    const T2* xr = x + (int64_t)rhs * a.n + pd.off[c];
     T2 v[R1];
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
@@ -204,6 +206,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_x_mix_direct(co
     griddep_launch_dependents();
     const int py = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
+    const PlateDesc<T> pd = plate_of(a, rhs);
     const int t = threadIdx.x % R2, gid = threadIdx.x / R2;
     const int team = gid / 4, c = gid % 2, px = (gid / 2) % 2;
     const int j = blockIdx.x * TEAMS + team;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_x_mix_direct(co
     const LineBuf<T2> buf{sm + gid * LB, R2 + 1, 1};
     T2* own = sm + gid * LB;
     const T2* partner = sm + (gid ^ 1) * LB;
-    const int rows = a.rows[c];
+    const int rows = pd.rows[c];
     T2* row = a.work + (int64_t)rhs * a.work_rhs + (int64_t)(py * a.ncomp + c) * QP + (int64_t)(on ? j : 0) * NP;
     T2 v[R1];
 #pragma unroll
@@ -232,10 +235,10 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_x_mix_direct(co
     __syncthreads();
     if (on) {
         const int sub = px + 2 * py;
-        const T2* spec = a.spec + (int64_t)(sub * 3) * QP + (int64_t)j * NP;
+        const T2* spec = pd.spec + (int64_t)(sub * 3) * QP + (int64_t)j * NP;
         const T2* ux = px ? a.ux1 : a.ux0;
         const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
-        const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+        const T cv = (vv.x * vv.x + vv.y * vv.y) * pd.inv_b2;
 #pragma unroll
         for (int s = 0; s < S; ++s)
 #pragma unroll
@@ -244,11 +247,11 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_x_mix_direct(co
                 const T2 E = __ldg(&spec[k]);
                 const T2 M = __ldg(&spec[(1 + c) * QP + k]);
                 const T2 uu = __ldg(&ux[k]);
-                const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                const T cu = (uu.x * uu.x + uu.y * uu.y) * pd.inv_a2;
                 // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
                 T2 qc = cmulc(uu, vv);
-                qc.x = -qc.x * a.inv_ab;
-                qc.y = -qc.y * a.inv_ab;
+                qc.x = -qc.x * pd.inv_ab;
+                qc.y = -qc.y * pd.inv_ab;
                 const T2 coupling = c ? cconj(qc) : qc;
                 const T cself = c ? cv : cu;
                 const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
@@ -337,10 +340,11 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
         if (spectra) {
             ++issued[1];
             mbar_expect_tx(&bar[1], 6 * BLOCK);
+            const T2* sp = a.plates ? a.plates[rhs].spec : a.spec;
             for (int q = 0; q < 2; ++q)
                 for (int kind = 0; kind < 3; ++kind)
                     bulk_load(sst + (q * 3 + kind) * TEAMS * NP,
-                              a.spec + (int64_t)((q + 2 * py) * 3 + kind) * QP + (int64_t)j0 * NP, BLOCK, &bar[1]);
+                              sp + (int64_t)((q + 2 * py) * 3 + kind) * QP + (int64_t)j0 * NP, BLOCK, &bar[1]);
         }
     };
     if (tid == 0) {
@@ -355,11 +359,12 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
     T2* own = sm + gid * LB;
     const T2* partner = sm + (gid ^ 1) * LB;
     const T2* odd = sm + (gid + 2) * LB;
-    const int rows = a.rows[c];
     const T2* ux = px ? a.ux1 : a.ux0;
     while (it < iters) {
         const int nxt = live(it + gridDim.x);
         const int rhs = it / per_rhs, r = it % per_rhs, py = r / per_py, j = (r % per_py) * TEAMS + team;
+        const PlateDesc<T> pd = plate_of(a, rhs);
+        const int rows = pd.rows[c];
         if (__syncthreads_or(!mbar_wait(&bar[0], done[0] & 1, a.fault))) break;
         ++done[0];
         T2 v[R1];
@@ -385,7 +390,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
             const T2* Es = sst + (px * 3 * TEAMS + team) * NP;
             const T2* Ms = sst + ((px * 3 + 1 + c) * TEAMS + team) * NP;
             const T2 vv = __ldg(&(py ? a.vy1 : a.vy0)[j]);
-            const T cv = (vv.x * vv.x + vv.y * vv.y) * a.inv_b2;
+            const T cv = (vv.x * vv.x + vv.y * vv.y) * pd.inv_b2;
 #pragma unroll
             for (int s = 0; s < S; ++s)
 #pragma unroll
@@ -394,11 +399,11 @@ __global__ void __launch_bounds__(Fast<T>::threads, (MixShape<T, NP>::blocks)) k
                     const T2 E = Es[k];
                     const T2 Mk = Ms[k];
                     const T2 uu = __ldg(&ux[k]);
-                    const T cu = (uu.x * uu.x + uu.y * uu.y) * a.inv_a2;
+                    const T cu = (uu.x * uu.x + uu.y * uu.y) * pd.inv_a2;
                     // qc = -u conj(v) / (ab): XY = qc E, YX = conj(qc) E
                     T2 qc = cmulc(uu, vv);
-                    qc.x = -qc.x * a.inv_ab;
-                    qc.y = -qc.y * a.inv_ab;
+                    qc.x = -qc.x * pd.inv_ab;
+                    qc.y = -qc.y * pd.inv_ab;
                     const T2 coupling = c ? cconj(qc) : qc;
                     const T cself = c ? cv : cu;
                     const T2 me = v[s * R2 + k2], other = partner[(s * R2 + k2) * R2 + t];
@@ -448,9 +453,11 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_y_inv(const Gri
     griddep_launch_dependents();
     const int c = blockIdx.y, rhs = blockIdx.z;
     if (skipped(a, rhs)) return;
+    const PlateDesc<T> pd = plate_of(a, rhs);
+    const int rows = pd.rows[c], cols = pd.cols[c];
+    if ((int)blockIdx.x * TI >= rows) return;  // a smaller plate of a batch
     const int l = threadIdx.x % TI, py = (threadIdx.x / TI) % 2, t = threadIdx.x / (2 * TI);
     const int g = l + TI * py;
-    const int rows = a.rows[c], cols = a.cols[c];
     const int i = blockIdx.x * TI + l;
     const bool on = i < rows;
     const LineBuf<T2> buf{sm + g, (R2 + 1) * G, G};
@@ -472,7 +479,7 @@ __global__ void __launch_bounds__(Fast<T>::threads, MINB) k_fast_y_inv(const Gri
     __syncthreads();
     if (py || !on) return;
     const LineBuf<T2> odd{sm + g + TI, (R2 + 1) * G, G};
-    T2* yr = y + (int64_t)rhs * a.n + a.off[c];
+    T2* yr = y + (int64_t)rhs * a.n + pd.off[c];
 #pragma unroll
     for (int m1 = 0; m1 < R1; ++m1) {
         const int j = R2 * m1 + t;

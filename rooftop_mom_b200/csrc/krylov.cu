@@ -1527,15 +1527,25 @@ int solve_mixed(LinearOp* A64, LinearOp* A32, LinearOp* M32, const SolveConfig& 
     res.history.resize((size_t)hs * nrhs);
     RTM_CUDA(cudaMemcpyAsync(res.history.data(), hist.ptr, hist.bytes, cudaMemcpyDeviceToHost, s));
     RTM_CUDA(cudaStreamSynchronize(s));
+    // IterativeMethod.m:53-56: the solution of a zero right-hand side is zero, whatever the initial guess
+    std::vector<int> zero(nrhs);
+    bool any_zero = false;
+    for (int k = 0; k < nrhs; ++k) any_zero |= (zero[k] = rb[k].y == 0.0) != 0;
+    if (any_zero) {
+        RTM_CUDA(cudaMemcpyAsync(done.ptr, zero.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, s));
+        k_zero_where<double2><<<grid, kRT, 0, s>>>(x, n, done.as<int>(), 1);
+        count_launch();
+        RTM_CUDA(cudaStreamSynchronize(s));
+    }
     RTM_TRY(device_fault_check(s));
     res.hist_stride = hs;
     res.stats.resize(nrhs);
     for (int k = 0; k < nrhs; ++k) {
         rtm_solve_stats& o = res.stats[k];
         o.converged = hc[k];
-        o.iteration_count = inner_total;
+        o.iteration_count = zero[k] ? 0 : inner_total;
         o.residual_norm = rb[k].y == 0 ? 0.0 : rb[k].x / rb[k].y;
-        o.refinements = steps;
+        o.refinements = zero[k] ? 0 : steps;
         o.matvecs = res.matvecs;
     }
     return RTM_OK;

@@ -205,6 +205,15 @@ int rtm_tune_product(int count_x, int count_y, int precision, int nrhs, int flag
     return RTM_OK;
 }
 
+int rtm_tune_set(int count_x, int count_y, int precision, int fft_x, int fft_y) {
+    if (count_x < 2 || count_y < 2) return fail(RTM_ERR_ARG, "transform grids are set for plates of at least 2 x 2 faces");
+    if (precision != RTM_FP64 && precision != RTM_FP32) return fail(RTM_ERR_ARG, "unknown precision");
+    if (fft_x < count_x || fft_y < count_y) return fail(RTM_ERR_ARG, "a transform grid smaller than the face grid");
+    if (fft_x > (1 << 16) || fft_y > (1 << 16)) return fail(RTM_ERR_SIZE, "transform lengths up to 65536");
+    register_choice(count_x, count_y, precision, fft_x, fft_y);
+    return RTM_OK;
+}
+
 int rtm_tune_clear(void) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned.clear();

@@ -75,6 +75,32 @@ def test_batched_calls_bound_the_vector_count(library):
     assert "positive" in _lib.last_error()
 
 
+def test_plate_batches_and_transform_sizes_check_their_arguments_first(library):
+    """rtm_plate_batch_* and rtm_tune_set reject null handles, entry counts outside 1..65535 and transform
+    grids smaller than the face grid before any device work."""
+    import ctypes as C
+
+    from rooftop_mom_b200 import _lib
+
+    lib = _lib.load()
+    out = C.c_void_p()
+    ops = (C.c_void_p * 2)(None, None)
+    assert lib.rtm_plate_batch_create(None, None, 1, C.byref(out)) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_create(ops, None, 0, C.byref(out)) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_create(ops, None, 65536, C.byref(out)) == _lib.ERR_SIZE
+    assert lib.rtm_plate_batch_create(ops, None, 2, C.byref(out)) == _lib.ERR_ARG
+    assert "null operator" in _lib.last_error()
+    v64, v = C.c_int64(), C.c_int()
+    assert lib.rtm_plate_batch_info(None, C.byref(v64), C.byref(v), C.byref(v)) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_apply(None, None, None, _lib.HOST, None) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_solve(None, None, None, None, None, _lib.HOST, None, None, None) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_destroy(None) == 0
+    assert lib.rtm_tune_set(100, 80, 0, 64, 128) == _lib.ERR_ARG
+    assert "smaller than the face grid" in _lib.last_error()
+    assert lib.rtm_tune_set(100, 80, 7, 128, 128) == _lib.ERR_ARG
+    assert lib.rtm_tune_set(1, 80, 0, 128, 128) == _lib.ERR_ARG
+
+
 def test_plane_waves_take_perpendicular_unit_vectors(library):
     """generatePlaneWave.m takes a unit direction and a unit polarization perpendicular to it; the ABI checks
     both before any device work."""

@@ -182,6 +182,14 @@ def test_invalid_solvers_and_solver_inputs_raise():
     with pytest.raises(RtmError) as e:
         Solver(method="gmres", gramSchmidtPasses=3)
     assert e.value.identifier == "rooftopMoM:solver:invalidGramSchmidtPasses"
+    from rooftop_mom_b200 import PlateBatch
+
+    with pytest.raises(RtmError) as e:
+        PlateBatch([])
+    assert e.value.identifier == "rooftopMoM:batch:empty"
+    with pytest.raises(RtmError) as e:
+        Solver(method="fgmres").solveBatch(None, [])
+    assert e.value.identifier == "rooftopMoM:solver:invalidMethod"
     solver = Solver()
     with pytest.raises(RtmError) as e:
         solver.solve("matrix", np.ones(3))

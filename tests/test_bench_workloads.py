@@ -76,7 +76,7 @@ def test_reference_arm_takes_the_oracle_iteration_count_of_each_sampled_workload
     import bench
 
     for name, w in bench.WORKLOADS.items():
-        if name in ("c4", "c5") or w["n"] <= bench.FULL_SOLVE_MAX_FACES:
+        if name in ("c4", "c4u", "c5") or w["n"] <= bench.FULL_SOLVE_MAX_FACES:
             continue
         assert bench.ORACLE_ITERATIONS[name] > 0
         assert bench.ORACLE_ITERATION_SOURCE[name]

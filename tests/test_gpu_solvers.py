@@ -235,6 +235,21 @@ def test_mixed_cocg_with_a_circulant_solves_several_right_hand_sides():
         assert rel(r.solution(), single.solution()) < 1e-4
 
 
+@pytest.mark.parametrize("inner", ["cg", "fgmres"])
+def test_mixed_solve_of_a_zero_right_hand_side_is_zero(inner):
+    """IterativeMethod.m:53-56: the solution of a zero right-hand side is zero, whatever the initial guess."""
+    import rooftop_mom_b200 as R
+
+    prob = R.Problem(R.Mesh(24, 20, 0.05, 0.05), 2 * np.pi)
+    n = prob.rooftopCount()
+    op64 = R.Operator(prob)
+    op32 = R.Operator(prob, precision="single")
+    res = R.Solver(method="fgmres", innerMethod=inner, tolerance=1e-6).solve(
+        op64, np.zeros(n, dtype=complex), innerOperator=op32, initialGuess=np.ones(n, dtype=complex))
+    assert res.converged() and res.iterationCount() == 0
+    assert np.all(np.asarray(res.solution()) == 0)
+
+
 def _wave(theta, phi):
     t, p = np.radians(theta), np.radians(phi)
     d = np.array([np.sin(t) * np.cos(p), np.sin(t) * np.sin(p), -np.cos(t)])
