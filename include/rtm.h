@@ -324,6 +324,12 @@ typedef struct rtm_server_config {
     int device;            /* CUDA device of the workers */
     int transform_sizes;   /* rtm_transform_sizes of the requests' split products (any size at least the face
                               count gives the same product up to rounding) */
+    int max_batch;         /* 0 or 1: every request solves alone on its worker. Above 1 (FP64, power-of-two
+                              sizes): max_active / max_batch workers (at least one), each taking up to
+                              max_batch admitted requests at once whose 2-D plates share their transform grid,
+                              method, preconditioner, restart and iteration bound, solved as one plate batch
+                              (rtm_plate_batch_solve), each on its own tolerance. A request cancelled while its
+                              batch runs is discarded when the batch ends. */
 } rtm_server_config;
 
 typedef enum rtm_excitation { RTM_EXCITE_PLANE_WAVE = 0, RTM_EXCITE_DELTA_GAP = 1 } rtm_excitation;

@@ -69,7 +69,7 @@ TRANSFORM_SIZES = {"reference": 0, "powerOfTwo": 1, "autotune": 2}
 
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_double), ("max_active", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-                ("transform_sizes", C.c_int)]
+                ("transform_sizes", C.c_int), ("max_batch", C.c_int)]
 
 
 class Request(C.Structure):

@@ -24,6 +24,7 @@
 #include <thread>
 #include <vector>
 
+#include "batch.h"
 #include "grid.h"
 #include "handles.h"
 #include "krylov.h"
@@ -130,7 +131,21 @@ struct rtm_server {
     int admitted = 0;
     uint64_t next_id = 1;
     bool stopping = false;
+    std::atomic<int> stop_flag{0};  // the cancel flag of batched solves: set when the server stops
     std::vector<std::thread> workers;
+
+    // Requests that may share one plate batch: 2-D plates whose split products take one power-of-two
+    // transform grid under the power-of-two policy, with one method, preconditioner, restart and iteration
+    // bound (each keeps its own tolerance). False when the request solves alone.
+    bool batch_key(const rtm_request& q, std::vector<int>& key) const {
+        if (cfg.max_batch < 2 || cfg.precision != RTM_FP64 || cfg.transform_sizes != RTM_SIZES_POWER_OF_TWO ||
+            q.count_x < 2 || q.count_y < 2)
+            return false;
+        const int P = next_pow2(q.count_x), Q = next_pow2(q.count_y);
+        if (!fast_split_eligible(P, Q, true)) return false;
+        key = {P, Q, q.method, q.preconditioner, q.restart, q.max_iterations};
+        return true;
+    }
 
     void admit_locked() {
         for (auto it = queue.begin(); it != queue.end() && admitted < cfg.max_active;) {
@@ -150,12 +165,12 @@ struct rtm_server {
     void worker() {
         cudaSetDevice(cfg.device);
         while (true) {
-            Record* r = nullptr;
+            std::vector<Record*> group;
             {
                 std::unique_lock<std::mutex> lk(mu);
                 work_cv.wait(lk, [&] { return stopping || !ready.empty(); });
                 if (ready.empty()) return;  // stopping
-                r = records.at(ready.front()).get();
+                Record* r = records.at(ready.front()).get();
                 ready.pop_front();
                 if (r->cancel) {
                     // Cancelled while admitted: give its bytes and slot back in this same critical
@@ -170,22 +185,39 @@ struct rtm_server {
                     done_cv.notify_all();
                     continue;
                 }
-                r->res.state = RTM_REQUEST_RUNNING;
-                r->res.started_s = seconds_since(epoch);
+                group.push_back(r);
+                std::vector<int> key, other;
+                if (batch_key(r->req, key))
+                    for (auto it = ready.begin(); it != ready.end() && (int)group.size() < cfg.max_batch;) {
+                        Record* o = records.at(*it).get();
+                        if (!o->cancel && batch_key(o->req, other) && other == key) {
+                            group.push_back(o);
+                            it = ready.erase(it);
+                        } else {
+                            ++it;
+                        }
+                    }
+                for (Record* g : group) {
+                    g->res.state = RTM_REQUEST_RUNNING;
+                    g->res.started_s = seconds_since(epoch);
+                }
             }
-            // RUNNING is not a finished state, so no poll releases the record while it runs.
-            Outcome out;
-            const int st = run(*r, out);
+            // RUNNING is not a finished state, so no poll releases the records while they run.
+            std::vector<Outcome> outs(group.size());
+            const int st = group.size() == 1 ? run(*group[0], outs[0]) : run_batch(group, outs);
             {
                 std::lock_guard<std::mutex> lk(mu);
-                out.commit(r->res);
-                r->current = std::move(out.current);
-                r->res.finished_s = seconds_since(epoch);
-                r->res.status = st;
-                held -= r->res.bytes;
-                --admitted;
-                r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
-                                         : (st == RTM_OK ? RTM_REQUEST_DONE : RTM_REQUEST_FAILED);
+                for (size_t k = 0; k < group.size(); ++k) {
+                    Record* r = group[k];
+                    outs[k].commit(r->res);
+                    r->current = std::move(outs[k].current);
+                    r->res.finished_s = seconds_since(epoch);
+                    r->res.status = st;
+                    held -= r->res.bytes;
+                    --admitted;
+                    r->res.state = r->cancel ? RTM_REQUEST_CANCELLED
+                                             : (st == RTM_OK ? RTM_REQUEST_DONE : RTM_REQUEST_FAILED);
+                }
                 admit_locked();
             }
             done_cv.notify_all();
@@ -208,24 +240,34 @@ struct rtm_server {
         return RTM_OK;
     }
 
-    // The whole pipeline of one request on this thread. Its results go to `out`, which the worker
-    // copies into the record under the lock, so a concurrent poll never sees them half written.
-    int run(const Record& r, Outcome& out) {
-        const rtm_request& q = r.req;
-        struct Handles {
-            rtm_generators* g = nullptr;
-            rtm_operator* op = nullptr;
-            rtm_operator* op32 = nullptr;
-            rtm_preconditioner* pc = nullptr;
-            rtm_preconditioner* pc64 = nullptr;  // mixed: the FP64 preconditioner of the FP64 finish
-            ~Handles() {
-                rtm_preconditioner_destroy(pc64);
-                rtm_preconditioner_destroy(pc);
-                rtm_operator_destroy(op32);
-                rtm_operator_destroy(op);
-                rtm_generators_destroy(g);
-            }
-        } h;
+    // A request's device state between the stages of its pipeline.
+    struct Prepared {
+        rtm_generators* g = nullptr;
+        rtm_operator* op = nullptr;
+        rtm_operator* op32 = nullptr;
+        rtm_preconditioner* pc = nullptr;
+        rtm_preconditioner* pc64 = nullptr;  // mixed: the FP64 preconditioner of the FP64 finish
+        DeviceBuffer b, x;
+        std::vector<int64_t> port;
+        int64_t n = 0;
+        cudaStream_t s = nullptr;
+        Prepared() = default;
+        Prepared(const Prepared&) = delete;
+        Prepared& operator=(const Prepared&) = delete;
+        ~Prepared() {
+            if (s) cudaStreamSynchronize(s);
+            b.reset();
+            x.reset();
+            rtm_preconditioner_destroy(pc64);
+            rtm_preconditioner_destroy(pc);
+            rtm_operator_destroy(op32);
+            rtm_operator_destroy(op);
+            rtm_generators_destroy(g);
+        }
+    };
+
+    // Assembly, split-FFT product(s), preconditioner(s) and the excitation on the device.
+    int prepare(const rtm_request& q, Prepared& h) {
         const bool mixed = cfg.precision == RTM_FP32;
         RTM_TRY(choose_sizes(q.count_x, q.count_y, RTM_FP64));
         if (mixed) RTM_TRY(choose_sizes(q.count_x, q.count_y, RTM_FP32));
@@ -243,23 +285,24 @@ struct rtm_server {
         else if (mixed && q.preconditioner == kPcCirculant)
             RTM_TRY(rtm_preconditioner_create(h.g, q.size_x, q.size_y, RTM_KERNEL_RCHAN, RTM_BUILDER_PARTWISE, nullptr,
                                               RTM_FP64, &h.pc64));
-        const int64_t n = h.op->op->n;
-        out.res.unknowns = n;
-        cudaStream_t s = h.op->stream;
-        DeviceBuffer b, x;
-        StreamSyncGuard guard(s);
-        RTM_TRY(b.alloc((size_t)n * sizeof(double2)));
-        RTM_TRY(x.alloc((size_t)n * sizeof(double2)));
-        std::vector<int64_t> port;
+        h.n = h.op->op->n;
+        h.s = h.op->stream;
+        RTM_TRY(h.b.alloc((size_t)h.n * sizeof(double2)));
+        RTM_TRY(h.x.alloc((size_t)h.n * sizeof(double2)));
         if (q.excitation == RTM_EXCITE_PLANE_WAVE) {
             const double one = 1.0;
             RTM_TRY(rtm_plane_wave(q.count_x, q.count_y, q.size_x, q.size_y, 8, q.wavenumber, q.direction,
-                                   q.polarization, &one, 1, b.ptr, RTM_DEVICE, s));
+                                   q.polarization, &one, 1, h.b.ptr, RTM_DEVICE, h.s));
         } else {
-            RTM_TRY(middle_port(q.count_x, q.count_y, q.port_direction, port));
-            RTM_TRY(rtm_delta_gap(q.count_x, q.count_y, q.size_x, q.size_y, port.data(), (int)port.size(), 0,
-                                  q.voltage, b.ptr, RTM_DEVICE));
+            RTM_TRY(middle_port(q.count_x, q.count_y, q.port_direction, h.port));
+            RTM_TRY(rtm_delta_gap(q.count_x, q.count_y, q.size_x, q.size_y, h.port.data(), (int)h.port.size(), 0,
+                                  q.voltage, h.b.ptr, RTM_DEVICE));
         }
+        return RTM_OK;
+    }
+
+    SolveConfig solve_config(const Record& r) const {
+        const rtm_request& q = r.req;
         SolveConfig sc;
         sc.method = q.method;
         sc.tolerance = q.tolerance;
@@ -267,23 +310,57 @@ struct rtm_server {
         sc.restart = q.restart;
         sc.right_preconditioned = 1;
         sc.cancel = &r.cancel;
+        return sc;
+    }
+
+    // The stats of right-hand side k of a solve, the RCS or input impedance, and the current if kept.
+    int finish(const rtm_request& q, Prepared& h, const SolveResult& res, int k, float solve_ms, Outcome& out) {
+        out.res.unknowns = h.n;
+        out.res.solve_s = solve_ms * 1e-3;
+        if ((int)res.stats.size() > k) {
+            out.res.converged = res.stats[k].converged;
+            out.res.iteration_count = res.stats[k].iteration_count;
+            out.res.residual_norm = res.stats[k].residual_norm;
+        }
+        if (q.excitation == RTM_EXCITE_PLANE_WAVE)
+            RTM_TRY(rtm_radar_cross_section(q.wavenumber, h.b.ptr, h.x.ptr, h.n, 1.0, RTM_DEVICE, &out.res.rcs));
+        else
+            RTM_TRY(rtm_input_impedance(q.count_x, q.count_y, q.size_x, q.size_y, h.x.ptr, h.port.data(),
+                                        (int)h.port.size(), q.voltage, RTM_DEVICE, out.res.impedance));
+        if (q.keep_current) {
+            out.current.resize((size_t)2 * h.n);
+            RTM_CUDA(cudaMemcpyAsync(out.current.data(), h.x.ptr, (size_t)h.n * sizeof(double2), cudaMemcpyDeviceToHost,
+                                     h.s));
+            RTM_CUDA(cudaStreamSynchronize(h.s));
+        }
+        return RTM_OK;
+    }
+
+    // The whole pipeline of one request on this thread. Its results go to `out`, which the worker
+    // copies into the record under the lock, so a concurrent poll never sees them half written.
+    int run(const Record& r, Outcome& out) {
+        const rtm_request& q = r.req;
+        Prepared h;
+        RTM_TRY(prepare(q, h));
+        const cudaStream_t s = h.s;
+        SolveConfig sc = solve_config(r);
         SolveResult res;
         cudaEvent_t e0, e1;
         RTM_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDefault));
         RTM_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDefault));
         cudaEventRecord(e0, s);
         int st;
-        if (mixed) {
-            // FP32 COCG can diverge on large plates (its short recurrence loses accuracy in FP32): a refinement
-            // step that does not halve the FP64 residual hands the solve to FP64 COCG from the current iterate,
-            // and no inner solve takes more than kInnerCap iterations
+        if (cfg.precision == RTM_FP32) {
+            // FP32 inner solves of at most kInnerCap iterations inside FP64 refinement; a refinement step that does
+            // not halve the FP64 residual (FP32 COCG can diverge on large plates: its short recurrence loses
+            // accuracy in FP32) hands the solve to the FP64 method from the current iterate
             sc.inner_tolerance = 1e-4;
             sc.inner_max_iterations = kInnerCap;
             sc.fallback_fp64 = 1;
-            st = solve_mixed(h.op->op.get(), h.op32->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr,
-                             x.ptr, n, 1, res, s, h.pc64 ? h.pc64->op.get() : nullptr);
+            st = solve_mixed(h.op->op.get(), h.op32->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, h.b.ptr, nullptr,
+                             h.x.ptr, h.n, 1, res, s, h.pc64 ? h.pc64->op.get() : nullptr);
         } else {
-            st = solve(h.op->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, b.ptr, nullptr, x.ptr, n, 1, res, s);
+            st = solve(h.op->op.get(), h.pc ? h.pc->op.get() : nullptr, sc, h.b.ptr, nullptr, h.x.ptr, h.n, 1, res, s);
         }
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
@@ -292,22 +369,68 @@ struct rtm_server {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (st != RTM_OK) return st;
-        out.res.solve_s = ms * 1e-3;
-        if (!res.stats.empty()) {
-            out.res.converged = res.stats[0].converged;
-            out.res.iteration_count = res.stats[0].iteration_count;
-            out.res.residual_norm = res.stats[0].residual_norm;
+        return finish(q, h, res, 0, ms, out);
+    }
+
+    // Several requests of one batch key (batch_key) solved as one plate batch: each is prepared on its own,
+    // then one solve takes them all, every right-hand side on its own tolerance, and each is finished.
+    int run_batch(const std::vector<Record*>& rs, std::vector<Outcome>& outs) {
+        const int count = (int)rs.size();
+        std::vector<std::unique_ptr<Prepared>> hs;
+        for (Record* r : rs) {
+            hs.push_back(std::make_unique<Prepared>());
+            RTM_TRY(prepare(r->req, *hs.back()));
         }
-        if (q.excitation == RTM_EXCITE_PLANE_WAVE)
-            RTM_TRY(rtm_radar_cross_section(q.wavenumber, b.ptr, x.ptr, n, 1.0, RTM_DEVICE, &out.res.rcs));
-        else
-            RTM_TRY(rtm_input_impedance(q.count_x, q.count_y, q.size_x, q.size_y, x.ptr, port.data(), (int)port.size(),
-                                        q.voltage, RTM_DEVICE, out.res.impedance));
-        if (q.keep_current) {
-            out.current.resize((size_t)2 * n);
-            RTM_CUDA(cudaMemcpyAsync(out.current.data(), x.ptr, (size_t)n * sizeof(double2), cudaMemcpyDeviceToHost, s));
-            RTM_CUDA(cudaStreamSynchronize(s));
+        for (auto& h : hs) RTM_CUDA(cudaStreamSynchronize(h->s));
+        std::vector<LinearOp*> ops, pcs;
+        int64_t stride = 0;
+        for (auto& h : hs) {
+            ops.push_back(h->op->op.get());
+            if (h->pc) pcs.push_back(h->pc->op.get());
+            stride = std::max(stride, h->n);
         }
+        const cudaStream_t s = hs[0]->s;
+        int st = RTM_OK;
+        std::unique_ptr<BatchOp> A = make_batch(ops, stride, true, s, &st), M;
+        RTM_TRY(st);
+        if (!pcs.empty()) {
+            M = make_batch(pcs, stride, false, s, &st);
+            RTM_TRY(st);
+        }
+        const size_t vec = (size_t)stride * sizeof(double2);
+        DeviceBuffer b, x;
+        StreamSyncGuard guard(s);
+        RTM_TRY(b.alloc(vec * count));
+        RTM_TRY(x.alloc(vec * count));
+        RTM_CUDA(cudaMemsetAsync(b.ptr, 0, b.bytes, s));
+        for (int k = 0; k < count; ++k)
+            RTM_CUDA(cudaMemcpyAsync(b.as<double2>() + k * stride, hs[k]->b.ptr, hs[k]->n * sizeof(double2),
+                                     cudaMemcpyDeviceToDevice, s));
+        SolveConfig sc = solve_config(*rs[0]);
+        std::vector<double> tol(count);
+        for (int k = 0; k < count; ++k) tol[k] = rs[k]->req.tolerance;
+        sc.tolerances = tol.data();
+        // a request cancelled while its batch runs is discarded when the batch ends; the batch itself stops
+        // at its next host check when the server stops
+        sc.cancel = &stop_flag;
+        SolveResult res;
+        cudaEvent_t e0, e1;
+        RTM_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDefault));
+        RTM_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDefault));
+        cudaEventRecord(e0, s);
+        st = solve(A.get(), M.get(), sc, b.ptr, nullptr, x.ptr, stride, count, res, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        RTM_TRY(st);
+        for (int k = 0; k < count; ++k)
+            RTM_CUDA(cudaMemcpyAsync(hs[k]->x.ptr, x.as<double2>() + k * stride, hs[k]->n * sizeof(double2),
+                                     cudaMemcpyDeviceToDevice, s));
+        RTM_CUDA(cudaStreamSynchronize(s));
+        for (int k = 0; k < count; ++k) RTM_TRY(finish(rs[k]->req, *hs[k], res, k, ms, outs[k]));
         return RTM_OK;
     }
 };
@@ -326,9 +449,13 @@ int rtm_server_create(const rtm_server_config* config, rtm_server** out) {
     if (srv->cfg.max_active > 256) return fail(RTM_ERR_ARG, "at most 256 active requests");
     if (srv->cfg.transform_sizes < RTM_SIZES_REFERENCE || srv->cfg.transform_sizes > RTM_SIZES_AUTOTUNE)
         return fail(RTM_ERR_ARG, "unknown transform size policy");
+    if (srv->cfg.max_batch < 0 || srv->cfg.max_batch > 256) return fail(RTM_ERR_ARG, "max_batch lies in 0..256");
     srv->epoch = Clock::now();
     rtm_server* p = srv.get();
-    for (int i = 0; i < srv->cfg.max_active; ++i) srv->workers.emplace_back([p] { p->worker(); });
+    // with batches, a worker takes up to max_batch admitted requests at once
+    const int workers = srv->cfg.max_batch > 1 ? std::max(1, srv->cfg.max_active / srv->cfg.max_batch)
+                                               : srv->cfg.max_active;
+    for (int i = 0; i < workers; ++i) srv->workers.emplace_back([p] { p->worker(); });
     *out = srv.release();
     return RTM_OK;
 }
@@ -404,6 +531,7 @@ int rtm_server_destroy(rtm_server* srv) {
     {
         std::lock_guard<std::mutex> lk(srv->mu);
         srv->stopping = true;
+        srv->stop_flag = 1;
         for (uint64_t id : srv->queue) {
             Record& r = *srv->records.at(id);
             r.res.state = RTM_REQUEST_CANCELLED;

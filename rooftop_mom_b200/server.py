@@ -79,15 +79,17 @@ def _result_dict(res: L.RequestResult):
 class Server:
     """rtm_server: admission by byte budget, maxActive requests on the device at once."""
 
-    def __init__(self, budgetBytes=150e9, maxActive=8, precision="double", device=0, transformSizes="reference"):
+    def __init__(self, budgetBytes=150e9, maxActive=8, precision="double", device=0, transformSizes="reference",
+                 maxBatch=0):
         """transformSizes: "reference" (generateFastFFTSize.m's 7-smooth sizes), "powerOfTwo" (plates: the next
         powers of two where the power-of-two kernels take them) or "autotune" (plates: rtm_tune_product on the
-        first request of each face grid)."""
+        first request of each face grid). maxBatch > 1 (FP64, "powerOfTwo"): maxActive / maxBatch workers, each
+        solving up to maxBatch admitted requests of one transform grid and solver setting as one plate batch."""
         if transformSizes not in L.TRANSFORM_SIZES:
             raise L.RtmError(L.ERR_ARG, "transformSizes is 'reference', 'powerOfTwo' or 'autotune'.",
                              "rooftopMoM:gpu:invalidArgument")
         cfg = L.ServerConfig(float(budgetBytes), int(maxActive), L.PRECISIONS[precision], int(device),
-                             L.TRANSFORM_SIZES[transformSizes])
+                             L.TRANSFORM_SIZES[transformSizes], int(maxBatch))
         h = C.c_void_p()
         L.call("rtm_server_create", C.byref(cfg), C.byref(h))
         self._h = h

@@ -180,3 +180,33 @@ def test_the_mixed_server_converges_on_large_plates():
     for a, b in zip(got, ref):
         assert a["state"] == "done" and a["converged"] and a["residual"] <= 1e-6
         assert _rel(a["current"], b["current"]) < 1e-4
+
+
+def test_batched_requests_match_their_solves_alone():
+    """maxBatch: admitted requests whose plates share a power-of-two transform grid (here 64 x 64) and solver
+    setting run as one plate batch; each result agrees with the same request served alone to the accuracy of
+    its tolerance, and requests of other grids or settings are served beside them."""
+    import rooftop_mom_b200 as R
+
+    same = [_plate(60, 50), _plate(64, 64, d=(0, 0, -1), p=(1, 0, 0)), _plate(40, 57),
+            R.Request.deltaGap(50, 40, LAM / 20, LAM / 20, K, portDirection="x", tolerance=TOL, keepCurrent=True),
+            _plate(33, 63)]
+    other = [_strip(41), _plate(20, 20, method="cg")]
+    with R.Server(maxActive=2, transformSizes="powerOfTwo") as srv:
+        alone = [srv.wait(srv.submit(q)) for q in same]
+    with R.Server(maxActive=8, maxBatch=8, transformSizes="powerOfTwo") as srv:
+        # the one worker takes the strip first; the requests submitted meanwhile wait admitted for it
+        ids = [srv.submit(other[0])] + [srv.submit(q) for q in same] + [srv.submit(other[1])]
+        res = [srv.wait(r) for r in ids]
+    batched = res[1:1 + len(same)]
+    # one worker took every request of the shared grid in one batch: they started and finished together
+    assert len({r["finished"] for r in batched}) == 1 and len({r["started"] for r in batched}) == 1
+    for a, b in zip(alone, batched):
+        assert a["state"] == b["state"] == "done"
+        assert b["converged"] and b["residual"] <= TOL
+        assert abs(a["iterations"] - b["iterations"]) <= 3
+        assert _rel(b["current"], a["current"]) < 1e-6
+        if a["rcs"]:
+            assert a["rcs"] == pytest.approx(b["rcs"], rel=1e-6)
+        assert abs(a["impedance"] - b["impedance"]) <= 1e-6 * max(1.0, abs(a["impedance"]))
+    assert all(o["state"] == "done" and o["converged"] for o in (res[0], res[-1]))
