@@ -51,8 +51,8 @@ WORKLOADS = {
                precision="double", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # plates of uneven size solved as one plate batch: Nx, Ny ~ U[lo, n] faces (all on one n x n power-of-two
     # transform grid), cell lambda/20, one plane wave each (theta ~ U[0, 80] deg, phi ~ U[0, 360) deg, TE / TM),
-    # COCG with each plate's rChan circulant to 1e-6 in FP64; against the same plates solved one by one
-    "c4u": dict(n=256, lo=160, density=20, plates=16, seed=0, method="cg", tol=1e-6, restart=50, pc="rChan",
+    # block-Jacobi (2 x 2 faces) GMRES(50) to 1e-6 in FP64 (the C2 method); against the same plates one by one
+    "c4u": dict(n=64, lo=33, density=20, plates=64, seed=0, method="gmres", tol=1e-6, restart=50, pc="blockJacobi",
                 precision="double", theta="U[0,80]", phi="U[0,360)", pol="TE/TM"),
     # request stream of plate solves (see serving_requests)
     "c5": dict(n=0, density=0, seed=0, method="cg", tol=1e-6, restart=50, pc="rChan", precision="double",
@@ -126,8 +126,11 @@ def uneven_plates(R, w):
 
 
 def plate_batch_step(R, w, batched, device=True):
-    """One c4u step: every plate's assembly, spectra, rChan circulant and plane wave, then the solves (one
-    plate batch, or one plate after another) and each plate's RCS. Returns (results, RCS values, fused)."""
+    """One c4u step: every plate's assembly, spectra, preconditioner and plane wave, then the solves (one
+    plate batch, or one plate after another) and each plate's RCS. Returns (results, RCS values, fused,
+    seconds of the solves alone)."""
+    import torch
+
     sizes, dirs, pols = uneven_plates(R, w)
     h = 1.0 / w["density"]
     plates = []
@@ -136,9 +139,13 @@ def plate_batch_step(R, w, batched, device=True):
         R.setTransformSize(mesh, (w["n"], w["n"]))
         prob = R.Problem(mesh, 2 * math.pi)
         op = R.Operator(prob)
-        pc = R.Preconditioner(prob, kernel=w["pc"])
+        pc = (R.Preconditioner.blockJacobi(prob, (2, 2)) if w["pc"] == "blockJacobi"
+              else R.Preconditioner(prob, kernel=w["pc"]))
         plates.append((op, pc, R.Excitation.planeWave(prob, direction=d, polarization=p, device=device)))
-    solver = R.Solver(method=w["method"], tolerance=w["tol"], restart=w["restart"], maxIterationCount=20000)
+    solver = R.Solver(method=w["method"], tolerance=w["tol"], restart=w["restart"], maxIterationCount=20000,
+                      side="right")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     if batched:
         batch = R.PlateBatch([op for op, _, _ in plates], [pc for _, pc, _ in plates])
         res = solver.solveBatch(batch, [e for _, _, e in plates])
@@ -146,7 +153,8 @@ def plate_batch_step(R, w, batched, device=True):
     else:
         res = [solver.solve(op, e, preconditioner=pc) for op, pc, e in plates]
         fused = False
-    return res, [r.radarCrossSection() for r in res], fused
+    torch.cuda.synchronize()
+    return res, [r.radarCrossSection() for r in res], fused, time.perf_counter() - t0
 
 
 def run_plate_batch(args, w):
@@ -166,8 +174,10 @@ def run_plate_batch(args, w):
             launches0 = L.launch_count()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
+            solve_s = 0.0
             for _ in range(args.steps):
-                res, rcs, fused = plate_batch_step(R, w, batched)
+                res, rcs, fused, ts = plate_batch_step(R, w, batched)
+                solve_s += ts
             e1.record()
             torch.cuda.synchronize()
             t = e0.elapsed_time(e1) / 1e3
@@ -175,14 +185,15 @@ def run_plate_batch(args, w):
                           "iterations": max(r.iterationCount() for r in res),
                           "true_residual": max(r.residualNorm() for r in res),
                           "all_converged_to_tolerance": all(r.converged() and r.residualNorm() <= w["tol"] for r in res),
-                          "gpu_launches": int(L.launch_count() - launches0), "fused": fused, "rcs": rcs}
+                          "gpu_launches": int(L.launch_count() - launches0), "fused": fused, "rcs": rcs,
+                          "solve_ms_per_step": solve_s / args.steps * 1e3}
         # e2e: the plane waves from host memory through the same public call, the currents back to it
         plate_batch_step(R, w, True, device=False)
         torch.cuda.synchronize()
         e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         e2[0].record()
         for _ in range(args.steps):
-            res_h, _, _ = plate_batch_step(R, w, True, device=False)
+            res_h, _, _, _ = plate_batch_step(R, w, True, device=False)
         e2[1].record()
         torch.cuda.synchronize()
         t_e2e = e2[0].elapsed_time(e2[1]) / 1e3
@@ -190,18 +201,21 @@ def run_plate_batch(args, w):
     unknowns = [(cx - 1) * cy + cx * (cy - 1) for cx, cy in sizes]
     rcs_b, rcs_s = arms["batch"].pop("rcs"), arms["one_by_one"].pop("rcs")
     line = {
-        "metric": "batched solves/s of plates of uneven size (one plane wave each) at rel. residual 1e-6, "
-                  "COCG + rChan, FP64",
+        "metric": f"batched solves/s of plates of uneven size (one plane wave each) at rel. residual 1e-6, "
+                  f"{w['method']} + {w['pc']}, FP64",
         "value": arms["batch"]["value"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": arms["batch"]["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128", "data": "synthetic plates and plane waves, seed 0",
         "config": {"workload": f"c4u: {w['plates']} plates, Nx, Ny ~ U[{w['lo']},{w['n']}] faces on one "
                                f"{w['n']}x{w['n']} transform grid, cell lambda/{w['density']}, one plane wave each, "
-                               f"COCG + rChan to {w['tol']:g}, FP64, one plate batch", "plates": w["plates"],
+                               f"{w['pc']} {w['method']}({w['restart']}) to {w['tol']:g}, FP64, one plate batch",
+                   "plates": w["plates"],
                    "unknowns": unknowns, "l2": "working set per step re-created every step"},
         "iterations": arms["batch"]["iterations"], "true_residual": arms["batch"]["true_residual"],
         "all_converged_to_tolerance": arms["batch"]["all_converged_to_tolerance"], "fused": arms["batch"]["fused"],
+        "solve_ms_per_step": arms["batch"]["solve_ms_per_step"],
         "one_by_one": arms["one_by_one"], "batch_over_one_by_one": arms["batch"]["value"] / arms["one_by_one"]["value"],
+        "solves_batch_over_one_by_one": arms["one_by_one"]["solve_ms_per_step"] / arms["batch"]["solve_ms_per_step"],
         "rcs_rel_batch_vs_one_by_one": max(abs(a - b) / abs(b) for a, b in zip(rcs_b, rcs_s)),
         "e2e": {"value": w["plates"] * args.steps / t_e2e, "unit": "solves/s",
                 "h2d_bytes_per_step": 16 * sum(unknowns), "d2h_bytes_per_step": 16 * sum(unknowns)},
@@ -236,7 +250,7 @@ def serving_requests(R, count, seed):
     return out
 
 
-def serve_stream(R, count, slots, precision, sizes, seed=0):
+def serve_stream(R, count, slots, precision, sizes, seed=0, batch=0):
     """The c5 stream on a server: a closed-loop burst measures capacity (a tenth of the stream, at least four
     requests a slot), then the stream arrives as a Poisson process at 0.8 x capacity; per-request latency
     (submission to result) gives p50 / p99. precision "double" (FP64) or "mixed" (FP32 inner solves, FP64
@@ -245,7 +259,7 @@ def serve_stream(R, count, slots, precision, sizes, seed=0):
 
     reqs = serving_requests(R, count, seed)
     prec = "single" if precision == "mixed" else "double"
-    with R.Server(budgetBytes=150e9, maxActive=slots, precision=prec, transformSizes=sizes) as srv:
+    with R.Server(budgetBytes=150e9, maxActive=slots, precision=prec, transformSizes=sizes, maxBatch=batch) as srv:
         warm = serving_requests(R, 4, seed + 1)
         for r in [srv.submit(q) for q in warm]:
             srv.wait(r, release=True)
@@ -283,7 +297,8 @@ def run_serving(args):
 
     R.load()
     with Clocks(0) as clk:
-        out = serve_stream(R, args.requests, args.slots, args.serving_precision, args.serving_sizes)
+        out = serve_stream(R, args.requests, args.slots, args.serving_precision, args.serving_sizes,
+                           batch=args.serving_batch)
     prec = "single" if args.serving_precision == "mixed" else "double"
     line = {
         "metric": "serving: solves/s and p50/p99 latency of a Poisson request stream at 0.8 x measured capacity",
@@ -293,8 +308,9 @@ def run_serving(args):
         "data": "synthetic request stream, seed 0",
         "config": {"workload": f"c5: {out['requests']} requests, Nx, Ny log-U[16,768] (half strips, delta gap), "
                                f"cell lambda/U[10,25], f U[0.5,3] GHz, COCG + rChan to 1e-6, "
-                               f"{args.serving_precision}, {args.serving_sizes} transform sizes",
-                   "slots": args.slots, "budget_bytes": 150e9, "capacity_solves_per_s": out["capacity_solves_per_s"],
+                               f"{args.serving_precision}, {args.serving_sizes} transform sizes"
+                               + (f", plate batches of up to {args.serving_batch}" if args.serving_batch > 1 else ""),
+                   "slots": args.slots, "max_batch": args.serving_batch, "budget_bytes": 150e9, "capacity_solves_per_s": out["capacity_solves_per_s"],
                    "arrival_rate": out["arrival_rate"]},
         "p50_ms": out["p50_ms"], "p99_ms": out["p99_ms"], "converged": out["converged"], "failed": out["failed"],
         "max_unknowns": out["max_unknowns"], "clocks": clk.summary(),
@@ -413,7 +429,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "500"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -852,6 +868,8 @@ def main():
     ap.add_argument("--serving-precision", default="double", choices=["double", "mixed"])
     ap.add_argument("--serving-sizes", default="powerOfTwo", choices=["reference", "powerOfTwo", "autotune"],
                     help="c5: the server's transform-size policy")
+    ap.add_argument("--serving-batch", type=int, default=0,
+                    help="c5: requests a worker solves together as one plate batch (0: each alone)")
     ap.add_argument("--serving-requests", type=int, default=32,
                     help="c2: requests of the short serving stream in the default line (0: none)")
     args = ap.parse_args()

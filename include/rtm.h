@@ -269,9 +269,14 @@ RTM_API int rtm_solve_mixed(rtm_operator* op, rtm_operator* inner_op, rtm_precon
 typedef struct rtm_plate_batch rtm_plate_batch;
 RTM_API int rtm_plate_batch_create(rtm_operator* const* ops, rtm_preconditioner* const* pcs, int count,
                                    rtm_plate_batch** out);
-RTM_API int rtm_plate_batch_info(const rtm_plate_batch* batch, int64_t* stride, int* count, int* fused);
-/* y = A x entry by entry (x and y count x stride elements). */
-RTM_API int rtm_plate_batch_apply(rtm_plate_batch* batch, const void* x, void* y, int where, void* stream);
+/* fused: the products share each kernel launch; fused_preconditioner: so do the block-Jacobi preconditioners
+ * (circulant preconditioners, whose transforms follow each face grid, run entry by entry). */
+RTM_API int rtm_plate_batch_info(const rtm_plate_batch* batch, int64_t* stride, int* count, int* fused,
+                                 int* fused_preconditioner);
+/* y = A x (preconditioner 0) or y = M x (preconditioner 1, a batch created with preconditioners), entry
+ * by entry; x and y are count x stride elements. */
+RTM_API int rtm_plate_batch_apply(rtm_plate_batch* batch, int preconditioner, const void* x, void* y, int where,
+                                  void* stream);
 /* rtm_solve over the batch (method RTM_METHOD_CG or RTM_METHOD_GMRES): every entry stops on its own
  * tolerance; history (count x (max_iterations+1)) and stats (count) as rtm_solve's. */
 RTM_API int rtm_plate_batch_solve(rtm_plate_batch* batch, const rtm_solve_config* config, const void* b,

@@ -113,8 +113,8 @@ _SIGNATURES = {
     "rtm_tune_clear": [],
     "rtm_tune_set": [C.c_int] * 5,
     "rtm_plate_batch_create": [_PP, _PP, C.c_int, _PP],
-    "rtm_plate_batch_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int)],
-    "rtm_plate_batch_apply": [_P, _P, _P, C.c_int, _P],
+    "rtm_plate_batch_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "rtm_plate_batch_apply": [_P, C.c_int, _P, _P, C.c_int, _P],
     "rtm_plate_batch_solve": [_P, C.POINTER(SolveConfig), _P, _P, _P, C.c_int, _P, C.POINTER(SolveStats), _P],
     "rtm_plate_batch_destroy": [_P],
     "rtm_operator_create_dense": [_P, C.c_int64, C.c_int, _PP],

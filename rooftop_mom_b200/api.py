@@ -831,9 +831,9 @@ class PlateBatch:
         out = C.c_void_p()
         L.call("rtm_plate_batch_create", ops, pcs, count, C.byref(out))
         self._handle = out
-        stride, n, fused = C.c_int64(), C.c_int(), C.c_int()
-        L.call("rtm_plate_batch_info", out, C.byref(stride), C.byref(n), C.byref(fused))
-        self._stride, self._fused = stride.value, bool(fused.value)
+        stride, n, fused, fused_pc = C.c_int64(), C.c_int(), C.c_int(), C.c_int()
+        L.call("rtm_plate_batch_info", out, C.byref(stride), C.byref(n), C.byref(fused), C.byref(fused_pc))
+        self._stride, self._fused, self._fused_pc = stride.value, bool(fused.value), bool(fused_pc.value)
         self._counts = [o.rooftopCount() for o in self._ops]
         self.precision = getattr(self._ops[0], "precision", "double")
 
@@ -853,6 +853,9 @@ class PlateBatch:
 
     def fused(self):
         return self._fused
+
+    def fusedPreconditioner(self):
+        return self._fused_pc
 
     def rooftopCounts(self):
         return list(self._counts)
@@ -879,20 +882,27 @@ class PlateBatch:
     def _unpack(self, packed):
         return [packed[k * self._stride:k * self._stride + n] for k, n in enumerate(self._counts)]
 
-    def apply(self, vectors):
-        """y_k = A_k x_k for every entry."""
+    def _apply(self, vectors, which):
         device = _is_device(vectors[0])
         x = self._pack(vectors, device)
         if device:
             import torch
             y = torch.empty_like(x)
-            L.call("rtm_plate_batch_apply", self._handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+            L.call("rtm_plate_batch_apply", self._handle, which, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                    L.DEVICE, None)
         else:
             y = np.empty_like(x)
-            L.call("rtm_plate_batch_apply", self._handle, x.ctypes.data_as(C.c_void_p),
+            L.call("rtm_plate_batch_apply", self._handle, which, x.ctypes.data_as(C.c_void_p),
                    y.ctypes.data_as(C.c_void_p), L.HOST, None)
         return self._unpack(y)
+
+    def apply(self, vectors):
+        """y_k = A_k x_k for every entry."""
+        return self._apply(vectors, 0)
+
+    def precondition(self, vectors):
+        """y_k = M_k x_k for every entry (a batch made with preconditioners)."""
+        return self._apply(vectors, 1)
 
 
 class Resources:

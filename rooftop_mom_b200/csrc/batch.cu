@@ -53,6 +53,9 @@ int BatchOp::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags s
         if (work.bytes < plates[0]->work_bytes_per_rhs() * ops.size())
             return fail(RTM_ERR_ARG, "the plate batch was not reserved");
         RTM_TRY(apply_plate_batch(plates, descs.ptr, stride, work.ptr, fault, x, y, s, skip));
+    } else if (fused_bj) {
+        RTM_TRY(apply_block_jacobi_batch(descs.as<BjEntry>(), (int)ops.size(), bj_blocks, bj_S, precision, x, y, stride,
+                                         s, skip));
     } else {
         const size_t elem = precision == RTM_FP64 ? sizeof(double2) : sizeof(float2);
         for (size_t k = 0; k < ops.size(); ++k) {
@@ -104,6 +107,19 @@ std::unique_ptr<BatchOp> make_batch(const std::vector<LinearOp*>& ops, int64_t s
             b->fused = true;
         } else {
             b->plates.clear();
+        }
+        std::vector<BjEntry> bj(ops.size());
+        bool all_bj = !b->fused;
+        for (size_t k = 0; k < ops.size() && all_bj; ++k)
+            all_bj = block_jacobi_entry(ops[k], &bj[k]) && bj[k].S == bj[0].S;
+        if (all_bj) {
+            for (const BjEntry& e : bj) b->bj_blocks = std::max(b->bj_blocks, e.nblocks);
+            b->bj_S = bj[0].S;
+            if ((*status = b->descs.alloc(sizeof(BjEntry) * bj.size())) != RTM_OK) return nullptr;
+            if ((*status = check_cuda(cudaMemcpyAsync(b->descs.ptr, bj.data(), b->descs.bytes, cudaMemcpyHostToDevice, s),
+                                      "cudaMemcpyAsync")) != RTM_OK)
+                return nullptr;
+            b->fused_bj = true;
         }
     }
     if ((*status = check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize")) != RTM_OK) return nullptr;

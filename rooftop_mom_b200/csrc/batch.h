@@ -4,9 +4,10 @@
 // keeps its plate's n_k rooftops first and zeros after them. A batch operator applies every entry's own
 // operator: split products that share their transform grid and precision on the power-of-two path run as
 // one launch of each of their three kernels for the whole batch (grid_fast.cu reads each right-hand side's
-// plate from a descriptor table); other operators and the preconditioners run one after another on their
-// entries. Every apply zeroes the entries' tails, so the Krylov solvers run on the batch unchanged: the
-// padding adds zeros to every sum.
+// plate from a descriptor table), block-Jacobi preconditioners of one packed block size as one launch too;
+// other operators (the circulant preconditioners among them) run one after another on their entries.
+// Every apply zeroes the entries' tails, so the Krylov solvers run on the batch unchanged: the padding adds
+// zeros to every sum.
 #pragma once
 
 #include <memory>
@@ -21,8 +22,10 @@ struct BatchOp : LinearOp {
     std::vector<int64_t> counts;         // per entry: unknowns
     int64_t stride = 0;                  // elements of an entry
     bool fused = false;                  // one launch per kernel for the whole batch
-    std::vector<const GridApplicator*> plates;  // fused: the entries' products
-    DeviceBuffer descs, tails, work;     // fused: plate table, per-entry unknowns (device), working grids
+    std::vector<const GridApplicator*> plates;  // fused products: the entries' products
+    bool fused_bj = false;               // fused block-Jacobi preconditioners
+    int bj_blocks = 0, bj_S = 0;         // fused block-Jacobi: the most blocks of an entry, their packed size
+    DeviceBuffer descs, tails, work;     // fused: plate or block-Jacobi table, per-entry unknowns (device), W
     int* fault = nullptr;
 
     int apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags skip) override;

@@ -728,34 +728,38 @@ int rtm_plate_batch_create(rtm_operator* const* ops, rtm_preconditioner* const* 
     h->op = make_batch(o, stride, true, h->stream, &st);
     RTM_TRY(st);
     if (pcs) {
-        h->pc = make_batch(p, stride, false, h->stream, &st);
+        h->pc = make_batch(p, stride, true, h->stream, &st);
         RTM_TRY(st);
     }
     *out = h.release();
     return RTM_OK;
 }
 
-int rtm_plate_batch_info(const rtm_plate_batch* b, int64_t* stride, int* count, int* fused) {
+int rtm_plate_batch_info(const rtm_plate_batch* b, int64_t* stride, int* count, int* fused, int* fused_preconditioner) {
     if (!b) return fail(RTM_ERR_ARG, "null handle");
     if (stride) *stride = b->op->stride;
     if (count) *count = (int)b->op->ops.size();
     if (fused) *fused = b->op->fused ? 1 : 0;
+    if (fused_preconditioner) *fused_preconditioner = b->pc && b->pc->fused_bj ? 1 : 0;
     return RTM_OK;
 }
 
-int rtm_plate_batch_apply(rtm_plate_batch* b, const void* x, void* y, int where, void* stream) {
+int rtm_plate_batch_apply(rtm_plate_batch* b, int preconditioner, const void* x, void* y, int where, void* stream) {
     if (!b || !x || !y) return fail(RTM_ERR_ARG, "null argument");
     RTM_TRY(check_where(where));
+    if (preconditioner != 0 && preconditioner != 1) return fail(RTM_ERR_ARG, "preconditioner is 0 or 1");
+    if (preconditioner && !b->pc) return fail(RTM_ERR_ARG, "the batch has no preconditioners");
+    BatchOp* op = preconditioner ? b->pc.get() : b->op.get();
     cudaStream_t s = pick(stream, b->stream);
-    const int count = (int)b->op->ops.size();
-    const int64_t total = b->op->stride * count;
-    const int prec = b->op->precision;
+    const int count = (int)op->ops.size();
+    const int64_t total = op->stride * count;
+    const int prec = op->precision;
     Staged in;
     Out o;
     RTM_TRY(stage_in(x, total, prec, where, in, s));
     RTM_TRY(out_prepare(y, total, prec, where, o, s));
-    RTM_TRY(b->op->reserve(count));
-    RTM_TRY(b->op->apply(in.ptr, o.ptr, count, s, SkipFlags{}));
+    RTM_TRY(op->reserve(count));
+    RTM_TRY(op->apply(in.ptr, o.ptr, count, s, SkipFlags{}));
     RTM_TRY(out_finish(y, total, prec, where, o, s));
     if (where == RTM_HOST || !stream) RTM_CUDA(cudaStreamSynchronize(s));
     return device_fault_check(s);

@@ -190,6 +190,43 @@ __global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, c
     y[rhs * n + idx[r]] = acc;
 }
 
+// k_bj_apply for a batch of block-Jacobi operators: right-hand side k takes entry k's blocks.
+template <typename T2>
+__global__ void k_bj_apply_batch(const BjEntry* __restrict__ entries, const T2* __restrict__ x, T2* __restrict__ y,
+                                 int64_t stride, const int* skip, int skip_stride) {
+    const int rhs = blockIdx.y;
+    if (skip && skip[(int64_t)rhs * skip_stride]) return;
+    const BjEntry e = entries[rhs];
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int S = e.S;
+    const int blk = (int)(t / S), r = (int)(t % S);
+    if (blk >= e.nblocks) return;
+    const int cnt = e.counts[blk];
+    if (r >= cnt) return;
+    const int64_t* idx = e.index + (int64_t)blk * S;
+    const T2* col = static_cast<const T2*>(e.inv) + (int64_t)blk * S * S + r;
+    const T2* xr = x + rhs * stride;
+    T2 acc = czero<T2>();
+#pragma unroll 8
+    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
+    y[rhs * stride + idx[r]] = acc;
+}
+
+int apply_block_jacobi_batch(const BjEntry* entries, int count, int max_blocks, int S, int precision, const void* x,
+                             void* y, int64_t stride, cudaStream_t s, SkipFlags skip) {
+    const int64_t threads = (int64_t)max_blocks * S;
+    const dim3 g((unsigned)((threads + 255) / 256), count);
+    if (precision == RTM_FP64)
+        k_bj_apply_batch<double2><<<g, 256, 0, s>>>(entries, static_cast<const double2*>(x), static_cast<double2*>(y),
+                                                    stride, skip.ptr, skip.stride);
+    else
+        k_bj_apply_batch<float2><<<g, 256, 0, s>>>(entries, static_cast<const float2*>(x), static_cast<float2*>(y),
+                                                   stride, skip.ptr, skip.stride);
+    count_launch();
+    RTM_CUDA(cudaGetLastError());
+    return RTM_OK;
+}
+
 struct BlockJacobi : LinearOp {
     int nblocks = 0;
     int S = kMaxBlockUnknowns;  // unknowns a block at most (packed stride)
@@ -211,6 +248,17 @@ struct BlockJacobi : LinearOp {
     }
     double stored_bytes() const override { return (double)(counts.bytes + index.bytes + inv.bytes); }
 };
+
+bool block_jacobi_entry(const LinearOp* op, BjEntry* out) {
+    const auto* bj = dynamic_cast<const BlockJacobi*>(op);
+    if (!bj) return false;
+    out->nblocks = bj->nblocks;
+    out->S = bj->S;
+    out->counts = bj->counts.as<int>();
+    out->index = bj->index.as<int64_t>();
+    out->inv = bj->inv.ptr;
+    return true;
+}
 
 std::unique_ptr<LinearOp> make_block_jacobi(const DeviceGenerators& gen, double size_x, double size_y, int bx, int by,
                                             int precision, cudaStream_t s, int* status) {

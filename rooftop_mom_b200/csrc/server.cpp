@@ -394,7 +394,7 @@ struct rtm_server {
         std::unique_ptr<BatchOp> A = make_batch(ops, stride, true, s, &st), M;
         RTM_TRY(st);
         if (!pcs.empty()) {
-            M = make_batch(pcs, stride, false, s, &st);
+            M = make_batch(pcs, stride, true, s, &st);
             RTM_TRY(st);
         }
         const size_t vec = (size_t)stride * sizeof(double2);

@@ -91,8 +91,8 @@ def test_plate_batches_and_transform_sizes_check_their_arguments_first(library):
     assert lib.rtm_plate_batch_create(ops, None, 2, C.byref(out)) == _lib.ERR_ARG
     assert "null operator" in _lib.last_error()
     v64, v = C.c_int64(), C.c_int()
-    assert lib.rtm_plate_batch_info(None, C.byref(v64), C.byref(v), C.byref(v)) == _lib.ERR_ARG
-    assert lib.rtm_plate_batch_apply(None, None, None, _lib.HOST, None) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_info(None, C.byref(v64), C.byref(v), C.byref(v), C.byref(v)) == _lib.ERR_ARG
+    assert lib.rtm_plate_batch_apply(None, 0, None, None, _lib.HOST, None) == _lib.ERR_ARG
     assert lib.rtm_plate_batch_solve(None, None, None, None, None, _lib.HOST, None, None, None) == _lib.ERR_ARG
     assert lib.rtm_plate_batch_destroy(None) == 0
     assert lib.rtm_tune_set(100, 80, 0, 64, 128) == _lib.ERR_ARG

@@ -73,8 +73,8 @@ def test_a_batch_product_on_the_device_keeps_the_tails_zero():
 
     from rooftop_mom_b200 import _lib as L
 
-    L.call("rtm_plate_batch_apply", batch._handle, C.c_void_p(packed.data_ptr()), C.c_void_p(y.data_ptr()), L.DEVICE,
-           None)
+    L.call("rtm_plate_batch_apply", batch._handle, 0, C.c_void_p(packed.data_ptr()), C.c_void_p(y.data_ptr()),
+           L.DEVICE, None)
     torch.cuda.synchronize()
     for k, op in enumerate(ops):
         n = op.rooftopCount()
@@ -100,14 +100,34 @@ def test_a_batch_solve_matches_each_plates_own_solve(method, pc):
     rhs = [R.Excitation.planeWave(prob, direction=d, polarization=p) for (prob, _), d, p in zip(plates, dirs, pols)]
     solver = R.Solver(method=method, tolerance=1e-6, restart=50, maxIterationCount=10000, side="right")
     batch = R.PlateBatch(ops, pcs)
-    assert batch.fused()
+    assert batch.fused() and batch.fusedPreconditioner() == (pc == "blockJacobi")
     res = solver.solveBatch(batch, rhs)
     for k, (r, op, p, e) in enumerate(zip(res, ops, pcs, rhs)):
         own = solver.solve(op, e, preconditioner=p)
         tight = R.Solver(method=method, tolerance=1e-10, restart=50, maxIterationCount=20000,
                          side="right").solve(op, e, preconditioner=p)
         assert r.converged() and r.residualNorm() <= 1e-6, (k, r.iterationCount(), r.residualNorm())
-        assert abs(r.iterationCount() - own.iterationCount()) <= max(3, own.iterationCount() // 50)
+        # the batch's sums run over the padded stride: rounding may move the stopping test by a few iterations
+        assert abs(r.iterationCount() - own.iterationCount()) <= max(5, own.iterationCount() // 20)
         assert rel(r.solution(), tight.solution()) < 20 * rel(own.solution(), tight.solution()) + 1e-12
         # the RCS of the entry's plane wave, through the entry's own excitation
         assert abs(r.radarCrossSection() - own.radarCrossSection()) <= 1e-4 * abs(own.radarCrossSection())
+
+
+@pytest.mark.parametrize("kind", ["blockJacobi", "rChan"])
+def test_a_batch_preconditioner_equals_each_plates_own(kind):
+    """Block-Jacobi preconditioners of a batch run as one launch, circulant ones entry by entry: either way
+    each entry's output is its plate's own preconditioner's, to the last bit."""
+    import rooftop_mom_b200 as R
+
+    plates = _plates(plates=[(40, 33), (64, 64), (50, 61)], fft=(64, 64))
+    ops = [op for _, op in plates]
+    if kind == "blockJacobi":
+        pcs = [R.Preconditioner.blockJacobi(prob, (2, 2)) for prob, _ in plates]
+    else:
+        pcs = [R.Preconditioner(prob, kernel="rChan") for prob, _ in plates]
+    batch = R.PlateBatch(ops, pcs)
+    assert batch.fused() and batch.fusedPreconditioner() == (kind == "blockJacobi")
+    xs = [random_vector(op.rooftopCount(), seed=70 + k) for k, op in enumerate(ops)]
+    for p, x, y in zip(pcs, xs, batch.precondition(xs)):
+        assert np.array_equal(np.asarray(y), np.asarray(p.apply(x)))
