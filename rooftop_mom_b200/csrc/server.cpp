@@ -197,9 +197,10 @@ struct rtm_server {
                             ++it;
                         }
                     }
+                const double now = seconds_since(epoch);  // a batch's requests start together
                 for (Record* g : group) {
                     g->res.state = RTM_REQUEST_RUNNING;
-                    g->res.started_s = seconds_since(epoch);
+                    g->res.started_s = now;
                 }
             }
             // RUNNING is not a finished state, so no poll releases the records while they run.
@@ -207,11 +208,12 @@ struct rtm_server {
             const int st = group.size() == 1 ? run(*group[0], outs[0]) : run_batch(group, outs);
             {
                 std::lock_guard<std::mutex> lk(mu);
+                const double now = seconds_since(epoch);  // and finish together
                 for (size_t k = 0; k < group.size(); ++k) {
                     Record* r = group[k];
                     outs[k].commit(r->res);
                     r->current = std::move(outs[k].current);
-                    r->res.finished_s = seconds_since(epoch);
+                    r->res.finished_s = now;
                     r->res.status = st;
                     held -= r->res.bytes;
                     --admitted;
