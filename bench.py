@@ -874,6 +874,15 @@ def main():
                     help="c2: requests of the short serving stream in the default line (0: none)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if args.workload == "c4u" and args.once:
+        # one batched step of the c4u plates (the profiler captures run)
+        import rooftop_mom_b200 as R
+
+        R.load()
+        res, _, fused, ts = plate_batch_step(R, w, True)
+        print(f"c4u: {len(res)} plates in one batch (fused {fused}), iterations {max(r.iterationCount() for r in res)}, "
+              f"residual {max(r.residualNorm() for r in res):.3e}, solves {ts * 1e3:.1f} ms")
+        return
     if args.workload in ("c4", "c4u", "c5") and not args.matvec:
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": f"the CPU oracle arm times single-plate solves "
