@@ -19,9 +19,11 @@ __global__ void k_zero_tails(T2* __restrict__ y, int64_t stride, const int64_t* 
 
 }  // namespace
 
-int zero_tails(void* y, int precision, int64_t stride, const int64_t* counts_device, int count, cudaStream_t s,
-               SkipFlags skip) {
-    const dim3 grid(64, count);
+int zero_tails(void* y, int precision, int64_t stride, const int64_t* counts_device, int count, int64_t max_tail,
+               cudaStream_t s, SkipFlags skip) {
+    if (max_tail <= 0) return RTM_OK;
+    // about eight elements a thread: a CTA or a few per entry
+    const dim3 grid((unsigned)std::min<int64_t>(64, (max_tail + 2047) / 2048), count);
     if (precision == RTM_FP64)
         k_zero_tails<double2><<<grid, 256, 0, s>>>(static_cast<double2*>(y), stride, counts_device, skip.ptr,
                                                    skip.stride);
@@ -64,7 +66,7 @@ int BatchOp::apply(const void* x, void* y, int nrhs, cudaStream_t s, SkipFlags s
                                   static_cast<char*>(y) + k * stride * elem, 1, s, sk));
         }
     }
-    return zero_tails(y, precision, stride, tails.as<int64_t>(), (int)ops.size(), s, skip);
+    return zero_tails(y, precision, stride, tails.as<int64_t>(), (int)ops.size(), max_tail, s, skip);
 }
 
 std::unique_ptr<BatchOp> make_batch(const std::vector<LinearOp*>& ops, int64_t stride, bool fuse, cudaStream_t s,
@@ -89,6 +91,7 @@ std::unique_ptr<BatchOp> make_batch(const std::vector<LinearOp*>& ops, int64_t s
             return nullptr;
         }
         b->counts.push_back(op->n);
+        b->max_tail = std::max(b->max_tail, stride - op->n);
     }
     if ((*status = b->tails.alloc(sizeof(int64_t) * ops.size())) != RTM_OK) return nullptr;
     if ((*status = check_cuda(cudaMemcpyAsync(b->tails.ptr, b->counts.data(), b->tails.bytes, cudaMemcpyHostToDevice, s),

@@ -20,6 +20,7 @@ namespace rtm {
 struct BatchOp : LinearOp {
     std::vector<LinearOp*> ops;          // per entry (borrowed; the handles outlive the batch)
     std::vector<int64_t> counts;         // per entry: unknowns
+    int64_t max_tail = 0;                // stride minus the fewest unknowns of an entry
     int64_t stride = 0;                  // elements of an entry
     bool fused = false;                  // one launch per kernel for the whole batch
     std::vector<const GridApplicator*> plates;  // fused products: the entries' products
@@ -38,8 +39,9 @@ struct BatchOp : LinearOp {
 std::unique_ptr<BatchOp> make_batch(const std::vector<LinearOp*>& ops, int64_t stride, bool fuse, cudaStream_t s,
                                     int* status);
 
-// Zeroes elements [counts[k], stride) of entry k of y (k < count, where the skip flag is zero).
-int zero_tails(void* y, int precision, int64_t stride, const int64_t* counts_device, int count, cudaStream_t s,
-               SkipFlags skip);
+// Zeroes elements [counts[k], stride) of entry k of y (k < count, where the skip flag is zero); max_tail, the
+// longest tail, sizes the launch.
+int zero_tails(void* y, int precision, int64_t stride, const int64_t* counts_device, int count, int64_t max_tail,
+               cudaStream_t s, SkipFlags skip);
 
 }  // namespace rtm

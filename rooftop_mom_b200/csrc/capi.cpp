@@ -789,11 +789,12 @@ int rtm_plate_batch_solve(rtm_plate_batch* b, const rtm_solve_config* config, co
     DeviceBuffer bz, xz;
     RTM_TRY(bz.alloc(total * elem));
     RTM_CUDA(cudaMemcpyAsync(bz.ptr, sb.ptr, total * elem, cudaMemcpyDeviceToDevice, s));
-    RTM_TRY(zero_tails(bz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, s, SkipFlags{}));
+    RTM_TRY(zero_tails(bz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, b->op->max_tail, s, SkipFlags{}));
     if (x0) {
         RTM_TRY(xz.alloc(total * elem));
         RTM_CUDA(cudaMemcpyAsync(xz.ptr, sx0.ptr, total * elem, cudaMemcpyDeviceToDevice, s));
-        RTM_TRY(zero_tails(xz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, s, SkipFlags{}));
+        RTM_TRY(zero_tails(xz.ptr, prec, stride, b->op->tails.as<int64_t>(), count, b->op->max_tail, s,
+                           SkipFlags{}));
     }
     SolveConfig cfg;
     cfg.method = config->method;
