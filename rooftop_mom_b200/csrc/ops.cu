@@ -168,7 +168,48 @@ __global__ void k_bj_pack(int nblocks, int S, const double2* __restrict__ inv64,
     }
 }
 
-// y(idx_r) = sum_c inv(r, c) x(idx_c) over the block's unknowns, one thread per (block, row).
+// y(idx_r) = sum_c inv(r, c) x(idx_c) over the block's unknowns, one thread per (block, row). Where S divides
+// the warp (blocks of 1, 2, 4, 8 or 16 unknowns, 2 x 2 faces among them), the S threads of a block each gather
+// their own x(idx_r) and pass it to the others by warp shuffles, so a thread issues one index and one vector
+// load instead of S of each; the sum runs over c in the same order either way.
+template <typename T2, int SC>  // SC: S as a compile-time constant (the loops unroll), or 0
+__device__ __forceinline__ void bj_rows(int nblocks, int S_, const int* __restrict__ counts,
+                                        const int64_t* __restrict__ index, const T2* __restrict__ inv,
+                                        const T2* __restrict__ xr, T2* __restrict__ yr, int64_t t) {
+    const int S = SC ? SC : S_;
+    const int blk = (int)(t / S), r = (int)(t % S);
+    if ((32 % S) == 0) {
+        // every lane reaches the shuffles: blocks past the end and rows past a block's count carry zeros
+        const bool in = blk < nblocks;
+        const int cnt = in ? counts[blk] : 0;
+        const int64_t* idx = index + (int64_t)blk * S;
+        const bool row = in && r < cnt;
+        const T2 mine = row ? xr[idx[r]] : czero<T2>();
+        const T2* col = inv + (int64_t)blk * S * S + r;
+        const int base = (int)(threadIdx.x & 31) - r;  // the block's first lane (blocks align with warps)
+        T2 acc = czero<T2>();
+#pragma unroll 16
+        for (int c = 0; c < S; ++c) {
+            T2 v;
+            v.x = __shfl_sync(0xffffffffu, mine.x, base + c);
+            v.y = __shfl_sync(0xffffffffu, mine.y, base + c);
+            if (c < cnt && row) acc = cadd(acc, cmul(col[c * S], v));
+        }
+        if (row) yr[idx[r]] = acc;
+        return;
+    }
+    if (blk >= nblocks) return;
+    const int cnt = counts[blk];
+    if (r >= cnt) return;
+    const int64_t* idx = index + (int64_t)blk * S;
+    const T2* col = inv + (int64_t)blk * S * S + r;
+    T2 acc = czero<T2>();
+    // unrolled so that the loads of all columns are in flight together (the order of the sum is unchanged)
+#pragma unroll 8
+    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
+    yr[idx[r]] = acc;
+}
+
 template <typename T2>
 __global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, const int64_t* __restrict__ index,
                            const T2* __restrict__ inv, const T2* __restrict__ x, T2* __restrict__ y, int64_t n,
@@ -176,18 +217,8 @@ __global__ void k_bj_apply(int nblocks, int S, const int* __restrict__ counts, c
     const int rhs = blockIdx.y;
     if (skip && skip[(int64_t)rhs * stride]) return;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int blk = (int)(t / S), r = (int)(t % S);
-    if (blk >= nblocks) return;
-    const int cnt = counts[blk];
-    if (r >= cnt) return;
-    const int64_t* idx = index + (int64_t)blk * S;
-    const T2* col = inv + (int64_t)blk * S * S + r;
-    const T2* xr = x + rhs * n;
-    T2 acc = czero<T2>();
-    // unrolled so that the loads of all columns are in flight together (the order of the sum is unchanged)
-#pragma unroll 8
-    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
-    y[rhs * n + idx[r]] = acc;
+    if (S == 8) bj_rows<T2, 8>(nblocks, S, counts, index, inv, x + rhs * n, y + rhs * n, t);
+    else bj_rows<T2, 0>(nblocks, S, counts, index, inv, x + rhs * n, y + rhs * n, t);
 }
 
 // k_bj_apply for a batch of block-Jacobi operators: right-hand side k takes entry k's blocks.
@@ -198,18 +229,12 @@ __global__ void k_bj_apply_batch(const BjEntry* __restrict__ entries, const T2* 
     if (skip && skip[(int64_t)rhs * skip_stride]) return;
     const BjEntry e = entries[rhs];
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int S = e.S;
-    const int blk = (int)(t / S), r = (int)(t % S);
-    if (blk >= e.nblocks) return;
-    const int cnt = e.counts[blk];
-    if (r >= cnt) return;
-    const int64_t* idx = e.index + (int64_t)blk * S;
-    const T2* col = static_cast<const T2*>(e.inv) + (int64_t)blk * S * S + r;
-    const T2* xr = x + rhs * stride;
-    T2 acc = czero<T2>();
-#pragma unroll 8
-    for (int c = 0; c < cnt; ++c) acc = cadd(acc, cmul(col[c * S], xr[idx[c]]));
-    y[rhs * stride + idx[r]] = acc;
+    if (e.S == 8)
+        bj_rows<T2, 8>(e.nblocks, e.S, e.counts, e.index, static_cast<const T2*>(e.inv), x + rhs * stride,
+                       y + rhs * stride, t);
+    else
+        bj_rows<T2, 0>(e.nblocks, e.S, e.counts, e.index, static_cast<const T2*>(e.inv), x + rhs * stride,
+                       y + rhs * stride, t);
 }
 
 int apply_block_jacobi_batch(const BjEntry* entries, int count, int max_blocks, int S, int precision, const void* x,
