@@ -584,10 +584,15 @@ __device__ __forceinline__ RowPack<T2, RL> load_rows(const T2* __restrict__ p, i
     return r;
 }
 
-template <typename T2, int RL>
+// KQE: the basis columns a warp takes at once in the dots (1, 2, 4 or 8; the launcher picks the fewest that
+// cover the step's columns); each lane then keeps KQ / KQE groups of rows in flight, so a dot pass over few
+// columns takes as many loads per round as one over many, in fewer rounds.
+template <typename T2, int RL, int KQE>
 __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict__ V, T2* __restrict__ w, int64_t n,
                                                            int nrhs, GmState* st, GmArrays ar, int mode, int chunk) {
-    constexpr int NW = kRT / 32, KQ = kStreamCols / NW;
+    // (two-row FP32 loads over one or two columns hold half the groups: the registers of two CTAs an SM
+    // spill otherwise)
+    constexpr int NW = kRT / 32, KQ = kStreamCols / NW, RU = (RL == 2 && KQE <= 2) ? KQ / KQE / 2 : KQ / KQE;
     using A2 = typename OrthAcc<T2>::type;  // arithmetic of the passes: FP64 for an FP64 basis, FP32 for FP32
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ A2 coef[kStreamCols];
@@ -680,53 +685,69 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
         __syncthreads();  // the chunk of w
         const bool wide = cols >= NW;
         const int G = wide ? 1 : NW / cols;  // warps per column
-        A2 acc[KQ];
+        const bool on = wide || warp < G * cols;
+        const int kw = wide ? warp : warp % cols;
+        const int slice = wide ? 0 : warp / cols;
+        // slices start on multiples of RL (the packed loads' alignment)
+        const int rs = (int)((int64_t)len * slice / G) / RL * RL;
+        const int re = slice + 1 == G ? len : (int)((int64_t)len * (slice + 1) / G) / RL * RL;
+        // groups of KQE columns (one group when the launcher's KQE covers the step's columns)
+        for (int q0 = 0; q0 < KQ; q0 += KQE) {
+            if (q0 > 0 && !(wide && kw + NW * q0 < cols)) {
+                // no column of this warp left: the group's sums are zero
 #pragma unroll
-        for (int q = 0; q < KQ; ++q) acc[q] = from_d2<A2>(make_double2(0, 0));
-        if (wide || warp < G * cols) {
-            const int kw = wide ? warp : warp % cols;
-            const int slice = wide ? 0 : warp / cols;
-            // slices start on multiples of RL (the packed loads' alignment)
-            const int rs = (int)((int64_t)len * slice / G) / RL * RL;
-            const int re = slice + 1 == G ? len : (int)((int64_t)len * (slice + 1) / G) / RL * RL;
-            // two groups of RL rows a lane per step: up to 2 KQ loads in flight
-            for (int r = rs + RL * lane; r < re; r += 64 * RL) {
-                const int r2 = r + 32 * RL;
-                const int n0 = min(RL, re - r), n1 = max(0, min(RL, re - r2));
-                RowPack<T2, RL> t[KQ], u[KQ];
+                for (int q = 0; q < KQE; ++q)
+                    if (lane == 0) red[warp][q0 + q] = make_double2(0, 0);
+                continue;
+            }
+            A2 acc[KQE];
 #pragma unroll
-                for (int q = 0; q < KQ; ++q) {
-                    const int k = kw + NW * q;
-                    const bool use = (wide || q == 0) && k < cols;
-                    t[q] = load_rows<T2, RL>(Vr + k * col + r, use ? n0 : 0);
-                    u[q] = load_rows<T2, RL>(Vr + k * col + r2, use ? n1 : 0);
-                }
-                T2 x[RL], x2[RL];  // kept in the stored precision until used (registers)
+            for (int q = 0; q < KQE; ++q) acc[q] = from_d2<A2>(make_double2(0, 0));
+            if (on) {
+                // RU steps of two groups of RL rows a lane at once: 2 KQE RU loads in flight (2 KQ but in one case)
+                for (int r0 = rs + RL * lane; r0 < re; r0 += 64 * RL * RU) {
+                    RowPack<T2, RL> t[RU][KQE], u[RU][KQE];
+                    T2 x[RU][RL], x2[RU][RL];  // kept in the stored precision until used (registers)
 #pragma unroll
-                for (int q = 0; q < RL; ++q) {
-                    x[q] = q < n0 ? ws[r + q] : from_d2<T2>(make_double2(0, 0));
-                    x2[q] = q < n1 ? ws[r2 + q] : from_d2<T2>(make_double2(0, 0));
-                }
+                    for (int g = 0; g < RU; ++g) {
+                        const int r = r0 + 64 * RL * g, r2 = r + 32 * RL;
+                        const int n0 = max(0, min(RL, re - r)), n1 = max(0, min(RL, re - r2));
 #pragma unroll
-                for (int q = 0; q < KQ; ++q)
+                        for (int q = 0; q < KQE; ++q) {
+                            const int k = kw + NW * (q0 + q);
+                            const bool use = (wide || q0 + q == 0) && k < cols;
+                            t[g][q] = load_rows<T2, RL>(Vr + k * col + r, use ? n0 : 0);
+                            u[g][q] = load_rows<T2, RL>(Vr + k * col + r2, use ? n1 : 0);
+                        }
 #pragma unroll
-                    for (int e = 0; e < RL; ++e) {
-                        const A2 a = amulc(t[q].v[e], x[e]), b = amulc(u[q].v[e], x2[e]);
-                        acc[q].x += a.x;
-                        acc[q].y += a.y;
-                        acc[q].x += b.x;
-                        acc[q].y += b.y;
+                        for (int e = 0; e < RL; ++e) {
+                            x[g][e] = e < n0 ? ws[r + e] : from_d2<T2>(make_double2(0, 0));
+                            x2[g][e] = e < n1 ? ws[r2 + e] : from_d2<T2>(make_double2(0, 0));
+                        }
                     }
-            }
-        }
 #pragma unroll
-        for (int q = 0; q < KQ; ++q) {
-            double2 v = to_d2(acc[q]);  // the sums over lanes, CTAs and chunks in FP64
-            for (int o = 16; o > 0; o >>= 1) {
-                v.x += __shfl_down_sync(0xffffffffu, v.x, o);
-                v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+                    for (int g = 0; g < RU; ++g)
+#pragma unroll
+                        for (int q = 0; q < KQE; ++q)
+#pragma unroll
+                            for (int e = 0; e < RL; ++e) {
+                                const A2 a = amulc(t[g][q].v[e], x[g][e]), b = amulc(u[g][q].v[e], x2[g][e]);
+                                acc[q].x += a.x;
+                                acc[q].y += a.y;
+                                acc[q].x += b.x;
+                                acc[q].y += b.y;
+                            }
+                }
             }
-            if (lane == 0) red[warp][q] = v;
+#pragma unroll
+            for (int q = 0; q < KQE; ++q) {
+                double2 v = to_d2(acc[q]);  // the sums over lanes, CTAs and chunks in FP64
+                for (int o = 16; o > 0; o >>= 1) {
+                    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+                    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+                }
+                if (lane == 0) red[warp][q0 + q] = v;
+            }
         }
         __syncthreads();
         for (int k = threadIdx.x; k < cols; k += kRT) {
@@ -796,19 +817,45 @@ static void stream_config(int64_t n, int* blocks, int* chunk) {
 }
 
 // (the dynamic shared-memory attributes are set before any capture, in gmres())
+template <typename T2, int KQE>
+static void launch_orth_stream(const T2* V, T2* w, int64_t n, int nrhs, GmState* st, const GmArrays& ar, int mode,
+                               cudaStream_t s) {
+    int blocks, chunk;
+    stream_config(n, &blocks, &chunk);
+    // FP32 reads two rows a load where every column starts on 16 bytes (an even length)
+    if (sizeof(T2) == 8 && n % 2 == 0)
+        k_gm_orth_stream<T2, (sizeof(T2) == 8 ? 2 : 1), KQE><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(
+            V, w, n, nrhs, st, ar, mode, chunk);
+    else
+        k_gm_orth_stream<T2, 1, KQE><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar,
+                                                                                                 mode, chunk);
+    count_launch();
+}
+
+// The shared-memory attribute of every form of k_gm_orth_stream (set before any capture).
+template <typename T2> static int stream_attrs(int bytes) {
+    const int b = std::max(bytes, 48 * 1024);
+    constexpr int RL = sizeof(T2) == 8 ? 2 : 1;
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, RL, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, RL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, RL, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, RL, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    return RTM_OK;
+}
+
+// cols: the basis columns of this Arnoldi step (the dots' column groups follow it).
 template <typename T2> static void launch_orth(const T2* V, T2* w, int64_t n, int nrhs, GmState* st, const GmArrays& ar,
-                                               int mode, cudaStream_t s) {
+                                               int mode, int cols, cudaStream_t s) {
     if (ar.m + 1 <= kStreamCols) {
-        int blocks, chunk;
-        stream_config(n, &blocks, &chunk);
-        // FP32 reads two rows a load where every column starts on 16 bytes (an even length)
-        if (sizeof(T2) == 8 && n % 2 == 0)
-            k_gm_orth_stream<T2, (sizeof(T2) == 8 ? 2 : 1)><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(
-                V, w, n, nrhs, st, ar, mode, chunk);
-        else
-            k_gm_orth_stream<T2, 1><<<dim3(blocks, nrhs), kRT, (size_t)chunk * sizeof(T2), s>>>(V, w, n, nrhs, st, ar,
-                                                                                               mode, chunk);
-        count_launch();
+        constexpr int NW = kRT / 32;
+        if (mode == 2 || cols > 4 * NW) launch_orth_stream<T2, 8>(V, w, n, nrhs, st, ar, mode, s);
+        else if (cols > 2 * NW) launch_orth_stream<T2, 4>(V, w, n, nrhs, st, ar, mode, s);
+        else if (cols > NW) launch_orth_stream<T2, 2>(V, w, n, nrhs, st, ar, mode, s);
+        else launch_orth_stream<T2, 1>(V, w, n, nrhs, st, ar, mode, s);
         return;
     }
     int TR;
@@ -1256,11 +1303,7 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
     {
         int sb, sc;
         stream_config(n, &sb, &sc);
-        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      std::max<int>(sc * (int)sizeof(T2), 48 * 1024)));
-        RTM_CUDA(cudaFuncSetAttribute(k_gm_orth_stream<T2, (sizeof(T2) == 8 ? 2 : 1)>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      std::max<int>(sc * (int)sizeof(T2), 48 * 1024)));
+        RTM_TRY(stream_attrs<T2>(sc * (int)sizeof(T2)));
     }
     RTM_CUDA(cudaFuncSetAttribute(k_gm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     std::vector<GmState> host(nrhs);
@@ -1285,9 +1328,9 @@ static int gmres(LinearOp* A, LinearOp* M, const SolveConfig& cfg, const void* b
             // CGS2: project (mode 0), subtract and project again (1), subtract the correction and take the
             // norm (2). One pass skips mode 1: mode 2 then subtracts the first projection, which mode 0
             // left in the coefficients it reads.
-            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 0, s);
-            if (cfg.gram_schmidt_passes != 1) launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, s);
-            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 2, s);
+            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 0, j + 1, s);
+            if (cfg.gram_schmidt_passes != 1) launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 1, j + 1, s);
+            launch_orth<T2>(Vp, w.as<T2>(), n, nrhs, st, ar, 2, j + 1, s);
             k_gm_next<T2><<<grid, kRT, 0, s>>>(w.as<T2>(), Vp, n, nrhs, st);
             count_launch(1);
         }
