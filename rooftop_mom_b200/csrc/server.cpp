@@ -11,7 +11,10 @@
 // the handles' own non-blocking streams: assembly, split-FFT product, preconditioner (block-Jacobi or rChan),
 // excitation on the device, the solve, the RCS or input impedance. Device work of different requests
 // overlaps; no call here synchronises the whole device. Results depend on the request alone, since
-// every launch shape follows from the request's sizes.
+// every launch shape follows from the request's sizes. With max_batch > 1 a worker takes several admitted
+// requests of one batch key and solves them as one plate batch (batch.h); their results then agree with
+// the same requests solved alone to their tolerances, and a batch that fails runs its requests alone.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -205,12 +208,25 @@ struct rtm_server {
             }
             // RUNNING is not a finished state, so no poll releases the records while they run.
             std::vector<Outcome> outs(group.size());
-            const int st = group.size() == 1 ? run(*group[0], outs[0]) : run_batch(group, outs);
+            std::vector<int> sts(group.size());
+            if (group.size() == 1) {
+                sts[0] = run(*group[0], outs[0]);
+            } else if (run_batch(group, outs) == RTM_OK) {
+                std::fill(sts.begin(), sts.end(), RTM_OK);
+            } else {
+                // the batch failed (one request's set-up, or the batch's own memory): each request runs alone,
+                // so one that cannot run fails without the others
+                for (size_t k = 0; k < group.size(); ++k) {
+                    outs[k] = Outcome{};
+                    sts[k] = run(*group[k], outs[k]);
+                }
+            }
             {
                 std::lock_guard<std::mutex> lk(mu);
                 const double now = seconds_since(epoch);  // and finish together
                 for (size_t k = 0; k < group.size(); ++k) {
                     Record* r = group[k];
+                    const int st = sts[k];
                     outs[k].commit(r->res);
                     r->current = std::move(outs[k].current);
                     r->res.finished_s = now;
