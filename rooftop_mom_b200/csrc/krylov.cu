@@ -625,7 +625,7 @@ __global__ void __launch_bounds__(kRT, 2) k_gm_orth_stream(const T2* __restrict_
                 v[q] = q < n0 ? wr[r + q] : from_d2<A2>(make_double2(0, 0));
                 v2[q] = q < n1 ? wr[r2 + q] : from_d2<A2>(make_double2(0, 0));
             }
-            constexpr int UB = 8 / RL;  // columns a batch: the same bytes in flight for every RL
+            constexpr int UB = 8;  // columns a batch: 16-byte loads, the same bytes in flight for every RL
             int k = 0;
             for (; k + UB <= cols; k += UB) {
                 RowPack<T2, RL> t[UB], t2[UB];
