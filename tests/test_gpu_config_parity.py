@@ -6,7 +6,7 @@ and whole solves of those plates against the oracle's.
       (the reference's own plate-scattering set-up, examples/plateScattering.m:31-32);
   C2: 256 x 256 faces of lambda/20, theta = 30 deg, phi = 0, TE, block-Jacobi (2 x 2 faces) GMRES(50).
 
-Tolerances are the north star's: generators 1e-12 relative, currents and RCS 1e-10 with both solves driven
+Tolerances are the path's parity bars: generators 1e-12 relative, currents and RCS 1e-10 with both solves driven
 to a relative residual of 1e-12. On the C2 plate the oracle's current at a residual of 1e-12 is within
 1.3e-12 of its current at 1e-14, so 1e-10 is well above what conditioning allows at that residual."""
 from __future__ import annotations
@@ -132,7 +132,7 @@ def test_generators_at_default_orders_match_the_oracle(count):
 # but the iteration counts drift apart (the oracle alone needs 1206 iterations to 1e-12 on the C2 plate on one
 # host and 1230 on another; with rChan the device reaches 1e-6 on that plate in 589 iterations and the oracle
 # in 694). So the iteration counts of the C1 plate are held to 5 % of the oracle's, and every solve is judged
-# by its current, with both driven to 1e-12 where the north star's 1e-10 bar applies.
+# by its current, with both driven to 1e-12 where the 1e-10 parity bar applies.
 
 def _first_below(history, tol):
     """Iterations a solve with this residual history takes to reach tol (the index of the first entry below
@@ -162,7 +162,7 @@ def test_c1_cocg_solve_matches_the_oracle():
     assert abs(got6 - want6) <= max(2, 0.05 * want6)
     assert abs(res.iterationCount() - ref.iteration_count) <= max(2, 0.05 * ref.iteration_count)
     assert rel(res.solution(), ref.solution) < 1e-6
-    # the north star's bar with both driven to 1e-12
+    # the 1e-10 parity bar with both driven to 1e-12
     res = R.Solver(method="cg", tolerance=1e-12, maxIterationCount=5000).solve(op, exc)
     ref = OS.solve("cg", apply, b, tol=1e-12, maxit=5000)
     assert res.converged() and ref.converged
