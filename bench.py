@@ -1059,8 +1059,9 @@ def main():
         # the metric's p50 / p99: a short serving stream (c5's mix), FP64 and mixed
         line["serving"] = {p: serve_stream(R, args.serving_requests, args.slots, p, args.serving_sizes)
                            for p in ("double", "mixed")}
-    if args.workload == "c2" and not args.no_arms:
-        # the metric's "mixed vs FP64": both precisions, single and batched, on the same plate
+    if args.workload == "c2" and not args.no_arms and world == 1:
+        # the metric's "mixed vs FP64": both precisions, single and batched, on the same plate (one GPU: the
+        # replicas of a multi-GPU run measure the solve rate alone)
         arms = precision_arms(R, w, min(args.steps, 5), min(args.warmup, 2))
         line["arms"] = arms
         # the target's ratio: the mixed-precision batched solver against the plain FP64 GPU path (one
