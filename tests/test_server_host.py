@@ -169,3 +169,34 @@ def test_an_unknown_transform_size_policy_is_rejected():
     h = C.c_void_p()
     with pytest.raises(L.RtmError):
         L.call("rtm_server_create", C.byref(cfg), C.byref(h))
+
+
+def test_batching_configuration_is_checked():
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    for bad in (-1, 257):
+        with pytest.raises(L.RtmError):
+            R.Server(maxBatch=bad)
+
+
+def test_batched_requests_that_fail_on_the_device_are_each_reported():
+    """The batching workers' grouping and their fallback: without a GPU a batch's set-up fails, its requests
+    then run one by one and fail at their first device call, each reported with its own status, and the
+    slots and bytes drain for the requests that wait behind them."""
+    import torch
+
+    import rooftop_mom_b200 as R
+    from rooftop_mom_b200 import _lib as L
+
+    if torch.cuda.is_available():
+        pytest.skip("on a GPU these requests run; this test follows the failure path")
+    # 40 x 32 and 50 x 60 faces share the 64 x 64 power-of-two grid; a strip never joins a batch
+    reqs = [_request((40, 32)), _request((50, 60)), _request((64, 33)), _request((33, 64)),
+            R.Request.deltaGap(41, 1, 0.05, 0.05, 2 * math.pi, portDirection="x"), _request((40, 32))]
+    with R.Server(budgetBytes=1e12, maxActive=4, maxBatch=4, transformSizes="powerOfTwo") as srv:
+        ids = [srv.submit(q) for q in reqs]
+        results = [srv.poll(rid, wait=60.0) for rid in ids]
+    assert [r["state"] for r in results] == ["failed"] * len(reqs)
+    assert all(r["status"] == L.ERR_CUDA for r in results)
+    assert all(r["finished"] >= r["started"] >= r["submitted"] for r in results)
